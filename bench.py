@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark: SSPRK(3,3) steps/s of the channel time step at 4096 x 2049, FP64.
+
+Workload (the production-size plain-method configuration): Nx = 4096, Ny = 2049, Lx = 2 pi,
+h = 1, tanh stretching beta = 2, Ub = 1, Re_b = 2e4, Kolmogorov forcing F0 = 0.05 at mode 12,
+linear drag 1e-3, adaptive dt at CFL 0.5. Synthetic initial state: Poiseuille vorticity plus a
+seeded (seed 1) random vorticity over streamwise modes 1-64 of amplitude 0.05 Ub/h, zero at
+the walls (see initial_vorticity()).
+
+One "step" = one SSPRK(3,3) step: device-side adaptive dt, three stages of (stage + forward FFT,
+cluster Thomas solve, inverse FFT, Thom closure), time advance.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl ours (default): `value` = steps/s with the state resident in HBM (CUDA graph of one step
+replayed K times, device events, max over ranks); `e2e` = the same metric through the public C
+ABI with host buffers (initial vorticity copied from pinned host memory, every step's t/dt/max
+read back to the host, final omega and psi copied back), all inside the timed region.
+--impl reference: the CPU restatement of the reference algorithm (the oracle, C++/OpenMP, all
+host threads) on the same configuration; the reference itself has no CPU path.
+Under torchrun (N > 1) every rank advances its own replica (the time step does not shard):
+value = steps of all ranks / max-over-ranks time.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nse2d-channel-gpu_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+
+WORKLOAD = dict(Nx=4096, Ny=2049, Lx=2 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, Reb=2.0e4, F0=0.05,
+                nforce=12, lin_drag=1e-3, adapt=1, cfl=0.5, dt_max=1e-2, dt_init=1e-3)
+METRIC = "SSPRK3 steps/s at 4096x2049 FP64"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _load(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def tanh_y(Ny, beta=2.0, h=1.0):
+    e = -1.0 + 2.0 * np.arange(Ny) / (Ny - 1)
+    return h * np.tanh(beta * e) / np.tanh(beta)
+
+
+def initial_vorticity(Nx, Ny, Lx, y, seed=1, amp=0.05, modes=64, Ub=1.0, h=1.0):
+    """Poiseuille vorticity 3 Ub y/h^2 plus sum_m A_m cos(k_m x + phi_m) sin(p_m pi (y+h)/(2h)),
+    m = 1..modes, A_m ~ amp (Ub/h) N(0,1)/sqrt(modes), phi_m ~ U[0, 2 pi), p_m ~ U{1..8};
+    the wall rows keep the Poiseuille value."""
+    rng = np.random.default_rng(seed)
+    M = min(modes, Nx // 2 - 1)
+    A = amp * (Ub / h) * rng.standard_normal(M) / np.sqrt(M)
+    phi = 2 * np.pi * rng.random(M)
+    p = rng.integers(1, 9, size=M)
+    x = np.arange(Nx) * (Lx / Nx)
+    k = 2 * np.pi * np.arange(1, M + 1) / Lx
+    C = A[:, None] * np.cos(k[:, None] * x[None, :] + phi[:, None])          # [M, Nx]
+    S = np.sin(p[:, None] * np.pi * (y[None, :] + h) / (2 * h))               # [M, Ny]
+    w = np.repeat((3.0 * Ub * y / (h * h))[:, None], Nx, axis=1) + S.T @ C
+    w[0] = 3.0 * Ub * y[0] / (h * h)
+    w[-1] = 3.0 * Ub * y[-1] / (h * h)
+    return np.ascontiguousarray(w)
+
+
+def algorithmic_bytes_per_step(Nx, Ny, real_bytes=8):
+    """Algorithmic HBM bytes of one step (every input read once, every output written once):
+    stage kernels read psi and omega^(s) (+ omega^n in stages 2, 3) and write omega^(s+1);
+    each Poisson solve reads omega^(s+1), writes psi-hat and reads the elimination table cp;
+    each inverse transform reads psi-hat and writes psi."""
+    N, H = Nx * Ny, Nx // 2 + 1
+    Rf, Cf, Tf = real_bytes, 2 * real_bytes, real_bytes
+    return (Rf * N * (3 + 4 + 4) + 3 * (Rf * N + Cf * H * Ny + Tf * H * (Ny - 2)) + 3 * (Cf * H * Ny + Rf * N))
+
+
+def kernel_bytes(name, stage, Nx, Ny):
+    """Algorithmic bytes of one launch of each kernel of this implementation."""
+    N, H = Nx * Ny, Nx // 2 + 1
+    if name == "k_stage_fft":
+        return 8 * N * (2 if stage == 1 else 3) + 8 * N + 16 * H * (Ny - 2)
+    if name == "k_thomas":
+        return 16 * H * (Ny - 2) * 2 + 8 * H * (Ny - 2)
+    if name == "k_ifft":
+        return 16 * H * (Ny - 2) + 8 * N
+    if name == "k_maxuv_dt":
+        return 8 * N
+    if name == "k_thom":
+        return 8 * 4 * Nx + 8 * 2 * Nx
+    return 0
+
+
+def hbm_peak():
+    try:
+        d = json.load(open(MEASURED_PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    nse = _load("nse2d_b200", os.path.join(PKG, "nse2d_b200.py"))
+    W = WORKLOAD
+    Nx, Ny = W["Nx"], W["Ny"]
+    y = tanh_y(Ny, W["beta"], W["h"])
+    w0 = initial_vorticity(Nx, Ny, W["Lx"], y, seed=1 + rank)
+    pinned_w0 = torch.from_numpy(w0).pin_memory()
+    stream = torch.cuda.Stream()
+    solver = nse.Solver(**W)
+    solver.set_omega(pinned_w0.numpy(), stream=stream)
+    with torch.cuda.stream(stream):
+        solver.step(args.warmup, use_graph=True, stream=stream)
+    stream.synchronize()
+    # ---- timed region (resident state): K graph replays ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        solver.step(args.steps, use_graph=True, stream=stream)
+        e1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    t_sim, dt_last, nsteps_done, umax = solver.time(stream=stream)
+    bad = solver.nonfinite(stream=stream)
+    # ---- per-kernel timing pass (device events around every kernel of every step) ----
+    per_kernel = solver.step_timed(args.steps, stream=stream)
+    # ---- e2e through the public API with host buffers ----
+    host_w = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
+    host_psi = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
+    solver2 = nse.Solver(**W)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        c0.record(stream)
+        solver2.set_omega(pinned_w0.numpy(), stream=stream)
+        for _ in range(args.steps):
+            solver2.step(1, use_graph=True, stream=stream)
+            solver2.time(stream=stream)          # per-step D2H of t, dt, step, max |u|, |v|
+        solver2.lib.nse2d_get_fields(solver2.h, ctypes.c_void_p(host_w.data_ptr()),
+                                     ctypes.c_void_p(host_psi.data_ptr()), 0, ctypes.c_void_p(stream.cuda_stream))
+        c1.record(stream)
+    stream.synchronize()
+    e2e_ms = max_over_ranks(c0.elapsed_time(c1), world)
+    wall_e2e = time.perf_counter() - t0
+    solver2.close()
+    launches = solver.launches_per_step()
+    solver.close()
+
+    N = Nx * Ny
+    B_step = algorithmic_bytes_per_step(Nx, Ny)
+    peak, peak_kind = hbm_peak()
+    step_ms = ms_max / args.steps
+    # per-kernel table; the dominant kernel carries the roofline object
+    agg = {}
+    stage = 0
+    for name, tot in per_kernel:
+        if name == "k_stage_fft":
+            stage += 1
+        b = kernel_bytes(name, stage, Nx, Ny)
+        a = agg.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0})
+        a["launches"] += args.steps
+        a["ms"] += tot
+        a["bytes"] += b * args.steps
+    total_ms = sum(v["ms"] for v in agg.values())
+    kernels = {}
+    for name, a in agg.items():
+        avg_ms = a["ms"] / a["launches"]
+        gbs = (a["bytes"] / a["launches"]) / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+        kernels[name] = {"launches_per_step": a["launches"] // args.steps, "avg_us": round(avg_ms * 1e3, 2),
+                         "share": round(a["ms"] / total_ms, 4), "achieved_gbs": round(gbs, 1),
+                         "algorithmic_bytes_per_launch": int(a["bytes"] / a["launches"])}
+    dom = max(agg, key=lambda k: agg[k]["ms"])
+    dk = kernels[dom]
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.isfile(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(dom)
+        except Exception:
+            traffic = None
+    step_gbs = B_step / (step_ms * 1e-3) / 1e9
+    h2d = N * 8 / args.steps + 8 * 3
+    d2h = 2 * N * 8 / args.steps + 128
+    line = {
+        "metric": METRIC, "value": round(world * args.steps / (ms_max * 1e-3), 3), "unit": "steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Poiseuille + random vorticity over x-modes 1-64)",
+        "config": {"workload": "channel SSPRK3 step 4096x2049 FP64, tanh beta=2, Re_b=2e4, F0=0.05 n=12, "
+                               "drag 1e-3, adaptive dt CFL 0.5",
+                   "Nx": Nx, "Ny": Ny, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (each field 67 MB, step working set ~0.5 GB)",
+                   "graph": "one CUDA graph per step, replayed"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": dk["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": round(dk["achieved_gbs"] / peak, 4), "traffic": traffic, "peak_kind": peak_kind},
+        "step_roofline": {"algorithmic_bytes_per_step": B_step, "achieved": round(step_gbs, 1), "peak": peak,
+                          "unit": "GB/s", "frac": round(step_gbs / peak, 4), "frac_of_8TBs": round(step_gbs / 8000.0, 4)},
+        "kernels": kernels,
+        "e2e": {"value": round(world * args.steps / (e2e_ms * 1e-3), 3), "unit": "steps/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "wall_s": round(wall_e2e, 3)},
+        "gpu_launches": int(launches * args.steps),
+        "clocks": clocks,
+        "sim": {"t": t_sim, "dt_last": dt_last, "steps_done": nsteps_done, "umax": umax[0], "nonfinite": bad},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, sample_steps=args.cpu_steps)
+    return line
+
+
+def cpu_baseline(args, sample_steps=3, max_seconds=60.0):
+    """The oracle (C++/OpenMP CPU restatement of the reference algorithm) on the same workload."""
+    ora = _load("nse2d_oracle_py", os.path.join(ORACLE, "oracle.py"))
+    W = WORKLOAD
+    L = ora.lib()
+    threads = os.cpu_count() or 1
+    L.or_set_threads(threads)
+    o = ora.OracleSolver(**{k: W[k] for k in W})
+    y = o.metric(0)
+    o.set_omega(initial_vorticity(W["Nx"], W["Ny"], W["Lx"], y, seed=1))
+    t = 0.0
+    dt, _ = o.adapt_dt()
+    o.step(t, dt)                                  # warm-up step
+    t += dt
+    n = 0
+    t0 = time.perf_counter()
+    while n < sample_steps and time.perf_counter() - t0 < max_seconds:
+        dt, _ = o.adapt_dt()
+        o.step(t, dt)
+        t += dt
+        n += 1
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": round(n / el, 4), "unit": "steps/s", "cores": int(L.or_get_threads()), "kind": "port",
+            "sample": f"{n} full SSPRK3 steps of the 4096x2049 workload (adaptive dt) after 1 warm-up step"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    steps = max(1, min(args.steps, args.ref_steps))
+    cb = cpu_baseline(args, sample_steps=steps, max_seconds=args.ref_seconds)
+    return {"metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
+            "warmup": 1, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poiseuille + random vorticity)",
+            "config": {"workload": "channel SSPRK3 step 4096x2049 FP64, tanh beta=2, Re_b=2e4, F0=0.05 n=12, "
+                                   "drag 1e-3, adaptive dt CFL 0.5", "Nx": 4096, "Ny": 2049},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-steps", type=int, default=20)
+    ap.add_argument("--ref-seconds", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                    int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_ours(args, world, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    if args.impl == "ours" and world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

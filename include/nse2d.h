@@ -1,0 +1,160 @@
+/*
+ * nse2d-b200: C ABI of the B200 channel time step (libnse2d_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ * 1. The C-linkage operator launchers of the reference, same names, same argument order
+ *    and meaning, asynchronous on the given stream, all pointers device memory owned by
+ *    the caller (reference: src/test_api.cu:8-92, built there with -DEXPORT_TEST_API).
+ *    Like the reference they return nothing; on a CUDA error they print the error and
+ *    abort the process (src/common.cuh:116-117), unless nse2d_set_abort_on_error(0) was
+ *    called, in which case the error is kept for nse2d_last_error().
+ *
+ * 2. nse2d_* entry points with an int status (0 = success, nonzero = error, message in
+ *    nse2d_last_error()). They drive the whole SSPRK(3,3) time step of the reference's
+ *    time loop (src/main.cu:434-541) on a solver context that owns its fields and
+ *    workspace; they replace the reference's C++ driver-side calls (Poisson2D_Z2Z in
+ *    src/poisson.cuh:18-119, the launch_* functions of src/ops.cuh and src/diag.cuh).
+ *
+ * Arrays are row-major [Ny][Nx] FP64 (x fastest), metrics [Ny] / [Ny-1], as in the
+ * reference (src/common.cuh:127-130).
+ */
+#ifndef NSE2D_B200_H
+#define NSE2D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* cudaStream_t;
+
+/* ---------------------------------------------------------------------------------------
+ * 1. Reference test API (src/test_api.cu)
+ * ------------------------------------------------------------------------------------- */
+/* u = a psi_eta / (2 deta), v = -psi_x / (2 dx), clamped at the walls. test_api.cu:8-18 */
+void testapi_uv_from_psi_mapped(const double* d_psi, double* d_u, double* d_v, int Nx, int Ny,
+                                double inv_dx, double inv_deta, const double* d_a_node,
+                                cudaStream_t s);
+/* omega = -(dxx psi + mapped dyy psi) on interior rows. test_api.cu:20-30 */
+void testapi_omega_from_psi_interior_mapped(double* d_w, const double* d_psi, int Nx, int Ny,
+                                            double inv_dx2, double inv_deta2,
+                                            const double* d_a_node, const double* d_a_edge,
+                                            cudaStream_t s);
+/* Thom wall vorticity (no-slip; zero with nse2d_testapi_set_free_slip(1)). test_api.cu:32-42 */
+void testapi_thom_wall_vorticity_mapped(double* d_w, const double* d_psi, int Nx, int Ny,
+                                        const double* d_dy_edge, double psi_bot, double psi_top,
+                                        cudaStream_t s);
+/* mapped Arakawa Jacobian u.grad(omega) = -(J1+J2+J3)/3, walls 0. test_api.cu:44-53 */
+void testapi_arakawa_J_mapped(const double* d_psi, const double* d_w, double* d_J, int Nx, int Ny,
+                              double inv_dx, double inv_deta, const double* d_a_node,
+                              cudaStream_t s);
+/* advective reference u omega_x + v omega_y from (u, v). test_api.cu:55-65 */
+void testapi_compute_adv_from_uv_mapped(const double* d_u, const double* d_v, const double* d_omg,
+                                        double* d_Jref, int Nx, int Ny, double inv_dx,
+                                        double inv_deta, const double* d_a_node, cudaStream_t s);
+/* conservative flux form. test_api.cu:67-77 */
+void testapi_compute_adv_flux_mapped(const double* d_u, const double* d_v, const double* d_omg,
+                                     double* d_Jref, int Nx, int Ny, double inv_dx,
+                                     double inv_deta, const double* d_a_node, cudaStream_t s);
+/* J1, J2, J3 and Jadv separately; any output may be NULL. test_api.cu:79-92 */
+void testapi_arakawa_J_mapped_split(const double* d_psi, const double* d_omg, double* d_J1,
+                                    double* d_J2, double* d_J3, double* d_Jadv, int Nx, int Ny,
+                                    double inv_dx, double inv_deta, const double* d_a_node,
+                                    cudaStream_t s);
+
+/* Behaviour switches of group 1 (no counterpart in the reference, which fixes both at
+ * compile time: CUDA_CHECK aborts, FREE_SLIP_WALLS selects the wall closure). */
+void nse2d_set_abort_on_error(int on);
+void nse2d_testapi_set_free_slip(int on);
+
+/* ---------------------------------------------------------------------------------------
+ * 2. Solver context API
+ * ------------------------------------------------------------------------------------- */
+/* The reference's Grid + Params fields used by the time step (src/common.cuh:42-114),
+ * with the reference defaults from nse2d_config_default(). */
+typedef struct nse2d_config {
+    int    Nx, Ny;            /* Nx a power of two >= 4; Ny >= 5 */
+    double Lx, h;
+    int    stretch;           /* 0 = none (uniform), 1 = tanh (src/grid.cu:33-45) */
+    double beta;
+    double Ub, Reb, nu_override;   /* nu = nu_override if >= 0, else 2 h Ub / Reb */
+    double dt_init, dt_max, cfl, cvisc;
+    int    adapt;             /* adaptive dt (src/main.cu:439-464) */
+    double t_end, F0;
+    int    nforce;
+    double lin_drag;
+    int    free_slip;         /* free-slip walls (omega_wall = 0) instead of Thom */
+    int    mms;
+    double mms_A0, mms_eps, mms_Om;
+    int    mms_kx;
+    int    closure_diag;      /* accumulate the wall-update enstrophy (Jwall columns) */
+    int    precision;         /* 64 */
+} nse2d_config;
+
+typedef struct nse2d_ctx nse2d_ctx;
+
+void nse2d_config_default(nse2d_config* cfg);
+int  nse2d_create(const nse2d_config* cfg, nse2d_ctx** out);
+int  nse2d_destroy(nse2d_ctx* ctx);
+
+/* Set omega (where = 0: host array, 1: device array), then the initial Poisson solve and
+ * Thom closure; t = 0, dt = dt_init (src/main.cu:197-215). Synchronous. */
+int  nse2d_set_omega(nse2d_ctx* ctx, const double* w, int where, cudaStream_t s);
+/* Set omega and psi as they are (resume), and the time t. Synchronous. */
+int  nse2d_set_state(nse2d_ctx* ctx, const double* w, const double* psi, int where, double t,
+                     cudaStream_t s);
+/* Copy omega and/or psi out (either may be NULL). where = 0: host (synchronous), 1: device. */
+int  nse2d_get_fields(nse2d_ctx* ctx, double* w, double* psi, int where, cudaStream_t s);
+/* Device pointer of a context field: 0 omega, 1 psi, 2 omega1, 3 omega2, 4 rhs, 5 J. */
+int  nse2d_field_ptr(nse2d_ctx* ctx, int which, double** d_ptr);
+
+/* Advance nsteps SSPRK(3,3) steps, asynchronously. With adapt, dt is computed on the
+ * device before every step (max |u|, |v|, |v| a, CFL and viscous limits, trimming to
+ * the next output time); otherwise the dt of nse2d_set_dt / dt_init is used. use_graph:
+ * replay one captured CUDA graph per step. */
+int  nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s);
+/* As nse2d_step without a graph, and the last step also stores its stage-3 rhs in the
+ * context (field 4), which the next nse2d_diagnostics(t0_row = 0) pairs with omega for the
+ * dOmega_rhs column (src/main.cu:586). */
+int  nse2d_step_store_rhs(nse2d_ctx* ctx, int nsteps, cudaStream_t s);
+/* As nse2d_step without a graph, with CUDA events on s around every kernel; kernel_ms[k]
+ * receives the summed duration of the k-th kernel of a step over the nsteps steps
+ * (nse2d_launches_per_step entries). Synchronous. */
+int  nse2d_step_timed(nse2d_ctx* ctx, int nsteps, double* kernel_ms, cudaStream_t s);
+/* Name of the k-th kernel of a step. */
+const char* nse2d_step_kernel_name(nse2d_ctx* ctx, int k);
+/* Number of kernels one step launches. */
+int  nse2d_launches_per_step(nse2d_ctx* ctx);
+int  nse2d_set_dt(nse2d_ctx* ctx, double dt, cudaStream_t s);
+/* Output times used for dt trimming and the snap after a step (1e300 = none). */
+int  nse2d_set_schedule(nse2d_ctx* ctx, double next_snap, double next_diag, cudaStream_t s);
+/* Read t, dt, step count and the last max |u|, |v|, |v| a (any may be NULL). Synchronous. */
+int  nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, double* umax3,
+                    cudaStream_t s);
+
+/* Poisson solve of the reference (src/poisson.cuh:83-118): psi from omega, Dirichlet
+ * psi = 0 / 2 h Ub at the walls on kx = 0. Device pointers, asynchronous. */
+int  nse2d_poisson_solve(nse2d_ctx* ctx, const double* d_w, double* d_psi, cudaStream_t s);
+/* max |u|, |v|, |v| a of the context's psi (src/diag.cu:821-866). Synchronous. */
+int  nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s);
+/* One diagnostics.csv row at the current state, columns umax .. Re_tau (16) followed by
+ * the 13 closure_diag columns (nan when not computed), as src/main.cu:566-692
+ * (t0_row = 0) or the t = 0 row of src/main.cu:325-421 (t0_row = 1). Synchronous. */
+int  nse2d_diagnostics(nse2d_ctx* ctx, int t0_row, double* out29, cudaStream_t s);
+/* J and rhs at the context's state and time t into fields 5 and 4. Synchronous. */
+int  nse2d_rhs_at_state(nse2d_ctx* ctx, double t, cudaStream_t s);
+/* u, v of the context's psi into caller device arrays (src/ops.cu:47-70). */
+int  nse2d_uv(nse2d_ctx* ctx, double* d_u, double* d_v, cudaStream_t s);
+/* 1 when a max reduction met a NaN or Inf since the context was created. Synchronous. */
+int  nse2d_nonfinite(nse2d_ctx* ctx, int* flag, cudaStream_t s);
+/* Host copy of a metric: 0 y, 1 a_node, 2 a_edge (Ny-1), 3 dy_edge (Ny-1), 4 w_node. */
+int  nse2d_metrics(nse2d_ctx* ctx, int which, double* out);
+/* Scalars: 0 nu, 1 dx, 2 deta, 3 invA_full, 4 meanFx_A, 5 psi_bot, 6 psi_top. */
+int  nse2d_scalar(nse2d_ctx* ctx, int which, double* out);
+
+const char* nse2d_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NSE2D_B200_H */

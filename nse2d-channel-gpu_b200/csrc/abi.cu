@@ -1,0 +1,229 @@
+// C ABI of the solver context (include/nse2d.h, group 2). Written for this project.
+#include <cstring>
+#include <vector>
+
+#include "nse2d_internal.h"
+#include "../../include/nse2d.h"
+
+using namespace nse2d;
+
+struct nse2d_ctx {
+    Context* c;
+};
+
+static Config to_config(const nse2d_config* a) {
+    Config c;
+    c.Nx = a->Nx; c.Ny = a->Ny; c.Lx = a->Lx; c.h = a->h; c.stretch = a->stretch; c.beta = a->beta;
+    c.Ub = a->Ub; c.Reb = a->Reb; c.nu_override = a->nu_override; c.dt_init = a->dt_init; c.dt_max = a->dt_max;
+    c.cfl = a->cfl; c.cvisc = a->cvisc; c.adapt = a->adapt; c.t_end = a->t_end; c.F0 = a->F0;
+    c.nforce = a->nforce; c.lin_drag = a->lin_drag; c.free_slip = a->free_slip; c.mms = a->mms;
+    c.mms_A0 = a->mms_A0; c.mms_eps = a->mms_eps; c.mms_Om = a->mms_Om; c.mms_kx = a->mms_kx;
+    c.closure_diag = a->closure_diag; c.precision = a->precision;
+    return c;
+}
+
+#define CHECK_CTX(ctx)                                    \
+    do {                                                  \
+        if (!(ctx) || !(ctx)->c) {                        \
+            set_error("%s: null context", __func__);      \
+            return -1;                                    \
+        }                                                 \
+    } while (0)
+
+extern "C" {
+
+void nse2d_config_default(nse2d_config* a) {
+    const Config d;   // the reference defaults, src/common.cuh:42-114
+    a->Nx = d.Nx; a->Ny = d.Ny; a->Lx = d.Lx; a->h = d.h; a->stretch = d.stretch; a->beta = d.beta;
+    a->Ub = d.Ub; a->Reb = d.Reb; a->nu_override = d.nu_override; a->dt_init = d.dt_init; a->dt_max = d.dt_max;
+    a->cfl = d.cfl; a->cvisc = d.cvisc; a->adapt = d.adapt; a->t_end = d.t_end; a->F0 = d.F0;
+    a->nforce = d.nforce; a->lin_drag = d.lin_drag; a->free_slip = d.free_slip; a->mms = d.mms;
+    a->mms_A0 = d.mms_A0; a->mms_eps = d.mms_eps; a->mms_Om = d.mms_Om; a->mms_kx = d.mms_kx;
+    a->closure_diag = d.closure_diag; a->precision = d.precision;
+}
+
+int nse2d_create(const nse2d_config* cfg, nse2d_ctx** out) {
+    if (!cfg || !out) { set_error("nse2d_create: null argument"); return -1; }
+    *out = nullptr;
+    Context* c = nullptr;
+    if (context_create(to_config(cfg), &c) != 0) return -1;
+    *out = new nse2d_ctx{c};
+    return 0;
+}
+
+int nse2d_destroy(nse2d_ctx* ctx) {
+    if (!ctx) return 0;
+    context_destroy(ctx->c);
+    delete ctx;
+    return 0;
+}
+
+int nse2d_set_omega(nse2d_ctx* ctx, const double* w, int where, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->w, w, c->N * sizeof(double), where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    return set_initial_omega(c, s);
+}
+
+int nse2d_set_state(nse2d_ctx* ctx, const double* w, const double* psi, int where, double t, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->w, w, c->N * sizeof(double), k, s));
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->psi, psi, c->N * sizeof(double), k, s));
+    Ctl h{};
+    h.t = t; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_get_fields(nse2d_ctx* ctx, double* w, double* psi, int where, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (w) NSE_CUDA_TRY(cudaMemcpyAsync(w, c->w, c->N * sizeof(double), k, s));
+    if (psi) NSE_CUDA_TRY(cudaMemcpyAsync(psi, c->psi, c->N * sizeof(double), k, s));
+    if (!where) NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_field_ptr(nse2d_ctx* ctx, int which, double** d_ptr) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    double* f[6] = {c->w, c->psi, c->w1, c->w2, c->rhs, c->J};
+    if (which < 0 || which > 5 || !d_ptr) { set_error("nse2d_field_ptr: bad field %d", which); return -1; }
+    *d_ptr = f[which];
+    return 0;
+}
+
+int nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return run_steps(ctx->c, nsteps, use_graph != 0, s, false);
+}
+
+int nse2d_step_store_rhs(nse2d_ctx* ctx, int nsteps, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return run_steps(ctx->c, nsteps, false, s, true);
+}
+
+int nse2d_step_timed(nse2d_ctx* ctx, int nsteps, double* kernel_ms, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const int nk = launches_per_step(c);
+    std::vector<cudaEvent_t> ev((size_t)nsteps * (nk + 1));
+    for (auto& e : ev) NSE_CUDA_TRY(cudaEventCreate(&e));
+    int rc = 0;
+    for (int i = 0; i < nsteps && rc == 0; ++i) rc = enqueue_step_timed(c, s, &ev[(size_t)i * (nk + 1)]);
+    if (rc == 0) {
+        NSE_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int k = 0; k < nk; ++k) kernel_ms[k] = 0.0;
+        for (int i = 0; i < nsteps; ++i)
+            for (int k = 0; k < nk; ++k) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[(size_t)i * (nk + 1) + k], ev[(size_t)i * (nk + 1) + k + 1]);
+                kernel_ms[k] += ms;
+            }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+const char* nse2d_step_kernel_name(nse2d_ctx* ctx, int k) {
+    if (!ctx || !ctx->c) return "";
+    return step_kernel_name(ctx->c, k);
+}
+
+int nse2d_launches_per_step(nse2d_ctx* ctx) {
+    CHECK_CTX(ctx);
+    return launches_per_step(ctx->c);
+}
+
+int nse2d_set_dt(nse2d_ctx* ctx, double dt, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    NSE_CUDA_TRY(cudaMemcpyAsync(&ctx->c->ctl->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_set_schedule(nse2d_ctx* ctx, double next_snap, double next_diag, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    double v[3] = {std::min(next_snap, next_diag), next_snap, next_diag};
+    NSE_CUDA_TRY(cudaMemcpyAsync(&c->ctl->next_out, v, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, double* umax3, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->h_ctl, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    if (t) *t = c->h_ctl->t;
+    if (dt) *dt = c->h_ctl->dt;
+    if (step) *step = c->h_ctl->step;
+    if (umax3) { umax3[0] = c->h_ctl->umax; umax3[1] = c->h_ctl->vmax; umax3[2] = c->h_ctl->vmaxm; }
+    return 0;
+}
+
+int nse2d_nonfinite(nse2d_ctx* ctx, int* flag, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->h_ctl, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    *flag = c->h_ctl->nonfinite;
+    return 0;
+}
+
+int nse2d_poisson_solve(nse2d_ctx* ctx, const double* d_w, double* d_psi, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return poisson_solve(ctx->c, d_w, d_psi, s);
+}
+
+int nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    if (launch_maxuv(c, c->psi, false, s)) return -1;
+    return nse2d_get_time(ctx, nullptr, nullptr, nullptr, out3, s);
+}
+
+int nse2d_diagnostics(nse2d_ctx* ctx, int t0_row, double* out29, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return diagnostics_row(ctx->c, t0_row, out29, s);
+}
+
+int nse2d_rhs_at_state(nse2d_ctx* ctx, double t, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    if (rhs_at_state(c, c->w, c->psi, c->J, c->rhs, t, s)) return -1;
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_uv(nse2d_ctx* ctx, double* d_u, double* d_v, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return uv_from_psi(ctx->c, ctx->c->psi, d_u, d_v, s);
+}
+
+int nse2d_metrics(nse2d_ctx* ctx, int which, double* out) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const std::vector<double>* v[5] = {&c->h_y, &c->h_a_node, &c->h_a_edge, &c->h_dy_edge, &c->h_w_node};
+    if (which < 0 || which > 4 || !out) { set_error("nse2d_metrics: bad metric %d", which); return -1; }
+    std::memcpy(out, v[which]->data(), v[which]->size() * sizeof(double));
+    return 0;
+}
+
+int nse2d_scalar(nse2d_ctx* ctx, int which, double* out) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const double v[7] = {c->nu, c->dx, c->deta, c->invA_full, c->meanFx_A, c->psi_bot, c->psi_top};
+    if (which < 0 || which > 6 || !out) { set_error("nse2d_scalar: bad index %d", which); return -1; }
+    *out = v[which];
+    return 0;
+}
+
+const char* nse2d_last_error(void) { return get_error(); }
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// Common types of the B200 channel time step: the solver context, its device control
+// block and error handling. Written for this project.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "fft.cuh"
+
+namespace nse2d {
+
+// ---- error handling: every entry point returns a status; the message is kept per thread ----
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+#define NSE_CUDA_TRY(expr)                                                                       \
+    do {                                                                                         \
+        cudaError_t e__ = (expr);                                                                \
+        if (e__ != cudaSuccess) {                                                                \
+            ::nse2d::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e__)); \
+            return -1;                                                                           \
+        }                                                                                        \
+    } while (0)
+
+// ---- run configuration (the reference's Grid + Params, src/common.cuh:42-114) ----
+struct Config {
+    int Nx = 1024, Ny = 1025;
+    double Lx = 12.566370612, h = 1.0;
+    int stretch = 0;         // 0 none, 1 tanh
+    double beta = 0.0;
+    double Ub = 1.0, Reb = 10000.0, nu_override = -1.0;
+    double dt_init = 1e-3, dt_max = 1e-2, cfl = 0.5, cvisc = 0.5;
+    int adapt = 1;
+    double t_end = 200.0, F0 = 0.0;
+    int nforce = 1;
+    double lin_drag = 0.0;
+    int free_slip = 0, mms = 0;
+    double mms_A0 = 1e-3, mms_eps = 0.1, mms_Om = 1.0;
+    int mms_kx = 1, closure_diag = 0;
+    int precision = 64;      // 64: FP64 throughout; 32: FP32 bulk with FP64 islands
+};
+
+// Device control block: time, step size and the step's reductions. Kept on the device so
+// that a sequence of steps (with adaptive dt) needs no host round trip and can be captured
+// in a CUDA graph.
+struct Ctl {
+    double t, dt;
+    double umax, vmax, vmaxm;      // max |u|, |v|, |v| a of the last reduction
+    double next_out;               // next output time for dt trimming (1e300: none)
+    double next_snap, next_diag;   // scheduled output times for the snap after a step (1e300: none)
+    double jwall[3];               // closure_diag: enstrophy added by the wall update, per stage
+    long long step;
+    unsigned int blocks_done;      // last-block-done counter of the max reduction
+    int nonfinite;                 // set when a reduction saw NaN/Inf
+};
+
+// Row-constant tables (device), length Ny unless noted.
+struct RowTables {
+    double* y;          // node coordinates
+    double* a_node;     // eta_y at nodes
+    double* a_edge;     // eta_y at j+1/2 (Ny-1)
+    double* dy_edge;    // y_{j+1}-y_j (Ny-1)
+    double* w_node;     // trapezoid weights
+    double* wt_node;    // deta / a_node on interior rows, 0 at walls
+    double* frow;       // vorticity forcing f(y_j)
+    double* asub;       // Thomas sub-diagonal a_j a_{j-1/2} / deta^2
+    double* csup;       // Thomas super-diagonal a_j a_{j+1/2} / deta^2
+    double* inv_csup;   // 1 / csup
+    // MMS tables (only when mms): per row g, g'', sin(2 theta); per column sin(kx), sin(2kx)
+    double* mms_g;
+    double* mms_gpp;
+    double* mms_sin2;
+    double* mms_sk;
+    double* mms_s2k;
+};
+
+struct Context {
+    Config cfg;
+    int Nx = 0, Ny = 0, M = 0, H = 0, Hp = 0, Ni = 0;
+    size_t N = 0;
+    double dx = 0, dy = 0, inv_dx = 0, inv_dx2 = 0, deta = 0, inv_deta = 0, inv_deta2 = 0;
+    double nu = 0, dy_min = 0, inv_dymin2 = 0, Ly_full = 0, invA_full = 0, meanFx_A = 0;
+    double psi_bot = 0, psi_top = 0;
+    // host copies of the metrics
+    std::vector<double> h_y, h_a_node, h_a_edge, h_dy_edge, h_w_node;
+    RowTables rt{};
+    // fields (FP64 state), owned by the context
+    double *w = nullptr, *w1 = nullptr, *w2 = nullptr, *psi = nullptr;
+    // scratch used by diagnostics: rhs and J at one state, and the stage-3 rhs of the last step
+    double *rhs = nullptr, *J = nullptr;
+    // spectral buffer [Ny][Hp] complex, FP64 (in place: omega-hat in, psi-hat out)
+    cpx<double>* hat = nullptr;
+    double* cp = nullptr;          // elimination table [Ni][Hp]
+    cpx<double>* tw = nullptr;     // M twiddles e^{-2 pi i t/M}
+    cpx<double>* wN = nullptr;     // M+1 twiddles e^{-2 pi i k/Nx}
+    // reductions
+    double* red_blocks = nullptr;  // per-block partials (max and diagnostics)
+    double* red_out = nullptr;     // reduced values
+    int red_nblocks = 0;
+    size_t red_capacity = 0;       // doubles in red_blocks
+    Ctl* ctl = nullptr;            // device control block
+    Ctl* h_ctl = nullptr;          // pinned host mirror
+    // launch shapes
+    int fft_threads = 256;
+    int stage_grid = 0, ifft_grid = 0;
+    int thomas_C = 1, thomas_R = 0, thomas_groups = 0;
+    size_t thomas_smem = 0;
+    int num_sms = 0;
+    cudaStream_t cap_stream = nullptr;     // private stream used only for graph capture
+    cudaGraphExec_t graph_exec = nullptr;  // one captured step
+    bool closure_diag = false;
+};
+
+}  // namespace nse2d

@@ -1,0 +1,26 @@
+// Internal interface between the C-ABI layer and the solver implementation.
+#pragma once
+#include "common.cuh"
+
+namespace nse2d {
+int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>& a_node,
+                    std::vector<double>& a_edge, std::vector<double>& dy_edge, std::vector<double>& w_node);
+int context_create(const Config& cfg, Context** out);
+void context_destroy(Context* c);
+int launch_rows_fft(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
+                    double* rhs_out = nullptr);
+int launch_thomas(Context* c, cudaStream_t s);
+int launch_ifft(Context* c, double* psi, cudaStream_t s);
+int launch_thom(Context* c, double* w, const double* psi, int stage, bool closure, cudaStream_t s);
+int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s);
+int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s);
+int enqueue_step(Context* c, cudaStream_t s, bool store_rhs);
+int launches_per_step(const Context* c);
+int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev);
+const char* step_kernel_name(const Context* c, int k);
+int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs);
+int set_initial_omega(Context* c, cudaStream_t s);
+int diagnostics_row(Context* c, int t0_row, double* out29, cudaStream_t s);
+int rhs_at_state(Context* c, const double* w, const double* psi, double* J, double* rhs, double tm, cudaStream_t s);
+int uv_from_psi(Context* c, const double* psi, double* u, double* v, cudaStream_t s);
+}  // namespace nse2d

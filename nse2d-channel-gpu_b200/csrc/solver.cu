@@ -1,0 +1,475 @@
+// Solver context: grid metrics, tables, device buffers and the enqueueing of one
+// SSPRK(3,3) step. Written for this project; the setup follows the reference's
+// src/grid.cu:7-94 (metrics), src/main.cu:49-87 (derived constants), src/poisson.cu:16-68
+// (kx^2 and the elimination table) and src/main.cu:210-213 (initial solve + Thom).
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+
+#include "nse2d_internal.h"
+#include "step_kernels.cuh"
+
+namespace nse2d {
+
+static thread_local char g_err[1024] = "";
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+const char* get_error() { return g_err; }
+
+// ---- grid metrics on the host: src/grid.cu:7-94 ----
+int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>& a_node,
+                    std::vector<double>& a_edge, std::vector<double>& dy_edge, std::vector<double>& w_node) {
+    const int Ny = c.Ny;
+    const double h = c.h;
+    y.assign(Ny, 0.0); a_node.assign(Ny, 0.0); a_edge.assign(Ny - 1, 0.0);
+    dy_edge.assign(Ny - 1, 0.0); w_node.assign(Ny, 0.0);
+    if (Ny <= 2 || c.stretch == 0) {
+        const double dy = (2.0 * h) / (double)(Ny - 1);
+        for (int j = 0; j < Ny; ++j) y[j] = -h + j * dy;
+        const double deta = 2.0 / (double)(Ny - 1);
+        const double y_eta = dy / deta;
+        const double a = 1.0 / y_eta;
+        for (int j = 0; j < Ny; ++j) a_node[j] = a;
+        for (int j = 0; j < Ny - 1; ++j) { a_edge[j] = a; dy_edge[j] = dy; }
+        for (int j = 0; j < Ny; ++j) w_node[j] = dy;
+        w_node[0] *= 0.5; w_node[Ny - 1] *= 0.5;
+        return 0;
+    }
+    if (c.stretch != 1) { set_error("unknown stretch code %d (0 none, 1 tanh)", c.stretch); return -1; }
+    const double b = (c.beta > 0 ? c.beta : 2.5);
+    for (int j = 0; j < Ny; ++j) {
+        const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
+        y[j] = h * std::tanh(b * e) / std::tanh(b);
+    }
+    for (int j = 0; j < Ny; ++j) {
+        const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
+        const double sech = 1.0 / std::cosh(b * e);
+        a_node[j] = 1.0 / (h * b * (sech * sech) / std::tanh(b));
+    }
+    for (int j = 0; j < Ny - 1; ++j) a_edge[j] = 0.5 * (a_node[j] + a_node[j + 1]);
+    for (int j = 0; j < Ny - 1; ++j) dy_edge[j] = y[j + 1] - y[j];
+    w_node[0] = 0.5 * dy_edge[0];
+    w_node[Ny - 1] = 0.5 * dy_edge[Ny - 2];
+    for (int j = 1; j < Ny - 1; ++j) w_node[j] = 0.5 * (dy_edge[j - 1] + dy_edge[j]);
+    return 0;
+}
+
+// ---- device setup kernels ----
+// Elimination table, one thread per kx: src/poisson.cu:16-22 (kx^2) and :38-68 (cp), the
+// same expressions; stored [Ni][Hp] so that a warp reads consecutive kx.
+__global__ void k_setup_cp(double* cp, const double* a_node, const double* a_edge, int Nx, int Ny,
+                           int Hp, int H, double Lx, double inv_deta2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= H) return;
+    const int Ni = Ny - 2;
+    const int kphys_i = (k <= Nx / 2 ? k : k - Nx);
+    const double kphys = (2.0 * kPiD * (double)kphys_i) / Lx;
+    const double kx2 = kphys * kphys;
+    int j = 1;
+    double an = a_node[j], ae_p = a_edge[j], ae_m = a_edge[j - 1];
+    double a_sub = an * ae_m * inv_deta2, c_sup = an * ae_p * inv_deta2;
+    double b = -(a_sub + c_sup) - kx2;
+    double cp_prev = c_sup / b;
+    cp[k] = cp_prev;
+    for (int r = 1; r < Ni; ++r) {
+        j = r + 1;
+        an = a_node[j]; ae_p = a_edge[j]; ae_m = a_edge[j - 1];
+        a_sub = an * ae_m * inv_deta2; c_sup = an * ae_p * inv_deta2;
+        b = -(a_sub + c_sup) - kx2;
+        const double den = b - a_sub * cp_prev;
+        const double cpi = c_sup / den;
+        cp[(size_t)r * Hp + k] = cpi;
+        cp_prev = cpi;
+    }
+}
+
+// Row tables: Thomas coefficients (poisson.cu:86-88), forcing f(y) (ops.cu:526-531), trapezoid
+// weights wt (main.cu:252-254) and the MMS row factors (ops.cu:587-603).
+__global__ void k_setup_rows(RowTables rt, int Ny, double inv_deta2, double deta, double F0, int nforce,
+                             double h, double mms_k, double mms_c) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Ny) return;
+    if (j >= 1 && j <= Ny - 2) {
+        const double an = rt.a_node[j];
+        rt.asub[j] = an * rt.a_edge[j - 1] * inv_deta2;
+        rt.csup[j] = an * rt.a_edge[j] * inv_deta2;
+        rt.inv_csup[j] = 1.0 / rt.csup[j];
+        rt.wt_node[j] = deta / an;
+    } else {
+        rt.asub[j] = 0.0; rt.csup[j] = 0.0; rt.inv_csup[j] = 0.0; rt.wt_node[j] = 0.0;
+    }
+    double f = 0.0;
+    if (F0 != 0.0) {
+        const double yy = rt.y[j];
+        const double arg = (double)nforce * kPiD * ((yy + h) / (2.0 * h));
+        f = -F0 * ((double)nforce * kPiD / (2.0 * h)) * cos(arg);
+    }
+    rt.frow[j] = f;
+    if (rt.mms_g) {
+        const double theta = mms_c * (rt.y[j] + h);
+        const double two_th = 2.0 * theta;
+        const double s_th = sin(theta);
+        const double s = s_th * s_th;
+        const double cos2 = cos(two_th), sin2 = sin(two_th);
+        const double c2 = mms_c * mms_c;
+        rt.mms_g[j] = (mms_k * mms_k) * s - 2.0 * c2 * cos2;
+        rt.mms_gpp[j] = 2.0 * c2 * cos2 * ((mms_k * mms_k) + 4.0 * c2);
+        rt.mms_sin2[j] = sin2;
+    }
+}
+
+__global__ void k_setup_mms_cols(double* sk, double* s2k, int Nx, double dx, double k) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nx) return;
+    const double x = (double)i * dx;
+    sk[i] = sin(k * x);
+    s2k[i] = sin(2.0 * k * x);
+}
+
+static void twiddles(int M, std::vector<cpx<double>>& tw, std::vector<cpx<double>>& wN) {
+    const long double PI = 3.141592653589793238462643383279502884L;
+    tw.resize(M);
+    wN.resize(M + 1);
+    for (int t = 0; t < M; ++t) {
+        const long double a = -2.0L * PI * (long double)t / (long double)M;
+        tw[t] = {(double)cosl(a), (double)sinl(a)};
+    }
+    for (int k = 0; k <= M; ++k) {
+        const long double a = -PI * (long double)k / (long double)M;
+        wN[k] = {(double)cosl(a), (double)sinl(a)};
+    }
+    tw[0] = {1.0, 0.0};
+    if (M % 4 == 0) { tw[M / 4] = {0.0, -1.0}; tw[M / 2] = {-1.0, 0.0}; tw[3 * M / 4] = {0.0, 1.0}; }
+    wN[0] = {1.0, 0.0};
+    wN[M] = {-1.0, 0.0};
+    if (M % 2 == 0) wN[M / 2] = {0.0, -1.0};
+}
+
+template <typename T> static int dalloc(T** p, size_t n) {
+    NSE_CUDA_TRY(cudaMalloc((void**)p, n * sizeof(T) + 16));
+    NSE_CUDA_TRY(cudaMemset(*p, 0, n * sizeof(T) + 16));
+    return 0;
+}
+
+static size_t fft_smem(int M) { return 2 * (size_t)padded_size(M) * sizeof(cpx<double>); }
+
+int context_create(const Config& cfg, Context** out) {
+    *out = nullptr;
+    if (cfg.Nx < 4 || (cfg.Nx & (cfg.Nx - 1)) != 0) {
+        set_error("Nx = %d: the B200 path needs a power of two >= 4", cfg.Nx);
+        return -1;
+    }
+    if (cfg.Ny < 5) { set_error("Ny = %d: need Ny >= 5", cfg.Ny); return -1; }
+    if (cfg.Nx > 16384) { set_error("Nx = %d exceeds 16384", cfg.Nx); return -1; }
+    if (cfg.precision != 64) { set_error("precision %d not built (64 only)", cfg.precision); return -1; }
+    auto* c = new Context();
+    c->cfg = cfg;
+    c->Nx = cfg.Nx; c->Ny = cfg.Ny; c->N = (size_t)cfg.Nx * cfg.Ny;
+    c->M = cfg.Nx / 2; c->H = c->M + 1; c->Hp = (c->H + 15) / 16 * 16; c->Ni = cfg.Ny - 2;
+    if (build_y_metrics(cfg, c->h_y, c->h_a_node, c->h_a_edge, c->h_dy_edge, c->h_w_node) != 0) { delete c; return -1; }
+    const int Ny = c->Ny;
+    c->nu = (cfg.nu_override >= 0 ? cfg.nu_override : (2.0 * cfg.h * cfg.Ub) / cfg.Reb);
+    c->dx = cfg.Lx / (double)c->Nx;
+    c->dy = (2.0 * cfg.h) / (double)(Ny - 1);
+    c->inv_dx = 1.0 / c->dx; c->inv_dx2 = c->inv_dx * c->inv_dx;
+    c->deta = 2.0 / (double)(Ny - 1);
+    c->inv_deta = 1.0 / c->deta; c->inv_deta2 = c->inv_deta * c->inv_deta;
+    c->dy_min = std::fabs(c->h_dy_edge[0]);
+    for (int j = 1; j < Ny - 1; ++j) c->dy_min = std::min(c->dy_min, std::fabs(c->h_dy_edge[j]));
+    c->inv_dymin2 = 1.0 / (c->dy_min * c->dy_min);
+    c->Ly_full = 0.0;
+    for (int j = 0; j < Ny; ++j) c->Ly_full += c->h_w_node[j];
+    c->invA_full = 1.0 / ((double)c->Nx * c->Ly_full);
+    c->meanFx_A = 0.0;
+    if (cfg.F0 != 0.0) {
+        for (int j = 0; j < Ny; ++j) {
+            const double arg = (double)cfg.nforce * kPiD * ((c->h_y[j] + cfg.h) / (2.0 * cfg.h));
+            c->meanFx_A += cfg.F0 * std::sin(arg) * c->h_w_node[j];
+        }
+        c->meanFx_A /= c->Ly_full;
+    }
+    c->psi_bot = 0.0; c->psi_top = 2.0 * cfg.h * cfg.Ub;
+    c->closure_diag = cfg.closure_diag != 0;
+
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (c->num_sms <= 0) c->num_sms = 148;
+
+    // Thomas launch shape: clusters of C CTAs (C <= 8) splitting Ni rows, R rows per CTA
+    c->thomas_C = std::min(8, std::max(1, (c->Ni + 255) / 256));
+    c->thomas_R = (c->Ni + c->thomas_C - 1) / c->thomas_C;
+    c->thomas_groups = (c->H + 15) / 16;
+    c->thomas_smem = ((size_t)c->thomas_R * 48 + 2 * KT_NW * 32 + 128) * sizeof(double);
+    if (c->thomas_smem > 220 * 1024) {
+        set_error("Ny = %d too large for the cluster Thomas solve (R = %d rows per CTA)", Ny, c->thomas_R);
+        delete c;
+        return -1;
+    }
+    auto fail = [&]() { context_destroy(c); return -1; };
+    RowTables& rt = c->rt;
+    if (dalloc(&rt.y, Ny) || dalloc(&rt.a_node, Ny) || dalloc(&rt.a_edge, Ny) || dalloc(&rt.dy_edge, Ny) ||
+        dalloc(&rt.w_node, Ny) || dalloc(&rt.wt_node, Ny) || dalloc(&rt.frow, Ny) || dalloc(&rt.asub, Ny) ||
+        dalloc(&rt.csup, Ny) || dalloc(&rt.inv_csup, Ny))
+        return fail();
+    if (cfg.mms) {
+        if (dalloc(&rt.mms_g, Ny) || dalloc(&rt.mms_gpp, Ny) || dalloc(&rt.mms_sin2, Ny) ||
+            dalloc(&rt.mms_sk, c->Nx) || dalloc(&rt.mms_s2k, c->Nx))
+            return fail();
+    }
+    if (dalloc(&c->w, c->N) || dalloc(&c->w1, c->N) || dalloc(&c->w2, c->N) || dalloc(&c->psi, c->N) ||
+        dalloc(&c->rhs, c->N) || dalloc(&c->J, c->N))
+        return fail();
+    if (dalloc(&c->hat, (size_t)Ny * c->Hp) || dalloc(&c->cp, (size_t)c->Ni * c->Hp) ||
+        dalloc(&c->tw, (size_t)c->M) || dalloc(&c->wN, (size_t)c->M + 1))
+        return fail();
+    // one buffer for the block partials of the max reduction (3 per block) and the per-row
+    // partials of the diagnostics (32 per row); never reallocated (graphs keep its address)
+    c->red_nblocks = 2 * c->num_sms;
+    c->red_capacity = std::max((size_t)c->red_nblocks * 3, (size_t)Ny * 32);
+    if (dalloc(&c->red_blocks, c->red_capacity) || dalloc(&c->red_out, 64)) return fail();
+    if (dalloc(&c->ctl, 1)) return fail();
+    if (cudaMallocHost((void**)&c->h_ctl, sizeof(Ctl)) != cudaSuccess) { set_error("cudaMallocHost failed"); return fail(); }
+
+    auto H2D = [&](double* d, const std::vector<double>& h) {
+        return cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+    };
+    if (H2D(rt.y, c->h_y) || H2D(rt.a_node, c->h_a_node) || H2D(rt.a_edge, c->h_a_edge) ||
+        H2D(rt.dy_edge, c->h_dy_edge) || H2D(rt.w_node, c->h_w_node)) {
+        set_error("metric upload failed");
+        return fail();
+    }
+    std::vector<cpx<double>> tw, wN;
+    twiddles(c->M, tw, wN);
+    if (cudaMemcpy(c->tw, tw.data(), tw.size() * sizeof(tw[0]), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->wN, wN.data(), wN.size() * sizeof(wN[0]), cudaMemcpyHostToDevice)) {
+        set_error("twiddle upload failed");
+        return fail();
+    }
+    const double mms_k = 2.0 * kPiD * (double)cfg.mms_kx / cfg.Lx;
+    const double mms_c = kPiD / (2.0 * cfg.h);
+    k_setup_rows<<<(Ny + 127) / 128, 128>>>(rt, Ny, c->inv_deta2, c->deta, cfg.F0, cfg.nforce, cfg.h, mms_k, mms_c);
+    if (cfg.mms) k_setup_mms_cols<<<(c->Nx + 127) / 128, 128>>>(rt.mms_sk, rt.mms_s2k, c->Nx, c->dx, mms_k);
+    k_setup_cp<<<(c->H + 127) / 128, 128>>>(c->cp, rt.a_node, rt.a_edge, c->Nx, Ny, c->Hp, c->H, cfg.Lx, c->inv_deta2);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail();
+    }
+    // launch shapes of the row kernels: up to 3 CTAs per SM, contiguous row bands
+    const size_t fsm = fft_smem(c->M);
+    if (cudaFuncSetAttribute(k_stage_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) ||
+        cudaFuncSetAttribute(k_ifft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) ||
+        cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem)) {
+        set_error("cudaFuncSetAttribute failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail();
+    }
+    Ctl h{};
+    h.t = 0.0; h.dt = cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
+    if (cudaMemcpy(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess) { set_error("ctl upload"); return fail(); }
+    *out = c;
+    return 0;
+}
+
+void context_destroy(Context* c) {
+    if (!c) return;
+    RowTables& rt = c->rt;
+    for (double* p : {rt.y, rt.a_node, rt.a_edge, rt.dy_edge, rt.w_node, rt.wt_node, rt.frow, rt.asub, rt.csup,
+                      rt.inv_csup, rt.mms_g, rt.mms_gpp, rt.mms_sin2, rt.mms_sk, rt.mms_s2k, c->w, c->w1, c->w2,
+                      c->psi, c->rhs, c->J, c->cp, c->red_blocks, c->red_out})
+        if (p) cudaFree(p);
+    if (c->hat) cudaFree(c->hat);
+    if (c->tw) cudaFree(c->tw);
+    if (c->wN) cudaFree(c->wN);
+    if (c->ctl) cudaFree(c->ctl);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    delete c;
+}
+
+// ---- launchers ----
+static int rows_per_cta(int Ny, int grid_target) {
+    const int g = std::max(1, std::min(Ny, grid_target));
+    return (Ny + g - 1) / g;
+}
+
+int launch_rows_fft(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
+                    double* rhs_out) {
+    StageParams p{};
+    p.psi = c->psi; p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out;
+    p.hat = c->hat; p.tw = c->tw; p.wN = c->wN; p.rt = c->rt; p.ctl = c->ctl;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.M = c->M; p.Hp = c->Hp; p.stage = stage; p.mms = c->cfg.mms;
+    p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.inv_dx2 = c->inv_dx2; p.inv_deta2 = c->inv_deta2;
+    p.nu = c->nu; p.lin_drag = c->cfg.lin_drag; p.Lx = c->cfg.Lx; p.h = c->cfg.h;
+    p.mms_A0 = c->cfg.mms_A0; p.mms_eps = c->cfg.mms_eps; p.mms_Om = c->cfg.mms_Om;
+    p.mms_k = 2.0 * kPiD * (double)c->cfg.mms_kx / c->cfg.Lx; p.mms_c = kPiD / (2.0 * c->cfg.h);
+    p.rows_per_cta = rows_per_cta(c->Ny, 3 * c->num_sms);
+    const int grid = (c->Ny + p.rows_per_cta - 1) / p.rows_per_cta;
+    k_stage_fft<<<grid, 256, fft_smem(c->M), s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int launch_thomas(Context* c, cudaStream_t s) {
+    ThomasParams p{};
+    p.hat = c->hat; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni; p.C = c->thomas_C; p.R = c->thomas_R;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(c->thomas_C * c->thomas_groups);
+    cfg.blockDim = dim3(KT_NW * 32);
+    cfg.dynamicSmemBytes = c->thomas_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c->thomas_C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    NSE_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_thomas, p));
+    return 0;
+}
+
+int launch_ifft(Context* c, double* psi, cudaStream_t s) {
+    IfftParams p{};
+    p.hat = c->hat; p.psi = psi; p.tw = c->tw; p.wN = c->wN;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.M = c->M; p.Hp = c->Hp;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
+    p.rows_per_cta = rows_per_cta(c->Ny, 3 * c->num_sms);
+    const int grid = (c->Ny + p.rows_per_cta - 1) / p.rows_per_cta;
+    k_ifft<<<grid, 256, fft_smem(c->M), s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int launch_thom(Context* c, double* w, const double* psi, int stage, bool closure, cudaStream_t s) {
+    ThomParams p{};
+    p.w = w; p.psi = psi; p.dy_edge = c->rt.dy_edge; p.w_node = c->rt.w_node; p.ctl = c->ctl;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.free_slip = c->cfg.free_slip; p.closure = closure ? 1 : 0; p.stage = stage;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top; p.invA_full = c->invA_full;
+    k_thom<<<1, 256, 0, s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
+    MaxParams p{};
+    p.psi = psi; p.a_node = c->rt.a_node; p.blocks = c->red_blocks; p.ctl = c->ctl;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.adapt = c->cfg.adapt; p.set_dt = set_dt ? 1 : 0;
+    p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
+    p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
+    p.dt_max = c->cfg.dt_max;
+    const size_t total = (size_t)c->Nx * (c->Ny - 2);
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)c->red_nblocks, (total + 255) / 256));
+    k_maxuv_dt<<<grid, 256, 0, s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Poisson solve of the reference (src/poisson.cuh:83-118): omega -> psi.
+int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s) {
+    if (launch_rows_fft(c, 0, w, nullptr, nullptr, s)) return -1;
+    if (launch_thomas(c, s)) return -1;
+    if (launch_ifft(c, psi, s)) return -1;
+    return 0;
+}
+
+// One SSPRK(3,3) step (src/main.cu:439-541) with dt from the control block.
+int enqueue_step(Context* c, cudaStream_t s, bool store_rhs) {
+    if (c->cfg.adapt && launch_maxuv(c, c->psi, true, s)) return -1;
+    double* wst[3] = {c->w1, c->w2, c->w};
+    const double* win[3] = {c->w, c->w1, c->w2};
+    for (int st = 1; st <= 3; ++st) {
+        if (launch_rows_fft(c, st, win[st - 1], c->w, wst[st - 1], s, (store_rhs && st == 3) ? c->rhs : nullptr))
+            return -1;
+        if (launch_thomas(c, s)) return -1;
+        if (launch_ifft(c, c->psi, s)) return -1;
+        if (launch_thom(c, wst[st - 1], c->psi, st, c->closure_diag, s)) return -1;
+    }
+    k_advance_time<<<1, 32, 0, s>>>(c->ctl);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// As enqueue_step, with events recorded on s around every kernel, for per-kernel timing:
+// ev[0] before the step and ev[1 + k] after kernel k (launches_per_step(c) + 1 events).
+int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev) {
+    int k = 0;
+    NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+    if (c->cfg.adapt) {
+        if (launch_maxuv(c, c->psi, true, s)) return -1;
+        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+    }
+    double* wst[3] = {c->w1, c->w2, c->w};
+    const double* win[3] = {c->w, c->w1, c->w2};
+    for (int st = 1; st <= 3; ++st) {
+        if (launch_rows_fft(c, st, win[st - 1], c->w, wst[st - 1], s, nullptr)) return -1;
+        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        if (launch_thomas(c, s)) return -1;
+        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        if (launch_ifft(c, c->psi, s)) return -1;
+        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        if (launch_thom(c, wst[st - 1], c->psi, st, c->closure_diag, s)) return -1;
+        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+    }
+    k_advance_time<<<1, 32, 0, s>>>(c->ctl);
+    NSE_CUDA_TRY(cudaGetLastError());
+    NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+    return 0;
+}
+
+// Names of the kernels of one step, in launch order (for the timed step).
+const char* step_kernel_name(const Context* c, int k) {
+    static const char* stage[4] = {"k_stage_fft", "k_thomas", "k_ifft", "k_thom"};
+    if (c->cfg.adapt) {
+        if (k == 0) return "k_maxuv_dt";
+        --k;
+    }
+    if (k < 12) return stage[k % 4];
+    return "k_advance_time";
+}
+
+int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 4 + 1; }
+
+// nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.
+int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs) {
+    if (nsteps <= 0) return 0;
+    if (!use_graph || store_rhs) {
+        for (int i = 0; i < nsteps; ++i)
+            if (enqueue_step(c, s, store_rhs && i == nsteps - 1)) return -1;
+        return 0;
+    }
+    if (!c->graph_exec) {
+        if (!c->cap_stream) NSE_CUDA_TRY(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+        NSE_CUDA_TRY(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_step(c, c->cap_stream, false);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->cap_stream, &g);
+        if (rc != 0) { if (g) cudaGraphDestroy(g); return -1; }
+        NSE_CUDA_TRY(e);
+        const cudaError_t e2 = cudaGraphInstantiate(&c->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        NSE_CUDA_TRY(e2);
+    }
+    for (int i = 0; i < nsteps; ++i) NSE_CUDA_TRY(cudaGraphLaunch(c->graph_exec, s));
+    return 0;
+}
+
+// omega (device) -> initial solve + Thom, t = 0 (src/main.cu:197-215)
+int set_initial_omega(Context* c, cudaStream_t s) {
+    if (poisson_solve(c, c->w, c->psi, s)) return -1;
+    if (launch_thom(c, c->w, c->psi, 1, false, s)) return -1;
+    Ctl h{};
+    h.t = 0.0; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+}  // namespace nse2d

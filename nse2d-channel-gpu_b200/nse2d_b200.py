@@ -1,0 +1,271 @@
+"""Python mirror of the nse2d-b200 C ABI (include/nse2d.h), over ctypes.
+
+This is the host-side interface a Python user (and the tests and bench.py) calls. It binds
+libnse2d_b200.so, built in this directory by `make`; there is no fallback: if the library
+or a CUDA device is missing, loading fails with an error.
+
+Two layers, as in the C header:
+  * the reference's C-linkage operator launchers (src/test_api.cu of the reference), which
+    take device pointers; `Testapi` wraps them for torch CUDA tensors;
+  * `Solver`, the status-returning solver-context API: the whole SSPRK(3,3) step of the
+    reference time loop (src/main.cu:434-541), its Poisson solve and its diagnostics.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnse2d_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "nse2d.h")
+
+DIAG_COLUMNS = ["umax", "vmax", "K", "Omega", "dOmega_rhs", "eta", "BOmega_wall", "Pin", "epsilon", "POmega",
+                "tauw_bot", "tauw_top", "dpdx", "utau_avg", "Cf", "Re_tau",
+                "dOmega_rhs_same", "dOmega_rhs_same_int", "Omega_int", "eta_int", "Jwall_s1_cum", "Jwall_s2_cum",
+                "Jwall_s3_cum", "Omega_int_w", "dOmega_same_int_w", "A_w", "P_int_w", "eta_h", "Phi_h"]
+
+
+class Nse2dError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    """struct nse2d_config: the reference's Grid + Params (src/common.cuh:42-114)."""
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Lx", ctypes.c_double), ("h", ctypes.c_double),
+                ("stretch", ctypes.c_int), ("beta", ctypes.c_double), ("Ub", ctypes.c_double),
+                ("Reb", ctypes.c_double), ("nu_override", ctypes.c_double), ("dt_init", ctypes.c_double),
+                ("dt_max", ctypes.c_double), ("cfl", ctypes.c_double), ("cvisc", ctypes.c_double),
+                ("adapt", ctypes.c_int), ("t_end", ctypes.c_double), ("F0", ctypes.c_double),
+                ("nforce", ctypes.c_int), ("lin_drag", ctypes.c_double), ("free_slip", ctypes.c_int),
+                ("mms", ctypes.c_int), ("mms_A0", ctypes.c_double), ("mms_eps", ctypes.c_double),
+                ("mms_Om", ctypes.c_double), ("mms_kx", ctypes.c_int), ("closure_diag", ctypes.c_int),
+                ("precision", ctypes.c_int)]
+
+
+_lib = None
+
+
+def header_functions(path=HEADER):
+    """Names of the functions declared in include/nse2d.h."""
+    import re
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(?:void|int|const char\*)\s+\**(\w+)\s*\(", txt)))
+
+
+def load(path=LIB_PATH):
+    """Load libnse2d_b200.so and declare the signatures. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(path):
+        raise Nse2dError(f"{path} is missing: build it with `make -C {HERE}` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(path)
+    P, I, D, V = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, None
+    sig = {
+        "nse2d_config_default": (V, [ctypes.POINTER(Config)]),
+        "nse2d_create": (I, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+        "nse2d_destroy": (I, [P]),
+        "nse2d_set_omega": (I, [P, P, I, P]),
+        "nse2d_set_state": (I, [P, P, P, I, D, P]),
+        "nse2d_get_fields": (I, [P, P, P, I, P]),
+        "nse2d_field_ptr": (I, [P, I, ctypes.POINTER(P)]),
+        "nse2d_step": (I, [P, I, I, P]),
+        "nse2d_step_store_rhs": (I, [P, I, P]),
+        "nse2d_launches_per_step": (I, [P]),
+        "nse2d_step_timed": (I, [P, I, P, P]),
+        "nse2d_step_kernel_name": (ctypes.c_char_p, [P, I]),
+        "nse2d_set_dt": (I, [P, D, P]),
+        "nse2d_set_schedule": (I, [P, D, D, P]),
+        "nse2d_get_time": (I, [P, P, P, P, P, P]),
+        "nse2d_poisson_solve": (I, [P, P, P, P]),
+        "nse2d_max_uv": (I, [P, P, P]),
+        "nse2d_diagnostics": (I, [P, I, P, P]),
+        "nse2d_rhs_at_state": (I, [P, D, P]),
+        "nse2d_uv": (I, [P, P, P, P]),
+        "nse2d_nonfinite": (I, [P, P, P]),
+        "nse2d_metrics": (I, [P, I, P]),
+        "nse2d_scalar": (I, [P, I, P]),
+        "nse2d_last_error": (ctypes.c_char_p, []),
+        "nse2d_set_abort_on_error": (V, [I]),
+        "nse2d_testapi_set_free_slip": (V, [I]),
+        "testapi_uv_from_psi_mapped": (V, [P, P, P, I, I, D, D, P, P]),
+        "testapi_omega_from_psi_interior_mapped": (V, [P, P, I, I, D, D, P, P, P]),
+        "testapi_thom_wall_vorticity_mapped": (V, [P, P, I, I, P, D, D, P]),
+        "testapi_arakawa_J_mapped": (V, [P, P, P, I, I, D, D, P, P]),
+        "testapi_compute_adv_from_uv_mapped": (V, [P, P, P, P, I, I, D, D, P, P]),
+        "testapi_compute_adv_flux_mapped": (V, [P, P, P, P, I, I, D, D, P, P]),
+        "testapi_arakawa_J_mapped_split": (V, [P, P, P, P, P, P, I, I, D, D, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise Nse2dError(load().nse2d_last_error().decode())
+
+
+def default_config(**kw):
+    cfg = Config()
+    load().nse2d_config_default(ctypes.byref(cfg))
+    for k, v in kw.items():
+        if k == "stretch" and isinstance(v, str):
+            v = {"none": 0, "uniform": 0, "tanh": 1}[v]
+        setattr(cfg, k, v)
+    return cfg
+
+
+def _ptr(a):
+    """Device or host address of a torch tensor or a numpy array."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if hasattr(s, "cuda_stream"):
+        return ctypes.c_void_p(s.cuda_stream)
+    return ctypes.c_void_p(int(s))
+
+
+class Solver:
+    """One channel on one GPU: the reference time loop's state and operators."""
+
+    def __init__(self, cfg=None, **kw):
+        self.lib = load()
+        self.cfg = cfg if cfg is not None else default_config(**kw)
+        h = ctypes.c_void_p()
+        _check(self.lib.nse2d_create(ctypes.byref(self.cfg), ctypes.byref(h)))
+        self.h = h
+        self.Nx, self.Ny = self.cfg.Nx, self.cfg.Ny
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nse2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state ----
+    def set_omega(self, w, stream=None):
+        """omega (host numpy [Ny,Nx] or CUDA tensor) -> initial Poisson solve + Thom, t = 0."""
+        if hasattr(w, "data_ptr"):
+            _check(self.lib.nse2d_set_omega(self.h, _ptr(w), 1, _stream(stream)))
+        else:
+            w = np.ascontiguousarray(w, dtype=np.float64)
+            assert w.size == self.Nx * self.Ny
+            _check(self.lib.nse2d_set_omega(self.h, _ptr(w), 0, _stream(stream)))
+
+    def set_state(self, w, psi, t=0.0, stream=None):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        _check(self.lib.nse2d_set_state(self.h, _ptr(w), _ptr(psi), 0, float(t), _stream(stream)))
+
+    def fields(self, stream=None):
+        w = np.empty((self.Ny, self.Nx))
+        psi = np.empty((self.Ny, self.Nx))
+        _check(self.lib.nse2d_get_fields(self.h, _ptr(w), _ptr(psi), 0, _stream(stream)))
+        return w, psi
+
+    def field_ptr(self, which):
+        p = ctypes.c_void_p()
+        _check(self.lib.nse2d_field_ptr(self.h, which, ctypes.byref(p)))
+        return p.value
+
+    # ---- time stepping ----
+    def step(self, nsteps=1, use_graph=False, stream=None):
+        _check(self.lib.nse2d_step(self.h, int(nsteps), 1 if use_graph else 0, _stream(stream)))
+
+    def step_store_rhs(self, nsteps=1, stream=None):
+        _check(self.lib.nse2d_step_store_rhs(self.h, int(nsteps), _stream(stream)))
+
+    def step_timed(self, nsteps, stream=None):
+        """nsteps steps with per-kernel CUDA events; returns [(kernel name, total ms)] in launch order."""
+        nk = self.launches_per_step()
+        out = (ctypes.c_double * nk)()
+        _check(self.lib.nse2d_step_timed(self.h, int(nsteps), out, _stream(stream)))
+        return [(self.lib.nse2d_step_kernel_name(self.h, k).decode(), out[k]) for k in range(nk)]
+
+    def launches_per_step(self):
+        return self.lib.nse2d_launches_per_step(self.h)
+
+    def set_dt(self, dt, stream=None):
+        _check(self.lib.nse2d_set_dt(self.h, float(dt), _stream(stream)))
+
+    def set_schedule(self, next_snap=1e300, next_diag=1e300, stream=None):
+        _check(self.lib.nse2d_set_schedule(self.h, float(next_snap), float(next_diag), _stream(stream)))
+
+    def time(self, stream=None):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        um = (ctypes.c_double * 3)()
+        _check(self.lib.nse2d_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st), um,
+                                       _stream(stream)))
+        return t.value, dt.value, st.value, tuple(um)
+
+    def nonfinite(self, stream=None):
+        f = ctypes.c_int()
+        _check(self.lib.nse2d_nonfinite(self.h, ctypes.byref(f), _stream(stream)))
+        return bool(f.value)
+
+    # ---- operators ----
+    def poisson_solve(self, w_dev, psi_dev, stream=None):
+        """psi from omega (CUDA tensors [Ny,Nx] float64), the reference's Poisson2D_Z2Z::solve."""
+        _check(self.lib.nse2d_poisson_solve(self.h, _ptr(w_dev), _ptr(psi_dev), _stream(stream)))
+
+    def max_uv(self, stream=None):
+        out = (ctypes.c_double * 3)()
+        _check(self.lib.nse2d_max_uv(self.h, out, _stream(stream)))
+        return tuple(out)
+
+    def diagnostics(self, t0_row=False, stream=None):
+        out = (ctypes.c_double * 29)()
+        _check(self.lib.nse2d_diagnostics(self.h, 1 if t0_row else 0, out, _stream(stream)))
+        return dict(zip(DIAG_COLUMNS, list(out)))
+
+    def rhs_at_state(self, t, stream=None):
+        _check(self.lib.nse2d_rhs_at_state(self.h, float(t), _stream(stream)))
+
+    def metric(self, which):
+        n = self.Ny if which in (0, 1, 4) else self.Ny - 1
+        out = np.empty(n)
+        _check(self.lib.nse2d_metrics(self.h, which, _ptr(out)))
+        return out
+
+    def scalar(self, which):
+        v = ctypes.c_double()
+        _check(self.lib.nse2d_scalar(self.h, which, ctypes.byref(v)))
+        return v.value
+
+
+class Testapi:
+    """The reference's C-linkage operator launchers (src/test_api.cu) on torch CUDA tensors."""
+
+    def __init__(self):
+        self.lib = load()
+
+    def __getattr__(self, name):
+        f = getattr(self.lib, "testapi_" + name)
+
+        def call(*args, stream=None):
+            conv = [_ptr(a) if hasattr(a, "data_ptr") or a is None else a for a in args]
+            return f(*conv, _stream(stream))
+        return call
