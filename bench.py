@@ -87,18 +87,19 @@ def algorithmic_bytes_per_step(Nx, Ny, real_bytes=8):
 
 
 def kernel_bytes(name, stage, Nx, Ny):
-    """Algorithmic bytes of one launch of each kernel of this implementation."""
-    N, H = Nx * Ny, Nx // 2 + 1
-    if name == "k_stage_fft":
-        return 8 * N * (2 if stage == 1 else 3) + 8 * N + 16 * H * (Ny - 2)
+    """Algorithmic bytes of one launch of each kernel of this implementation (inputs read
+    once, outputs written once)."""
+    N, H, Ni = Nx * Ny, Nx // 2 + 1, Ny - 2
+    if name == "k_stage":
+        return 8 * N * (2 if stage == 1 else 3) + 8 * N          # psi, omega^(s) [, omega^n] -> omega^(s+1)
+    if name == "k_fft_fwd":
+        return 8 * Nx * Ni + 16 * H * Ni                         # omega^(s+1) rows -> omega-hat
     if name == "k_thomas":
-        return 16 * H * (Ny - 2) * 2 + 8 * H * (Ny - 2)
-    if name == "k_ifft":
-        return 16 * H * (Ny - 2) + 8 * N
+        return 16 * H * Ni * 2 + 8 * H * Ni                      # omega-hat, cp -> psi-hat
+    if name == "k_ifft_thom":
+        return 16 * H * Ni + 8 * N + 8 * 6 * Nx                  # psi-hat -> psi, + Thom rows
     if name == "k_maxuv_dt":
         return 8 * N
-    if name == "k_thom":
-        return 8 * 4 * Nx + 8 * 2 * Nx
     return 0
 
 
@@ -252,7 +253,7 @@ def run_ours(args, world, rank, local):
     agg = {}
     stage = 0
     for name, tot in per_kernel:
-        if name == "k_stage_fft":
+        if name == "k_stage":
             stage += 1
         b = kernel_bytes(name, stage, Nx, Ny)
         a = agg.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0})
@@ -347,8 +348,30 @@ def run_reference(args, world, rank):
             "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def profile_steps(args):
+    """A short, untimed run of the workload for profilers: initial solve, then K plain steps
+    (no graph), so that every kernel launch is visible separately."""
+    import torch
+    nse = _load("nse2d_b200", os.path.join(PKG, "nse2d_b200.py"))
+    W = dict(WORKLOAD)
+    if args.nx:
+        W["Nx"], W["Ny"] = args.nx, args.ny
+    y = tanh_y(W["Ny"], W["beta"], W["h"])
+    s = nse.Solver(**W)
+    s.set_omega(initial_vorticity(W["Nx"], W["Ny"], W["Lx"], y, seed=1))
+    s.step(args.profile_steps, use_graph=False)
+    torch.cuda.synchronize()
+    t, dt, n, m = s.time()
+    print(json.dumps({"profile_steps": n, "t": t, "dt": dt, "umax": m[0], "nonfinite": s.nonfinite()}))
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="untimed run of K plain steps for a profiler (no JSON bench line)")
+    ap.add_argument("--nx", type=int, default=0)
+    ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
@@ -358,6 +381,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.profile_steps > 0:
+        profile_steps(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

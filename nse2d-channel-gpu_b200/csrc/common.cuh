@@ -53,6 +53,7 @@ struct Ctl {
     double jwall[3];               // closure_diag: enstrophy added by the wall update, per stage
     long long step;
     unsigned int blocks_done;      // last-block-done counter of the max reduction
+    unsigned int ifft_done;        // last-block-done counter of the stage-3 inverse transform
     int nonfinite;                 // set when a reduction saw NaN/Inf
 };
 

@@ -7,11 +7,13 @@ int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>
                     std::vector<double>& a_edge, std::vector<double>& dy_edge, std::vector<double>& w_node);
 int context_create(const Config& cfg, Context** out);
 void context_destroy(Context* c);
-int launch_rows_fft(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
-                    double* rhs_out = nullptr);
+int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
+                 double* rhs_out = nullptr);
+int launch_fft_fwd(Context* c, const double* src, cudaStream_t s);
 int launch_thomas(Context* c, cudaStream_t s);
-int launch_ifft(Context* c, double* psi, cudaStream_t s);
-int launch_thom(Context* c, double* w, const double* psi, int stage, bool closure, cudaStream_t s);
+int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom, bool closure, cudaStream_t s,
+                     bool advance = false);
+int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s);
 int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s);
 int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s);
 int enqueue_step(Context* c, cudaStream_t s, bool store_rhs);

@@ -166,7 +166,7 @@ int rhs_at_state(Context* c, const double* w, const double* psi, double* J, doub
     p.psi = psi; p.w_in = w; p.rt = c->rt;
     p.Nx = c->Nx; p.Ny = c->Ny; p.mms = c->cfg.mms;
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.inv_dx2 = c->inv_dx2; p.inv_deta2 = c->inv_deta2;
-    p.nu = c->nu; p.lin_drag = c->cfg.lin_drag; p.Lx = c->cfg.Lx; p.h = c->cfg.h;
+    p.nu = c->nu; p.lin_drag = c->cfg.lin_drag;
     p.mms_A0 = c->cfg.mms_A0; p.mms_eps = c->cfg.mms_eps; p.mms_Om = c->cfg.mms_Om;
     p.mms_k = 2.0 * kPiD * (double)c->cfg.mms_kx / c->cfg.Lx; p.mms_c = kPiD / (2.0 * c->cfg.h);
     const dim3 tb(128, 2);
@@ -209,9 +209,9 @@ void testapi_omega_from_psi_interior_mapped(double* d_w, const double* d_psi, in
 void testapi_thom_wall_vorticity_mapped(double* d_w, const double* d_psi, int Nx, int Ny, const double* d_dy_edge,
                                         double psi_bot, double psi_top, cudaStream_t s) {
     ThomParams p{};
-    p.w = d_w; p.psi = d_psi; p.dy_edge = d_dy_edge; p.w_node = nullptr; p.ctl = nullptr;
-    p.Nx = Nx; p.Ny = Ny; p.free_slip = g_free_slip ? 1 : 0; p.closure = 0; p.stage = 1;
-    p.psi_bot = psi_bot; p.psi_top = psi_top; p.invA_full = 0.0;
+    p.w = d_w; p.psi = d_psi; p.dy_edge = d_dy_edge;
+    p.Nx = Nx; p.Ny = Ny; p.free_slip = g_free_slip ? 1 : 0;
+    p.psi_bot = psi_bot; p.psi_top = psi_top;
     k_thom<<<(Nx + 255) / 256, 256, 0, s>>>(p);
     after_launch("testapi_thom_wall_vorticity_mapped");
 }

@@ -156,8 +156,6 @@ template <typename T> static int dalloc(T** p, size_t n) {
     return 0;
 }
 
-static size_t fft_smem(int M) { return 2 * (size_t)padded_size(M) * sizeof(cpx<double>); }
-
 int context_create(const Config& cfg, Context** out) {
     *out = nullptr;
     if (cfg.Nx < 4 || (cfg.Nx & (cfg.Nx - 1)) != 0) {
@@ -201,16 +199,7 @@ int context_create(const Config& cfg, Context** out) {
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (c->num_sms <= 0) c->num_sms = 148;
 
-    // Thomas launch shape: clusters of C CTAs (C <= 8) splitting Ni rows, R rows per CTA
-    c->thomas_C = std::min(8, std::max(1, (c->Ni + 255) / 256));
-    c->thomas_R = (c->Ni + c->thomas_C - 1) / c->thomas_C;
     c->thomas_groups = (c->H + 15) / 16;
-    c->thomas_smem = ((size_t)c->thomas_R * 48 + 2 * KT_NW * 32 + 128) * sizeof(double);
-    if (c->thomas_smem > 220 * 1024) {
-        set_error("Ny = %d too large for the cluster Thomas solve (R = %d rows per CTA)", Ny, c->thomas_R);
-        delete c;
-        return -1;
-    }
     auto fail = [&]() { context_destroy(c); return -1; };
     RowTables& rt = c->rt;
     if (dalloc(&rt.y, Ny) || dalloc(&rt.a_node, Ny) || dalloc(&rt.a_edge, Ny) || dalloc(&rt.dy_edge, Ny) ||
@@ -260,13 +249,44 @@ int context_create(const Config& cfg, Context** out) {
         set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail();
     }
-    // launch shapes of the row kernels: up to 3 CTAs per SM, contiguous row bands
-    const size_t fsm = fft_smem(c->M);
-    if (cudaFuncSetAttribute(k_stage_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) ||
-        cudaFuncSetAttribute(k_ifft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) ||
-        cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem)) {
-        set_error("cudaFuncSetAttribute failed: %s", cudaGetErrorString(cudaGetLastError()));
-        return fail();
+    // Thomas launch shape: clusters of C CTAs splitting the Ni interior rows, R rows per CTA,
+    // aiming at R ~ 128 (54 KB of shared memory, 4 CTAs per SM). Clusters of more than 8 CTAs
+    // are used only when the occupancy query says they can be scheduled.
+    {
+        auto shape = [&](int C) {
+            c->thomas_C = C;
+            c->thomas_R = (c->Ni + C - 1) / C;
+            c->thomas_smem = thomas_smem_doubles(c->thomas_R, C) * sizeof(double);
+        };
+        int C = std::min(16, std::max(1, (c->Ni + 127) / 128));
+        if (C > 8) {
+            shape(C);
+            int nclusters = 0;
+            cudaLaunchConfig_t lc{};
+            lc.gridDim = dim3(C * c->thomas_groups);
+            lc.blockDim = dim3(KT_NW * 32);
+            lc.dynamicSmemBytes = c->thomas_smem;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            if (cudaFuncSetAttribute(k_thomas, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+                cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem) != cudaSuccess ||
+                cudaOccupancyMaxActiveClusters(&nclusters, k_thomas, &lc) != cudaSuccess || nclusters < 1) {
+                cudaGetLastError();
+                C = 8;
+            }
+        }
+        shape(C);
+        if (c->thomas_smem > 220 * 1024) {
+            set_error("Ny = %d too large for the cluster Thomas solve (R = %d rows per CTA)", Ny, c->thomas_R);
+            return fail();
+        }
+        if (cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem)) {
+            set_error("cudaFuncSetAttribute failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return fail();
+        }
     }
     Ctl h{};
     h.t = 0.0; h.dt = cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
@@ -293,26 +313,90 @@ void context_destroy(Context* c) {
 }
 
 // ---- launchers ----
-static int rows_per_cta(int Ny, int grid_target) {
-    const int g = std::max(1, std::min(Ny, grid_target));
-    return (Ny + g - 1) / g;
+static int rows_per_cta(int rows, int grid_target) {
+    const int g = std::max(1, std::min(rows, grid_target));
+    return (rows + g - 1) / g;
 }
 
-int launch_rows_fft(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
-                    double* rhs_out) {
+static StageParams stage_params(Context* c) {
     StageParams p{};
-    p.psi = c->psi; p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out;
-    p.hat = c->hat; p.tw = c->tw; p.wN = c->wN; p.rt = c->rt; p.ctl = c->ctl;
-    p.Nx = c->Nx; p.Ny = c->Ny; p.M = c->M; p.Hp = c->Hp; p.stage = stage; p.mms = c->cfg.mms;
+    p.psi = c->psi; p.rt = c->rt; p.ctl = c->ctl;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.mms = c->cfg.mms;
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.inv_dx2 = c->inv_dx2; p.inv_deta2 = c->inv_deta2;
-    p.nu = c->nu; p.lin_drag = c->cfg.lin_drag; p.Lx = c->cfg.Lx; p.h = c->cfg.h;
+    p.nu = c->nu; p.lin_drag = c->cfg.lin_drag;
     p.mms_A0 = c->cfg.mms_A0; p.mms_eps = c->cfg.mms_eps; p.mms_Om = c->cfg.mms_Om;
     p.mms_k = 2.0 * kPiD * (double)c->cfg.mms_kx / c->cfg.Lx; p.mms_c = kPiD / (2.0 * c->cfg.h);
-    p.rows_per_cta = rows_per_cta(c->Ny, 3 * c->num_sms);
-    const int grid = (c->Ny + p.rows_per_cta - 1) / p.rows_per_cta;
-    k_stage_fft<<<grid, 256, fft_smem(c->M), s>>>(p);
+    return p;
+}
+
+int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, double* w_out, cudaStream_t s,
+                 double* rhs_out) {
+    StageParams p = stage_params(c);
+    p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out; p.stage = stage;
+    const dim3 grid((c->Nx + ST_TX - 1) / ST_TX, (c->Ny + ST_TY - 1) / ST_TY);
+    k_stage<<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+static size_t fft_smem(int M) { return (size_t)fft_smem_elems(M) * sizeof(cpx<double>); }
+
+static FftParams fft_params(Context* c) {
+    FftParams p{};
+    p.hat = c->hat; p.tw = c->tw; p.wN = c->wN; p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp;
+    p.dy_edge = c->rt.dy_edge; p.w_node = c->rt.w_node; p.ctl = c->ctl; p.free_slip = c->cfg.free_slip;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top; p.invA_full = c->invA_full;
+    return p;
+}
+
+template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) {
+    const size_t sm = fft_smem(M);
+    NSE_CUDA_TRY(cudaFuncSetAttribute(k_fft_fwd<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    p.rows_per_cta = rows_per_cta(c->Ni, 3 * c->num_sms);
+    const int grid = (c->Ni + p.rows_per_cta - 1) / p.rows_per_cta;
+    k_fft_fwd<M><<<grid, FFT_NT, sm, s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
+    const size_t sm = fft_smem(M);
+    NSE_CUDA_TRY(cudaFuncSetAttribute(k_ifft_thom<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    p.rows_per_cta = std::max(3, rows_per_cta(c->Ny, 3 * c->num_sms));
+    const int grid = std::max(1, c->Ny / p.rows_per_cta);   // the last band takes the remainder
+    k_ifft_thom<M><<<grid, FFT_NT, sm, s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+#define NSE_FFT_DISPATCH(FN)                                                       \
+    switch (c->M) {                                                                \
+        case 2: return FN<2>(c, p, s);       case 4: return FN<4>(c, p, s);        \
+        case 8: return FN<8>(c, p, s);       case 16: return FN<16>(c, p, s);      \
+        case 32: return FN<32>(c, p, s);     case 64: return FN<64>(c, p, s);      \
+        case 128: return FN<128>(c, p, s);   case 256: return FN<256>(c, p, s);    \
+        case 512: return FN<512>(c, p, s);   case 1024: return FN<1024>(c, p, s);  \
+        case 2048: return FN<2048>(c, p, s); case 4096: return FN<4096>(c, p, s);  \
+        case 8192: return FN<8192>(c, p, s);                                       \
+        default: set_error("no FFT kernel for M = %d", c->M); return -1;           \
+    }
+
+int launch_fft_fwd(Context* c, const double* src, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(src) % 16 != 0) {
+        set_error("omega must be 16-byte aligned for the row transform (got %p)", (const void*)src);
+        return -1;
+    }
+    FftParams p = fft_params(c);
+    p.src = src;
+    NSE_FFT_DISPATCH(fft_fwd_t)
+}
+
+int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom, bool closure, cudaStream_t s,
+                     bool advance) {
+    FftParams p = fft_params(c);
+    p.psi = psi; p.w = w; p.stage = stage; p.do_thom = do_thom ? 1 : 0; p.closure = closure ? 1 : 0;
+    p.advance = advance ? 1 : 0;
+    NSE_FFT_DISPATCH(fft_inv_t)
 }
 
 int launch_thomas(Context* c, cudaStream_t s) {
@@ -336,24 +420,12 @@ int launch_thomas(Context* c, cudaStream_t s) {
     return 0;
 }
 
-int launch_ifft(Context* c, double* psi, cudaStream_t s) {
-    IfftParams p{};
-    p.hat = c->hat; p.psi = psi; p.tw = c->tw; p.wN = c->wN;
-    p.Nx = c->Nx; p.Ny = c->Ny; p.M = c->M; p.Hp = c->Hp;
-    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
-    p.rows_per_cta = rows_per_cta(c->Ny, 3 * c->num_sms);
-    const int grid = (c->Ny + p.rows_per_cta - 1) / p.rows_per_cta;
-    k_ifft<<<grid, 256, fft_smem(c->M), s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
-}
-
-int launch_thom(Context* c, double* w, const double* psi, int stage, bool closure, cudaStream_t s) {
+// the reference's standalone Thom launcher (src/ops.cu:270-276)
+int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s) {
     ThomParams p{};
-    p.w = w; p.psi = psi; p.dy_edge = c->rt.dy_edge; p.w_node = c->rt.w_node; p.ctl = c->ctl;
-    p.Nx = c->Nx; p.Ny = c->Ny; p.free_slip = c->cfg.free_slip; p.closure = closure ? 1 : 0; p.stage = stage;
-    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top; p.invA_full = c->invA_full;
-    k_thom<<<1, 256, 0, s>>>(p);
+    p.w = w; p.psi = psi; p.dy_edge = c->rt.dy_edge; p.Nx = c->Nx; p.Ny = c->Ny; p.free_slip = c->cfg.free_slip;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
+    k_thom<<<(c->Nx + 255) / 256, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -365,8 +437,7 @@ int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
     p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
     p.dt_max = c->cfg.dt_max;
-    const size_t total = (size_t)c->Nx * (c->Ny - 2);
-    const int grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)c->red_nblocks, (total + 255) / 256));
+    const int grid = std::max(1, std::min(4 * c->num_sms, c->Ny - 2));   // partials fit red_blocks (>= 32 Ny)
     k_maxuv_dt<<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -374,68 +445,51 @@ int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
 
 // Poisson solve of the reference (src/poisson.cuh:83-118): omega -> psi.
 int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s) {
-    if (launch_rows_fft(c, 0, w, nullptr, nullptr, s)) return -1;
+    if (launch_fft_fwd(c, w, s)) return -1;
     if (launch_thomas(c, s)) return -1;
-    if (launch_ifft(c, psi, s)) return -1;
+    if (launch_ifft_thom(c, psi, nullptr, 0, false, false, s)) return -1;
     return 0;
 }
 
-// One SSPRK(3,3) step (src/main.cu:439-541) with dt from the control block.
-int enqueue_step(Context* c, cudaStream_t s, bool store_rhs) {
-    if (c->cfg.adapt && launch_maxuv(c, c->psi, true, s)) return -1;
-    double* wst[3] = {c->w1, c->w2, c->w};
-    const double* win[3] = {c->w, c->w1, c->w2};
-    for (int st = 1; st <= 3; ++st) {
-        if (launch_rows_fft(c, st, win[st - 1], c->w, wst[st - 1], s, (store_rhs && st == 3) ? c->rhs : nullptr))
-            return -1;
-        if (launch_thomas(c, s)) return -1;
-        if (launch_ifft(c, c->psi, s)) return -1;
-        if (launch_thom(c, wst[st - 1], c->psi, st, c->closure_diag, s)) return -1;
-    }
-    k_advance_time<<<1, 32, 0, s>>>(c->ctl);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
-}
-
-// As enqueue_step, with events recorded on s around every kernel, for per-kernel timing:
-// ev[0] before the step and ev[1 + k] after kernel k (launches_per_step(c) + 1 events).
-int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev) {
+// One SSPRK(3,3) step (src/main.cu:439-541) with dt from the control block. With ev != nullptr
+// an event is recorded before the step and after every kernel (for per-kernel timing).
+static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
     int k = 0;
-    NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+    auto mark = [&]() -> int {
+        if (ev) NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        return 0;
+    };
+    if (mark()) return -1;
     if (c->cfg.adapt) {
-        if (launch_maxuv(c, c->psi, true, s)) return -1;
-        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        if (launch_maxuv(c, c->psi, true, s) || mark()) return -1;
     }
     double* wst[3] = {c->w1, c->w2, c->w};
     const double* win[3] = {c->w, c->w1, c->w2};
     for (int st = 1; st <= 3; ++st) {
-        if (launch_rows_fft(c, st, win[st - 1], c->w, wst[st - 1], s, nullptr)) return -1;
-        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
-        if (launch_thomas(c, s)) return -1;
-        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
-        if (launch_ifft(c, c->psi, s)) return -1;
-        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
-        if (launch_thom(c, wst[st - 1], c->psi, st, c->closure_diag, s)) return -1;
-        NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
+        if (launch_stage(c, st, win[st - 1], c->w, wst[st - 1], s, (store_rhs && st == 3) ? c->rhs : nullptr) || mark())
+            return -1;
+        if (launch_fft_fwd(c, wst[st - 1], s) || mark()) return -1;
+        if (launch_thomas(c, s) || mark()) return -1;
+        // the stage-3 transform also advances the time (its last CTA)
+        if (launch_ifft_thom(c, c->psi, wst[st - 1], st, true, c->closure_diag, s, st == 3) || mark()) return -1;
     }
-    k_advance_time<<<1, 32, 0, s>>>(c->ctl);
-    NSE_CUDA_TRY(cudaGetLastError());
-    NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
     return 0;
 }
+
+int enqueue_step(Context* c, cudaStream_t s, bool store_rhs) { return step_impl(c, s, store_rhs, nullptr); }
+int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev) { return step_impl(c, s, false, ev); }
 
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
-    static const char* stage[4] = {"k_stage_fft", "k_thomas", "k_ifft", "k_thom"};
+    static const char* stage[4] = {"k_stage", "k_fft_fwd", "k_thomas", "k_ifft_thom"};
     if (c->cfg.adapt) {
         if (k == 0) return "k_maxuv_dt";
         --k;
     }
-    if (k < 12) return stage[k % 4];
-    return "k_advance_time";
+    return (k < 12) ? stage[k % 4] : "";
 }
 
-int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 4 + 1; }
+int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 4; }
 
 // nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.
 int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs) {
@@ -464,7 +518,7 @@ int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store
 // omega (device) -> initial solve + Thom, t = 0 (src/main.cu:197-215)
 int set_initial_omega(Context* c, cudaStream_t s) {
     if (poisson_solve(c, c->w, c->psi, s)) return -1;
-    if (launch_thom(c, c->w, c->psi, 1, false, s)) return -1;
+    if (launch_thom(c, c->w, c->psi, s)) return -1;
     Ctl h{};
     h.t = 0.0; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));

@@ -1,20 +1,22 @@
 // Device kernels of one SSPRK(3,3) step (FP64). Written for this project.
 //
 // Per stage s (reference loop src/main.cu:482-538):
-//   k_stage_fft   rows: omega^(s+1) = RK combine of omega^(s) + dt rhs(psi, omega^(s)) with
-//                 rhs = -J_arakawa + nu lap + f(y) - r omega (+ MMS forcing), written to HBM,
-//                 and the forward real FFT of every interior row -> omega-hat [Ny][Hp].
+//   k_stage       2-D tiles: omega^(s+1) = RK combine of omega^(s) + dt rhs(psi, omega^(s)),
+//                 rhs = -J_arakawa + nu lap + f(y) - r omega (+ MMS forcing). psi and omega
+//                 tiles with a one-cell halo are staged in shared memory.
+//   k_fft_fwd     forward real FFT of every interior row of omega^(s+1) -> omega-hat [Ny][Hp].
 //   k_thomas      y-direction tridiagonal solve of every kx column, in place
 //                 (omega-hat -> psi-hat). One thread-block cluster owns 16 kx columns and
-//                 splits the Ny-2 rows among its CTAs; each warp sweeps a 32-row segment and
+//                 splits the Ny-2 rows among its CTAs; each warp sweeps a segment of rows and
 //                 the segments are joined through their affine carries (smem + DSMEM).
-//   k_ifft        inverse real FFT of every row -> psi [Ny][Nx].
-//   k_thom        Thom wall vorticity on the two wall rows of omega^(s+1).
-// Per step: k_maxuv_dt (max|u|,|v|,|v|a -> adaptive dt on the device) before stage 1 and
-// k_advance_time after stage 3.
+//   k_ifft_thom   inverse real FFT of every row -> psi [Ny][Nx], then the Thom wall vorticity
+//                 of omega^(s+1) by the CTAs that own rows 1-2 and Ny-3..Ny-2.
+// Per step: k_maxuv_dt (max|u|,|v|,|v|a -> adaptive dt on the device) before stage 1; the
+// last CTA of the stage-3 k_ifft_thom advances the time.
 #pragma once
 #include <cooperative_groups.h>
 #include "common.cuh"
+#include "fft_rows.cuh"
 
 namespace nse2d {
 
@@ -28,133 +30,341 @@ struct StageParams {
     const double* w_n;       // omega^n (stages 2, 3); may alias w_out in stage 3
     double* w_out;           // omega^(s+1)
     double* rhs_out;         // optional: store rhs (the stage-3 rhs read by the diagnostics)
-    cpx<double>* hat;        // [Ny][Hp]
-    const cpx<double>* tw;
-    const cpx<double>* wN;
     RowTables rt;
     const Ctl* ctl;
-    int Nx, Ny, M, Hp, stage, mms, rows_per_cta;
-    double inv_dx, inv_deta, inv_dx2, inv_deta2, nu, lin_drag, Lx, h;
+    int Nx, Ny, stage, mms;
+    double inv_dx, inv_deta, inv_dx2, inv_deta2, nu, lin_drag;
     double mms_A0, mms_eps, mms_Om, mms_k, mms_c;
 };
 
-// rhs at one point; follows src/ops.cu:283-326 (Arakawa), :471-499 (Laplacian),
-// :515-534 (rhs) and :559-626 (MMS) with the same grouping of terms.
+// Mapped Arakawa Jacobian (src/ops.cu:305-325) and Laplacian (src/ops.cu:488-498) from the
+// 3x3 neighbourhood: p[r][c], o[r][c] with r = 0,1,2 for rows j-1, j, j+1 and c for x-1, x, x+1.
+__device__ __forceinline__ void stencil_J_lap(const double p[3][3], const double o[3][3], double a, double ap,
+                                              double am, double inv_dx, double inv_deta, double inv_dx2,
+                                              double inv_deta2, double& J, double& lap) {
+    const double inv4dxde = 0.25 * inv_dx * inv_deta;
+    const double psi_xp = p[1][2], psi_xm = p[1][0], psi_yp = p[2][1], psi_ym = p[0][1];
+    const double psi_pp = p[2][2], psi_pm = p[0][2], psi_mp = p[2][0], psi_mm = p[0][0];
+    const double om_xp = o[1][2], om_xm = o[1][0], om_yp = o[2][1], om_ym = o[0][1];
+    const double om_pp = o[2][2], om_pm = o[0][2], om_mp = o[2][0], om_mm = o[0][0];
+    const double wc = o[1][1];
+    const double J1 = ((psi_xp - psi_xm) * (a * (om_yp - om_ym)) - (a * (psi_yp - psi_ym)) * (om_xp - om_xm)) * inv4dxde;
+    const double J2 = (psi_xp * (a * (om_pp - om_pm)) - psi_xm * (a * (om_mp - om_mm))
+                       - a * (psi_yp * (om_pp - om_mp) - psi_ym * (om_pm - om_mm))) * inv4dxde;
+    const double J3 = (-om_xp * (a * (psi_pp - psi_pm)) + om_xm * (a * (psi_mp - psi_mm))
+                       + a * (om_yp * (psi_pp - psi_mp) - om_ym * (psi_pm - psi_mm))) * inv4dxde;
+    J = -((J1 + J2 + J3) * (1.0 / 3.0));
+    const double dxx = (om_xp - 2 * wc + om_xm) * inv_dx2;
+    const double dyy = a * (ap * (om_yp - wc) - am * (wc - om_ym)) * inv_deta2;
+    lap = dxx + dyy;
+}
+
+// MMS forcing at one point (src/ops.cu:587-624), with per-row and per-column tables.
+__device__ __forceinline__ double mms_term(const StageParams& p, int j, int i, double mA, double mAp) {
+    const double k = p.mms_k, c = p.mms_c, c2 = c * c, c3 = c2 * c;
+    const double g = p.rt.mms_g[j], gpp = p.rt.mms_gpp[j], sin2 = p.rt.mms_sin2[j];
+    const double sk = p.rt.mms_sk[i], s2k = p.rt.mms_s2k[i];
+    const double term_lin = mAp * g + (p.nu * mA) * ((k * k) * g - gpp) + (p.lin_drag * mA) * g;
+    const double term_adv = -(mA * mA) * k * c3 * s2k * sin2;
+    return sk * term_lin + term_adv;
+}
+
+// rhs at one point from global memory (used outside the step: diagnostics, J/rhs at a state)
 __device__ __forceinline__ double point_rhs(const StageParams& p, int j, int i, double fj, double wc,
-                                            double mA, double mAp) {
+                                            double mA, double mAp, double* Jout = nullptr) {
     const int Nx = p.Nx;
     double J = 0.0, lap = 0.0;
     if (j != 0 && j != p.Ny - 1) {
-        const int xm = wrapi(i - 1, Nx), xp = wrapi(i + 1, Nx);
-        const double* __restrict__ ps = p.psi;
-        const double* __restrict__ om = p.w_in;
-        const size_t r0 = (size_t)j * Nx, rm = r0 - Nx, rp = r0 + Nx;
-        const double a = __ldg(&p.rt.a_node[j]);
-        const double inv4dxde = 0.25 * p.inv_dx * p.inv_deta;
-        const double psi_xp = __ldg(&ps[r0 + xp]), psi_xm = __ldg(&ps[r0 + xm]);
-        const double psi_yp = __ldg(&ps[rp + i]), psi_ym = __ldg(&ps[rm + i]);
-        const double psi_pp = __ldg(&ps[rp + xp]), psi_pm = __ldg(&ps[rm + xp]);
-        const double psi_mp = __ldg(&ps[rp + xm]), psi_mm = __ldg(&ps[rm + xm]);
-        const double om_xp = __ldg(&om[r0 + xp]), om_xm = __ldg(&om[r0 + xm]);
-        const double om_yp = __ldg(&om[rp + i]), om_ym = __ldg(&om[rm + i]);
-        const double om_pp = __ldg(&om[rp + xp]), om_pm = __ldg(&om[rm + xp]);
-        const double om_mp = __ldg(&om[rp + xm]), om_mm = __ldg(&om[rm + xm]);
-        const double J1 = ((psi_xp - psi_xm) * (a * (om_yp - om_ym))
-                           - (a * (psi_yp - psi_ym)) * (om_xp - om_xm)) * inv4dxde;
-        const double J2 = (psi_xp * (a * (om_pp - om_pm))
-                           - psi_xm * (a * (om_mp - om_mm))
-                           - a * (psi_yp * (om_pp - om_mp)
-                                  - psi_ym * (om_pm - om_mm))) * inv4dxde;
-        const double J3 = (-om_xp * (a * (psi_pp - psi_pm))
-                           + om_xm * (a * (psi_mp - psi_mm))
-                           + a * (om_yp * (psi_pp - psi_mp)
-                                  - om_ym * (psi_pm - psi_mm))) * inv4dxde;
-        J = -((J1 + J2 + J3) * (1.0 / 3.0));
-        const double dxx = (om_xp - 2 * wc + om_xm) * p.inv_dx2;
-        const double ap = __ldg(&p.rt.a_edge[j]), am = __ldg(&p.rt.a_edge[j - 1]);
-        const double dyy = a * (ap * (om_yp - wc) - am * (wc - om_ym)) * p.inv_deta2;
-        lap = dxx + dyy;
+        double ps[3][3], om[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const size_t id = (size_t)(j - 1 + r) * Nx + wrapi(i - 1 + c, Nx);
+                ps[r][c] = p.psi[id];
+                om[r][c] = p.w_in[id];
+            }
+        stencil_J_lap(ps, om, p.rt.a_node[j], p.rt.a_edge[j], p.rt.a_edge[j - 1], p.inv_dx, p.inv_deta, p.inv_dx2,
+                      p.inv_deta2, J, lap);
     }
+    if (Jout) *Jout = J;
     double rhs = -J + p.nu * lap + fj - p.lin_drag * wc;
-    if (p.mms) {
-        const double k = p.mms_k, c = p.mms_c, c2 = c * c, c3 = c2 * c;
-        const double g = __ldg(&p.rt.mms_g[j]), gpp = __ldg(&p.rt.mms_gpp[j]), sin2 = __ldg(&p.rt.mms_sin2[j]);
-        const double sk = __ldg(&p.rt.mms_sk[i]), s2k = __ldg(&p.rt.mms_s2k[i]);
-        const double term_lin = mAp * g + (p.nu * mA) * ((k * k) * g - gpp) + (p.lin_drag * mA) * g;
-        const double term_adv = -(mA * mA) * k * c3 * s2k * sin2;
-        rhs += sk * term_lin + term_adv;
-    }
+    if (p.mms) rhs += mms_term(p, j, i, mA, mAp);
     return rhs;
 }
 
-// One stockham pass over the row buffer by the whole CTA.
-template <bool INV>
-__device__ __forceinline__ void cta_fft(cpx<double>*& in, cpx<double>*& out, int M, const cpx<double>* tw) {
-    int rad[24];
-    const int np = fft_schedule(M, rad);
-    int Ns = 1;
-    for (int ps = 0; ps < np; ++ps) {
-        const int R = rad[ps];
-        const int nb = M / R;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            if (R == 8) stockham_butterfly<double, 8, INV>(b, M, Ns, in, out, tw);
-            else if (R == 4) stockham_butterfly<double, 4, INV>(b, M, Ns, in, out, tw);
-            else stockham_butterfly<double, 2, INV>(b, M, Ns, in, out, tw);
-        }
-        __syncthreads();
-        Ns *= R;
-        cpx<double>* t = in; in = out; out = t;
-    }
-}
+// ---- k_stage: 2-D tile of TX x TY points, halo staged in shared memory ----
+// 256 threads = 64 columns x 4 row groups; a thread sweeps 8 consecutive rows of one column
+// with a sliding 3-row window of psi and omega in registers (6 shared loads per point).
+constexpr int ST_TX = 64, ST_TY = 32, ST_RPT = 8, ST_W = ST_TX + 2, ST_H = ST_TY + 2;
 
-static __global__ void __launch_bounds__(256) k_stage_fft(StageParams p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int M = p.M, Nx = p.Nx;
-    cpx<double>* bufA = reinterpret_cast<cpx<double>*>(smem_raw);
-    cpx<double>* bufB = bufA + padded_size(M);
-    const double dt = p.ctl->dt;
-    const double t = p.ctl->t;
-    // stage times: t, t + dt, t + dt/2 (src/main.cu:487-528)
-    const double ts = (p.stage == 1) ? t : (p.stage == 2 ? t + dt : t + 0.5 * dt);
+static __global__ void __launch_bounds__(256) k_stage(StageParams p) {
+    __shared__ double sp[ST_H][ST_W + 1];
+    __shared__ double so[ST_H][ST_W + 1];
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int x0 = blockIdx.x * ST_TX, y0 = blockIdx.y * ST_TY;
+    // all halo loads of a thread are issued before any of them is stored (fixed trip count)
+    constexpr int NLD = (ST_H * ST_W + 255) / 256;
+    {
+        double vp[NLD], vo[NLD];
+#pragma unroll
+        for (int u = 0; u < NLD; ++u) {
+            const int idx = threadIdx.x + 256 * u;
+            const int r = idx / ST_W, c = idx - r * ST_W;
+            const int gy = y0 - 1 + r;
+            int gx = x0 - 1 + c;
+            // x0 + ST_TX <= Nx when Nx >= ST_TX (Nx a power of two), so gx lies in [-1, Nx]
+            gx = (Nx >= ST_TX) ? (gx < 0 ? gx + Nx : (gx >= Nx ? gx - Nx : gx)) : ((gx % Nx) + Nx) % Nx;
+            vp[u] = 0.0;
+            vo[u] = 0.0;
+            if (idx < ST_H * ST_W && gy >= 0 && gy < Ny) {
+                const size_t id = (size_t)gy * Nx + gx;
+                vp[u] = __ldg(&p.psi[id]);
+                vo[u] = __ldg(&p.w_in[id]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NLD; ++u) {
+            const int idx = threadIdx.x + 256 * u;
+            if (idx < ST_H * ST_W) {
+                const int r = idx / ST_W, c = idx - r * ST_W;
+                sp[r][c] = vp[u];
+                so[r][c] = vo[u];
+            }
+        }
+    }
+    __syncthreads();
+    const double dt = p.ctl->dt, t = p.ctl->t;
+    const double ts = (p.stage == 1) ? t : (p.stage == 2 ? t + dt : t + 0.5 * dt);   // main.cu:487-528
     double mA = 0.0, mAp = 0.0;
     if (p.mms) {
         mA = p.mms_A0 * (1.0 + p.mms_eps * sin(p.mms_Om * ts));
         mAp = p.mms_A0 * (p.mms_eps * p.mms_Om * cos(p.mms_Om * ts));
     }
-    const int j0 = blockIdx.x * p.rows_per_cta;
-    const int j1 = min(p.Ny, j0 + p.rows_per_cta);
-    for (int j = j0; j < j1; ++j) {
-        const double fj = __ldg(&p.rt.frow[j]);
-        const bool interior = (j != 0 && j != p.Ny - 1);
-        const size_t row = (size_t)j * Nx;
-        if (p.stage == 0 && !interior) continue;   // plain transform: interior rows only
-        for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
-            const double wc = __ldg(&p.w_in[row + i]);
-            if (p.stage == 0) {
-                reinterpret_cast<double*>(&bufA[pad_idx(i >> 1)])[i & 1] = wc;
-                continue;
-            }
-            const double rhs = point_rhs(p, j, i, fj, wc, mA, mAp);
-            if (p.rhs_out) p.rhs_out[row + i] = rhs;
-            double wnew;
-            if (p.stage == 1) {
-                wnew = wc + dt * rhs;                                        // ops.cu:646
-            } else if (p.stage == 2) {
-                wnew = 0.75 * p.w_n[row + i] + 0.25 * (wc + dt * rhs);       // ops.cu:650
-            } else {
-                wnew = (1.0 / 3.0) * p.w_n[row + i] + (2.0 / 3.0) * (wc + dt * rhs);  // ops.cu:654
-            }
-            p.w_out[row + i] = wnew;
-            if (interior) reinterpret_cast<double*>(&bufA[pad_idx(i >> 1)])[i & 1] = wnew;
+    const int lx = threadIdx.x & (ST_TX - 1), g = threadIdx.x / ST_TX;
+    const int i = x0 + lx;
+    if (i >= Nx) return;
+    const int ly0 = g * ST_RPT;                         // first local row (tile row ly0 <-> smem row ly0 + 1)
+    double ps[3][3], om[3][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { ps[r + 1][c] = sp[ly0 + r][lx + c]; om[r + 1][c] = so[ly0 + r][lx + c]; }
+#pragma unroll
+    for (int q = 0; q < ST_RPT; ++q) {
+        const int ly = ly0 + q, j = y0 + ly;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ps[0][c] = ps[1][c]; ps[1][c] = ps[2][c]; ps[2][c] = sp[ly + 2][lx + c];
+            om[0][c] = om[1][c]; om[1][c] = om[2][c]; om[2][c] = so[ly + 2][lx + c];
         }
-        if (!interior) continue;   // uniform across the CTA
+        if (j >= Ny) break;
+        const double fj = __ldg(&p.rt.frow[j]);
+        const double wc = om[1][1];
+        double J = 0.0, lap = 0.0;
+        if (j != 0 && j != Ny - 1)
+            stencil_J_lap(ps, om, __ldg(&p.rt.a_node[j]), __ldg(&p.rt.a_edge[j]), __ldg(&p.rt.a_edge[j - 1]),
+                          p.inv_dx, p.inv_deta, p.inv_dx2, p.inv_deta2, J, lap);
+        double rhs = -J + p.nu * lap + fj - p.lin_drag * wc;                             // ops.cu:532
+        if (p.mms) rhs += mms_term(p, j, i, mA, mAp);
+        const size_t id = (size_t)j * Nx + i;
+        if (p.rhs_out) p.rhs_out[id] = rhs;
+        double wnew;
+        if (p.stage == 1) wnew = wc + dt * rhs;                                            // ops.cu:646
+        else if (p.stage == 2) wnew = 0.75 * p.w_n[id] + 0.25 * (wc + dt * rhs);           // ops.cu:650
+        else wnew = (1.0 / 3.0) * p.w_n[id] + (2.0 / 3.0) * (wc + dt * rhs);              // ops.cu:654
+        p.w_out[id] = wnew;
+    }
+}
+
+// t += dt, step++, and the snap to the scheduled output times (src/main.cu:541-551): the
+// tolerance is re-evaluated after the first snap, as the reference does.
+__device__ __forceinline__ double time_tol_d(double t) { return 64.0 * 2.220446049250313e-16 * fmax(1.0, fabs(t)); }
+
+__device__ __forceinline__ void advance_time(Ctl* ctl) {
+    const double dt = ctl->dt;
+    double t = ctl->t + dt;
+    const double ns = ctl->next_snap, nd = ctl->next_diag;
+    if (ns < 1e299 && fabs(t - ns) <= fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)))) t = ns;
+    if (nd < 1e299 && fabs(t - nd) <= fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)))) t = nd;
+    ctl->t = t;
+    ctl->step += 1;
+}
+
+// ---- row FFT kernels ----
+struct FftParams {
+    const double* src;       // forward: real rows [Ny][Nx]
+    cpx<double>* hat;        // [Ny][Hp]
+    double* psi;             // inverse output [Ny][Nx]
+    const cpx<double>* tw;   // M twiddles e^{-2 pi i t/M}
+    const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
+    int Nx, Ny, Hp, rows_per_cta;
+    // inverse only: Thom closure (src/ops.cu:102-158) and the closure_diag wall bookkeeping
+    double* w;               // omega^(s+1): wall rows rewritten
+    const double* dy_edge;
+    const double* w_node;
+    Ctl* ctl;
+    int free_slip, closure, stage, do_thom, advance;
+    double psi_bot, psi_top, invA_full;
+};
+
+constexpr int FFT_NT = 256;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared memory of the row FFT kernels: S (staging, M + 8 entries, unpadded), A (M, unpadded)
+// and B (padded_size(M)).
+__host__ __device__ constexpr int fft_smem_elems(int M) { return (M + 8) + M + (M + (M >> 3) + 1); }
+
+// Forward real FFT of rows 1..Ny-2 (the reference's pack + cuFFT forward, src/poisson.cuh:93-96):
+// a row is read as M complex points z_n = x_2n + i x_2n+1 into S by cp.async; pass 0 reads S,
+// after which the next row is loaded into S while the remaining passes run; the split step
+// then writes X_k, k = 0..M.
+template <int M>
+static __global__ void __launch_bounds__(FFT_NT, 2) k_fft_fwd(FftParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<double>* S = reinterpret_cast<cpx<double>*>(smem_raw);
+    cpx<double>* A = S + (M + 8);
+    cpx<double>* B = A + M;
+    constexpr bool OUTB = fft_out<M>::in_B;
+    const int jb = 1 + blockIdx.x * p.rows_per_cta;
+    const int je = min(p.Ny - 1, jb + p.rows_per_cta);
+    auto stage_row = [&](int j) {
+        const cpx<double>* row = reinterpret_cast<const cpx<double>*>(p.src + (size_t)j * p.Nx);
+        for (int n = threadIdx.x; n < M; n += FFT_NT) cp_async16(&S[n], &row[n]);
+    };
+    if (jb < je) stage_row(jb);
+    for (int j = jb; j < je; ++j) {
+        cp_async_wait_all();
         __syncthreads();
-        cpx<double>* in = bufA;
-        cpx<double>* out = bufB;
-        cta_fft<false>(in, out, M, p.tw);
-        cpx<double>* dst = p.hat + (size_t)j * p.Hp;
-        for (int k = threadIdx.x; k <= M; k += blockDim.x) dst[k] = rfft_split(k, M, in, p.wN);
+        fft_passes<double, M, 1, 0, false, FFT_NT>(S, A, B, p.tw, [&]() {
+            if (j + 1 < je) stage_row(j + 1);
+        });
+        const cpx<double>* Z = OUTB ? B : A;
+        double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+        for (int k = threadIdx.x; k <= M; k += FFT_NT) {
+            const int ka = (k == M ? 0 : k), kb = (k == 0 ? 0 : M - k);
+            const cpx<double> a = Z[OUTB ? pad_idx(ka) : ka];
+            const cpx<double> b0 = Z[OUTB ? pad_idx(kb) : kb];
+            const cpx<double> b = {b0.x, -b0.y};
+            const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
+            const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
+            const cpx<double> X = cadd(E, cmul(ldtw(p.wN, k), mul_mi(D)));
+            dst[k] = make_double2(X.x, X.y);
+        }
         __syncthreads();
+    }
+}
+
+// Thom wall vorticity of one wall (src/ops.cu:114-151) from the psi rows this CTA just wrote,
+// with the closure_diag enstrophy jump of the wall row (src/main.cu:271-298).
+__device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
+    const int Nx = p.Nx, Ny = p.Ny;
+    const double d1 = top ? p.dy_edge[Ny - 2] : p.dy_edge[0];
+    const double d2 = top ? p.dy_edge[Ny - 3] : p.dy_edge[1];
+    const double A = 2.0 * (1.0 / (d1 * d1) + 1.0 / (d1 * d2));
+    const double B = (-2.0) * d1 / (d2 * (d1 + d2) * (d1 + d2));
+    const double pw = top ? p.psi_top : p.psi_bot;
+    const double* r1 = p.psi + (size_t)(top ? Ny - 2 : 1) * Nx;
+    const double* r2 = p.psi + (size_t)(top ? Ny - 3 : 2) * Nx;
+    double* wr = p.w + (size_t)(top ? Ny - 1 : 0) * Nx;
+    const double wq = p.closure ? p.w_node[top ? Ny - 1 : 0] : 0.0;
+    double sb = 0.0, sa = 0.0;
+    for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
+        double nv = 0.0;
+        if (!p.free_slip) nv = -(A * (__ldcg(&r1[i]) - pw) + B * (__ldcg(&r2[i]) - pw));
+        const double ov = wr[i];
+        wr[i] = nv;
+        sb += wq * ov * ov;
+        sa += wq * nv * nv;
+    }
+    if (!p.closure) return;
+    __shared__ double rb[FFT_NT], ra[FFT_NT];
+    rb[threadIdx.x] = sb; ra[threadIdx.x] = sa;
+    __syncthreads();
+    for (int s = FFT_NT / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) { rb[threadIdx.x] += rb[threadIdx.x + s]; ra[threadIdx.x] += ra[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(&p.ctl->jwall[p.stage - 1], 0.5 * ra[0] * p.invA_full - 0.5 * rb[0] * p.invA_full);
+    __syncthreads();
+}
+
+// Contiguous row bands of L rows; the last band also takes a short remainder. With L >= 3
+// and Ny >= 5 the first band holds rows 0..2 and the last band rows Ny-3..Ny-1.
+__host__ __device__ __forceinline__ void band_of(int b, int nb, int L, int Ny, int& j0, int& j1) {
+    j0 = b * L;
+    j1 = (b == nb - 1) ? Ny : min(Ny, (b + 1) * L);
+}
+
+// Inverse real FFT of every row (the reference's cuFFT inverse + scale, src/poisson.cuh:110-114)
+// and the Thom closure of omega^(s+1) by the first and the last CTA. The half spectrum of a
+// row is staged into S by cp.async; after the merge step S is free and the next row is
+// loaded into it while the passes run.
+template <int M>
+static __global__ void __launch_bounds__(FFT_NT, 2) k_ifft_thom(FftParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<double>* S = reinterpret_cast<cpx<double>*>(smem_raw);
+    cpx<double>* A = S + (M + 8);
+    cpx<double>* B = A + M;
+    constexpr bool OUTB = fft_out<M>::in_B;
+    const int Nx = p.Nx, Ny = p.Ny;
+    int j0, j1;
+    band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
+    constexpr double scale = 1.0 / (double)M;
+    auto stage_row = [&](int j) {
+        const cpx<double>* row = p.hat + (size_t)j * p.Hp;
+        for (int k = threadIdx.x; k <= M; k += FFT_NT) cp_async16(&S[k], &row[k]);
+    };
+    int jn = (j0 < 1) ? 1 : j0;                     // next interior row to stage
+    if (jn < j1 && jn < Ny - 1) stage_row(jn);
+    for (int j = j0; j < j1; ++j) {
+        double* dst = p.psi + (size_t)j * Nx;
+        if (j == 0 || j == Ny - 1) {
+            const double v = (j == 0) ? p.psi_bot : p.psi_top;
+            for (int i = threadIdx.x; i < Nx; i += FFT_NT) dst[i] = v;
+            continue;
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        for (int k = threadIdx.x; k < M; k += FFT_NT) {
+            const cpx<double> a = S[k], b0 = S[M - k];
+            const cpx<double> b = {b0.x, -b0.y};
+            const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
+            const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
+            A[k] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, k))));
+        }
+        __syncthreads();
+        if (j + 1 < j1 && j + 1 < Ny - 1) stage_row(j + 1);
+        fft_passes<double, M, 1, 0, true, FFT_NT>(A, A, B, p.tw, []() {});
+        const cpx<double>* Z = OUTB ? B : A;
+        for (int n = threadIdx.x; n < M; n += FFT_NT) {
+            const cpx<double> z = Z[OUTB ? pad_idx(n) : n];
+            reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
+        }
+        __syncthreads();
+    }
+    if (p.do_thom) {
+        if (j0 <= 1 && j1 >= 3) thom_row(p, false);
+        if (j0 <= Ny - 3 && j1 >= Ny - 1) thom_row(p, true);
+    }
+    if (p.advance) {
+        // the last CTA to finish advances the time: t += dt and the output snap
+        __shared__ bool last;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last = (atomicAdd(&p.ctl->ifft_done, 1u) == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            p.ctl->ifft_done = 0;
+            advance_time(p.ctl);
+        }
     }
 }
 
@@ -170,56 +380,79 @@ struct ThomasParams {
 
 constexpr int KT_NW = 8;     // warps per CTA
 
-// Affine carries: a segment maps its incoming value c to d + P c.
+// Thomas sweeps of the reference (src/poisson.cu:70-133) split into segments. A segment maps
+// the value entering it to d + P c (forward elimination) and x + Q X (back substitution);
+// the maps of consecutive segments compose, so every warp sweeps its own rows and only the
+// maps travel between warps (shared memory) and CTAs (distributed shared memory).
+//
+// Shared memory of a CTA with R rows: data [R][32] (16 kx, re/im interleaved as in HBM),
+// cp [R][16], the row coefficients asub and 1/csup [R] each, per-warp maps and the maps of
+// all CTAs of the cluster.
+__host__ __device__ constexpr size_t thomas_smem_doubles(int R, int C) {
+    return (size_t)R * 32 + (size_t)R * 16 + 2 * (size_t)R + 2 * KT_NW * 32 + 2 * 64 + (size_t)C * 64;
+}
+
 static __global__ void __launch_bounds__(KT_NW * 32) k_thomas(ThomasParams p) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q = (int)cluster.block_rank();
-    const int g = blockIdx.x / p.C;                   // kx group of 16 columns
+    const int C = p.C;
+    const int g = blockIdx.x / C;                     // kx group of 16 columns
     const int R = p.R;
     double* data = reinterpret_cast<double*>(smem_raw);          // [R][32]
     double* cpv = data + (size_t)R * 32;                         // [R][16]
-    double* aggP = cpv + (size_t)R * 16;                         // [NW][32]
+    double* sasub = cpv + (size_t)R * 16;                        // [R]
+    double* sinvc = sasub + R;                                   // [R]
+    double* aggP = sinvc + R;                                    // [NW][32]
     double* aggD = aggP + KT_NW * 32;                            // [NW][32]
-    double* ctaF = aggD + KT_NW * 32;                            // [2][32]  (P, d) of this CTA
-    double* ctaB = ctaF + 64;                                    // [2][32]  (Q, x) of this CTA
+    double* ctaF = aggD + KT_NW * 32;                            // [64]  (P, d) of this CTA
+    double* ctaB = ctaF + 64;                                    // [64]  (Q, x) of this CTA
+    double* allc = ctaB + 64;                                    // [C][64] maps of the cluster's CTAs
     const int kx = g * 16 + (lane >> 1);
     const int part = lane & 1;
     const bool valid = kx < p.H;
     const int r0 = q * R;                                         // first interior row index (0-based)
     const int r1 = min(p.Ni, r0 + R);
+    const int nr = max(0, r1 - r0);
     const int RW = (R + KT_NW - 1) / KT_NW;
     const int wa = min(r1, r0 + warp * RW), wb = min(r1, r0 + (warp + 1) * RW);   // [wa, wb)
     const double* hatd = reinterpret_cast<const double*>(p.hat);
     const size_t rowstride = (size_t)p.Hp * 2;
-    // ---- load the warp's rows: rhs = -omega-hat plus the k = 0 wall terms (poisson.cu:91-95,109-114)
+    // ---- stage the CTA's tile: 16-byte chunks, all in flight (the padding columns kx >= H of
+    //      the spectral buffer and of cp hold zeros, so every chunk is a valid address)
+    for (int ch = threadIdx.x; ch < nr * 16; ch += blockDim.x) {
+        const int rr = ch >> 4, cc = (ch & 15) * 2;
+        cp_async16(&data[(size_t)rr * 32 + cc], &hatd[(size_t)(r0 + rr + 1) * rowstride + (size_t)g * 32 + cc]);
+    }
+    for (int ch = threadIdx.x; ch < nr * 8; ch += blockDim.x) {
+        const int rr = ch >> 3, cc = (ch & 7) * 2;
+        cp_async16(&cpv[(size_t)rr * 16 + cc], &p.cp[(size_t)(r0 + rr) * p.Hp + (size_t)g * 16 + cc]);
+    }
+    for (int rr = threadIdx.x; rr < nr; rr += blockDim.x) {
+        sasub[rr] = p.asub[r0 + rr + 1];
+        sinvc[rr] = p.inv_csup[r0 + rr + 1];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // ---- phase 1: local forward elimination, dp_j = alpha_j r_j + beta_j dp_{j-1}, with
+    //      r_j = -omega-hat_j plus the k = 0 wall terms (poisson.cu:91-95,109-114),
+    //      alpha_j = 1/den_j = cp_j / csup_j, beta_j = -asub_j alpha_j (poisson.cu:97-119)
+    double d = 0.0, P = 1.0;
+#pragma unroll 4
     for (int r = wa; r < wb; ++r) {
-        const int jrow = r + 1;
-        double v = valid ? -hatd[(size_t)jrow * rowstride + (size_t)g * 32 + lane] : 0.0;
+        const int jrow = r + 1, rr = r - r0;
+        double v = -data[(size_t)rr * 32 + lane];
         if (kx == 0 && part == 0) {
             if (jrow == 1) v -= p.asub[1] * p.psi_bot * (double)p.Nx;
             if (jrow == p.Ny - 2) v -= p.csup[p.Ny - 2] * p.psi_top * (double)p.Nx;
         }
-        data[(size_t)(r - r0) * 32 + lane] = v;
-        if (lane < 16) {
-            const int kk = g * 16 + lane;
-            cpv[(size_t)(r - r0) * 16 + lane] = (kk < p.H) ? p.cp[(size_t)r * p.Hp + kk] : 0.0;
-        }
-    }
-    __syncwarp();
-    // ---- phase 1: local forward elimination, dp_j = alpha_j r_j + beta_j dp_{j-1}
-    //      alpha_j = 1/den_j = cp_j / csup_j, beta_j = -asub_j alpha_j (poisson.cu:97-119)
-    double d = 0.0, P = 1.0;
-    for (int r = wa; r < wb; ++r) {
-        const int jrow = r + 1;
-        const double cpj = cpv[(size_t)(r - r0) * 16 + (lane >> 1)];
-        const double alpha = cpj * __ldg(&p.inv_csup[jrow]);
-        const double beta = -__ldg(&p.asub[jrow]) * alpha;
-        d = alpha * data[(size_t)(r - r0) * 32 + lane] + beta * d;
+        const double alpha = cpv[(size_t)rr * 16 + (lane >> 1)] * sinvc[rr];
+        const double beta = -sasub[rr] * alpha;
+        d = alpha * v + beta * d;
         P = beta * P;
-        data[(size_t)(r - r0) * 32 + lane] = d;
+        data[(size_t)rr * 32 + lane] = d;
     }
     aggP[warp * 32 + lane] = P;
     aggD[warp * 32 + lane] = d;
@@ -235,32 +468,36 @@ static __global__ void __launch_bounds__(KT_NW * 32) k_thomas(ThomasParams p) {
         ctaF[32 + lane] = cD;
     }
     cluster.sync();
-    // incoming carry of this CTA: compose the maps of the lower-ranked CTAs
-    double c = 0.0;
-    for (int qq = 0; qq < q; ++qq) {
-        const double* rf = cluster.map_shared_rank(ctaF, qq);
-        c = rf[32 + lane] + rf[lane] * c;
+    // gather the maps of all CTAs of the cluster in one parallel pass over DSMEM
+    for (int idx = threadIdx.x; idx < C * 64; idx += blockDim.x) {
+        const int qq = idx >> 6;
+        allc[idx] = cluster.map_shared_rank(ctaF, qq)[idx & 63];
     }
+    __syncthreads();
+    // incoming carry of this warp: the maps of the lower-ranked CTAs, then of the lower warps
+    double c = 0.0;
+    for (int qq = 0; qq < q; ++qq) c = allc[qq * 64 + 32 + lane] + allc[qq * 64 + lane] * c;
     for (int w = 0; w < warp; ++w) c = aggD[w * 32 + lane] + aggP[w * 32 + lane] * c;
     // ---- phase 2: dp_j = dtilde_j + P_j c
     P = 1.0;
+#pragma unroll 4
     for (int r = wa; r < wb; ++r) {
-        const int jrow = r + 1;
-        const double cpj = cpv[(size_t)(r - r0) * 16 + (lane >> 1)];
-        const double alpha = cpj * __ldg(&p.inv_csup[jrow]);
-        const double beta = -__ldg(&p.asub[jrow]) * alpha;
-        P = beta * P;
-        data[(size_t)(r - r0) * 32 + lane] += P * c;
+        const int rr = r - r0;
+        const double alpha = cpv[(size_t)rr * 16 + (lane >> 1)] * sinvc[rr];
+        P = (-sasub[rr] * alpha) * P;
+        data[(size_t)rr * 32 + lane] += P * c;
     }
     // ---- phase 3: local back substitution x_j = dp_j - cp_j x_{j+1} (poisson.cu:121-129)
     double x = 0.0, Q = 1.0;
+#pragma unroll 4
     for (int r = wb - 1; r >= wa; --r) {
-        const double cpj = cpv[(size_t)(r - r0) * 16 + (lane >> 1)];
-        x = data[(size_t)(r - r0) * 32 + lane] - cpj * x;
+        const int rr = r - r0;
+        const double cpj = cpv[(size_t)rr * 16 + (lane >> 1)];
+        x = data[(size_t)rr * 32 + lane] - cpj * x;
         Q = -cpj * Q;
-        data[(size_t)(r - r0) * 32 + lane] = x;
+        data[(size_t)rr * 32 + lane] = x;
     }
-    __syncthreads();                                   // phase-1 aggregates no longer needed
+    __syncthreads();                                   // forward maps no longer needed
     aggP[warp * 32 + lane] = Q;
     aggD[warp * 32 + lane] = x;
     __syncthreads();
@@ -275,87 +512,45 @@ static __global__ void __launch_bounds__(KT_NW * 32) k_thomas(ThomasParams p) {
         ctaB[32 + lane] = cX;
     }
     cluster.sync();
-    double X = 0.0;                                    // x at the row above this CTA
-    for (int qq = p.C - 1; qq > q; --qq) {
-        const double* rb = cluster.map_shared_rank(ctaB, qq);
-        X = rb[32 + lane] + rb[lane] * X;
+    for (int idx = threadIdx.x; idx < C * 64; idx += blockDim.x) {
+        const int qq = idx >> 6;
+        allc[idx] = cluster.map_shared_rank(ctaB, qq)[idx & 63];
     }
+    __syncthreads();
+    double X = 0.0;                                    // x at the row above this warp
+    for (int qq = C - 1; qq > q; --qq) X = allc[qq * 64 + 32 + lane] + allc[qq * 64 + lane] * X;
     for (int w = KT_NW - 1; w > warp; --w) X = aggD[w * 32 + lane] + aggP[w * 32 + lane] * X;
     // ---- phase 4: x_j = xtilde_j + Q_j X, Q_j = prod_{i=j}^{top} (-cp_i); store psi-hat
     double* hatw = reinterpret_cast<double*>(p.hat);
     Q = 1.0;
+#pragma unroll 4
     for (int r = wb - 1; r >= wa; --r) {
-        const double cpj = cpv[(size_t)(r - r0) * 16 + (lane >> 1)];
-        Q = -cpj * Q;
-        const double xv = data[(size_t)(r - r0) * 32 + lane] + Q * X;
+        const int rr = r - r0;
+        Q = -cpv[(size_t)rr * 16 + (lane >> 1)] * Q;
+        const double xv = data[(size_t)rr * 32 + lane] + Q * X;
         if (valid) hatw[(size_t)(r + 1) * rowstride + (size_t)g * 32 + lane] = xv;
     }
     // wall rows of psi-hat: Nx psi_bot / Nx psi_top at kx = 0, else 0 (poisson.cu:130-132)
     if (warp == 0 && valid) {
         if (q == 0) hatw[(size_t)g * 32 + lane] = (kx == 0 && part == 0) ? (double)p.Nx * p.psi_bot : 0.0;
-        if (q == p.C - 1)
+        if (q == C - 1)
             hatw[(size_t)(p.Ny - 1) * rowstride + (size_t)g * 32 + lane] =
                 (kx == 0 && part == 0) ? (double)p.Nx * p.psi_top : 0.0;
     }
     cluster.sync();                                    // keep smem alive for remote readers
 }
 
-struct IfftParams {
-    const cpx<double>* hat;
-    double* psi;
-    const cpx<double>* tw;
-    const cpx<double>* wN;
-    int Nx, Ny, M, Hp, rows_per_cta;
-    double psi_bot, psi_top;
-};
-
-static __global__ void __launch_bounds__(256) k_ifft(IfftParams p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int M = p.M, Nx = p.Nx;
-    cpx<double>* bufA = reinterpret_cast<cpx<double>*>(smem_raw);
-    cpx<double>* bufB = bufA + padded_size(M);
-    const int j0 = blockIdx.x * p.rows_per_cta;
-    const int j1 = min(p.Ny, j0 + p.rows_per_cta);
-    const double scale = 1.0 / (double)M;
-    for (int j = j0; j < j1; ++j) {
-        double* dst = p.psi + (size_t)j * Nx;
-        if (j == 0 || j == p.Ny - 1) {
-            const double v = (j == 0) ? p.psi_bot : p.psi_top;
-            for (int i = threadIdx.x; i < Nx; i += blockDim.x) dst[i] = v;
-            continue;
-        }
-        const cpx<double>* src = p.hat + (size_t)j * p.Hp;
-        for (int k = threadIdx.x; k <= M; k += blockDim.x) bufB[k] = src[k];
-        __syncthreads();
-        for (int k = threadIdx.x; k < M; k += blockDim.x) bufA[pad_idx(k)] = irfft_merge(k, M, bufB, p.wN);
-        __syncthreads();
-        cpx<double>* in = bufA;
-        cpx<double>* out = bufB;
-        cta_fft<true>(in, out, M, p.tw);
-        for (int n = threadIdx.x; n < M; n += blockDim.x) {
-            const cpx<double> z = in[pad_idx(n)];
-            reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
-        }
-        __syncthreads();
-    }
-}
-
-// Thom wall vorticity (src/ops.cu:102-158); with closure_diag also the wall-row enstrophy
-// jump of this stage (src/main.cu:271-298), accumulated into ctl->jwall[stage-1].
+// Thom wall vorticity alone (the reference's launcher, src/ops.cu:102-158,270-276).
 struct ThomParams {
     double* w;
     const double* psi;
     const double* dy_edge;
-    const double* w_node;
-    Ctl* ctl;
-    int Nx, Ny, free_slip, closure, stage;
-    double psi_bot, psi_top, invA_full;
+    int Nx, Ny, free_slip;
+    double psi_bot, psi_top;
 };
 
 static __global__ void __launch_bounds__(256) k_thom(ThomParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
-    double sb = 0.0, sa = 0.0;
-    const double wq_b = p.closure ? p.w_node[0] : 0.0, wq_t = p.closure ? p.w_node[Ny - 1] : 0.0;
     const double b1 = p.dy_edge[0], b2 = p.dy_edge[1];
     const double Ab = 2.0 * (1.0 / (b1 * b1) + 1.0 / (b1 * b2));
     const double Bb = (-2.0) * b1 / (b2 * (b1 + b2) * (b1 + b2));
@@ -363,39 +558,17 @@ static __global__ void __launch_bounds__(256) k_thom(ThomParams p) {
     const double At = 2.0 * (1.0 / (t1 * t1) + 1.0 / (t1 * t2));
     const double Bt = (-2.0) * t1 / (t2 * (t1 + t2) * (t1 + t2));
     double* wt = p.w + (size_t)(Ny - 1) * Nx;
-    // one CTA when closure sums are wanted (the reduction below is CTA-local)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Nx; i += gridDim.x * blockDim.x) {
-        const double ob = p.w[i], ot = wt[i];
-        double nb, nt;
-        if (p.free_slip) {
-            nb = 0.0; nt = 0.0;
-        } else {
-            const double d1 = p.psi[(size_t)1 * Nx + i] - p.psi_bot, d2 = p.psi[(size_t)2 * Nx + i] - p.psi_bot;
-            nb = -(Ab * d1 + Bb * d2);
-            const double e1 = p.psi[(size_t)(Ny - 2) * Nx + i] - p.psi_top, e2 = p.psi[(size_t)(Ny - 3) * Nx + i] - p.psi_top;
-            nt = -(At * e1 + Bt * e2);
-        }
-        p.w[i] = nb;
-        wt[i] = nt;
-        if (p.closure) {
-            sb += wq_b * ob * ob + wq_t * ot * ot;
-            sa += wq_b * nb * nb + wq_t * nt * nt;
-        }
+        if (p.free_slip) { p.w[i] = 0.0; wt[i] = 0.0; continue; }
+        const double d1 = p.psi[(size_t)1 * Nx + i] - p.psi_bot, d2 = p.psi[(size_t)2 * Nx + i] - p.psi_bot;
+        p.w[i] = -(Ab * d1 + Bb * d2);
+        const double e1 = p.psi[(size_t)(Ny - 2) * Nx + i] - p.psi_top, e2 = p.psi[(size_t)(Ny - 3) * Nx + i] - p.psi_top;
+        wt[i] = -(At * e1 + Bt * e2);
     }
-    if (!p.closure) return;
-    __shared__ double rb[256], ra[256];
-    rb[threadIdx.x] = sb; ra[threadIdx.x] = sa;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) { rb[threadIdx.x] += rb[threadIdx.x + s]; ra[threadIdx.x] += ra[threadIdx.x + s]; }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        p.ctl->jwall[p.stage - 1] += 0.5 * ra[0] * p.invA_full - 0.5 * rb[0] * p.invA_full;
 }
 
-// max |u|, |v|, |v| a over the interior (src/diag.cu:702-816) and, in the last block, the
-// adaptive time step with output trimming (src/main.cu:439-480).
+// max |u|, |v|, |v| a over the interior (src/diag.cu:702-816), one row at a time per CTA,
+// and, in the last block, the adaptive time step with output trimming (src/main.cu:439-480).
 struct MaxParams {
     const double* psi;
     const double* a_node;
@@ -405,24 +578,38 @@ struct MaxParams {
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
-__device__ __forceinline__ double time_tol_d(double t) { return 64.0 * 2.220446049250313e-16 * fmax(1.0, fabs(t)); }
-
 static __global__ void __launch_bounds__(256) k_maxuv_dt(MaxParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
     double um = 0.0, vm = 0.0, vmm = 0.0;
     int nonfinite = 0;
-    const size_t total = (size_t)Nx * (size_t)(Ny - 2);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int j = 1 + (int)(q / Nx);
-        const int i = (int)(q - (size_t)(j - 1) * Nx);
-        const int ip = (i + 1 < Nx) ? i + 1 : 0, im = (i > 0) ? i - 1 : Nx - 1;
-        const double dpsideta = (p.psi[(size_t)(j + 1) * Nx + i] - p.psi[(size_t)(j - 1) * Nx + i]) * (0.5 * p.inv_deta);
-        const double dpsidx = (p.psi[(size_t)j * Nx + ip] - p.psi[(size_t)j * Nx + im]) * (0.5 * p.inv_dx);
+    constexpr int U = 4;                       // independent points per thread and iteration
+    for (int j = 1 + blockIdx.x; j < Ny - 1; j += gridDim.x) {
         const double a = __ldg(&p.a_node[j]);
-        const double u = a * dpsideta, v = -dpsidx;
-        const double au = fabs(u), av = fabs(v), avm = av * a;
-        if (!(au <= 1e300) || !(av <= 1e300)) nonfinite = 1;
-        um = fmax(um, au); vm = fmax(vm, av); vmm = fmax(vmm, avm);
+        const double* rm = p.psi + (size_t)(j - 1) * Nx;
+        const double* r0 = p.psi + (size_t)j * Nx;
+        const double* rp = p.psi + (size_t)(j + 1) * Nx;
+        for (int i0 = threadIdx.x; i0 < Nx; i0 += U * blockDim.x) {
+            double up[U], dn[U], xp[U], xm[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < Nx) {
+                    const int ip = (i + 1 < Nx) ? i + 1 : 0, im = (i > 0) ? i - 1 : Nx - 1;
+                    up[u] = __ldg(&rp[i]); dn[u] = __ldg(&rm[i]); xp[u] = __ldg(&r0[ip]); xm[u] = __ldg(&r0[im]);
+                } else {
+                    up[u] = dn[u] = xp[u] = xm[u] = 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double dpsideta = (up[u] - dn[u]) * (0.5 * p.inv_deta);
+                const double dpsidx = (xp[u] - xm[u]) * (0.5 * p.inv_dx);
+                const double uu = a * dpsideta, v = -dpsidx;
+                const double au = fabs(uu), av = fabs(v), avm = av * a;
+                if (!(au <= 1e300) || !(av <= 1e300)) nonfinite = 1;
+                um = fmax(um, au); vm = fmax(vm, av); vmm = fmax(vmm, avm);
+            }
+        }
     }
     __shared__ double s[3][256];
     __shared__ int snf;
@@ -477,19 +664,6 @@ static __global__ void __launch_bounds__(256) k_maxuv_dt(MaxParams p) {
         if (rem > tol && rem < 0.5 * dt) dt = rem;
     }
     ctl->dt = dt;
-}
-
-// t += dt, step++, and the snap to the scheduled output times (src/main.cu:541-551): the
-// tolerance is re-evaluated after the first snap, as the reference does.
-static __global__ void k_advance_time(Ctl* ctl) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double dt = ctl->dt;
-    double t = ctl->t + dt;
-    const double ns = ctl->next_snap, nd = ctl->next_diag;
-    if (ns < 1e299 && fabs(t - ns) <= fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)))) t = ns;
-    if (nd < 1e299 && fabs(t - nd) <= fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)))) t = nd;
-    ctl->t = t;
-    ctl->step += 1;
 }
 
 }  // namespace nse2d
