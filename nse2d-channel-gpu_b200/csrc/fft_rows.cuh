@@ -1,13 +1,6 @@
-// Compile-time-sized shared-memory FFT of one row by a whole CTA (NT threads).
-// Written for this project; the pass formula is the Stockham auto-sort form documented in
-// fft.cuh. With M a template constant every index is a shift or a mask, the pass schedule
-// unrolls, and the first pass reads an unpadded buffer (its stride-M/R reads are already
-// conflict free), so a row can be staged into that buffer with plain vector loads.
-//
-// Buffers: A = M elements unpadded, B = padded_size(M) elements. Pass p reads the buffer
-// written by pass p-1 (A for p = 0) and writes B when p is even, A when p is odd. Only the
-// first pass (sub-transform length 1, stride-R stores) needs the padded layout; later
-// passes store runs of at least 8 consecutive elements per 8 lanes.
+// Compile-time-sized shared-memory FFT of one row by a whole CTA (NT threads), written for
+// this project. With M a template constant every index is a shift or a mask and the pass
+// schedule unrolls.
 #pragma once
 #include "fft.cuh"
 
@@ -15,8 +8,6 @@ namespace nse2d {
 
 template <int X> struct ilog2 { static constexpr int v = 1 + ilog2<X / 2>::v; };
 template <> struct ilog2<1> { static constexpr int v = 0; };
-
-template <bool PAD> __device__ __forceinline__ int bidx(int i) { return PAD ? pad_idx(i) : i; }
 
 // twiddle load through the read-only path
 __device__ __forceinline__ cpx<double> ldtw(const cpx<double>* tw, int i) {
@@ -28,68 +19,7 @@ __device__ __forceinline__ cpx<float> ldtw(const cpx<float>* tw, int i) {
     return {v.x, v.y};
 }
 
-template <typename T, int M, int R, int NS, bool INV, bool IN_PAD, bool OUT_PAD, int NT>
-__device__ __forceinline__ void fft_pass(const cpx<T>* __restrict__ in, cpx<T>* __restrict__ out,
-                                         const cpx<T>* __restrict__ tw) {
-    constexpr int NB = M / R;
-    constexpr int STRIDE = M / R;
-    constexpr int TSTEP = M / (NS * R);
-#pragma unroll
-    for (int j0 = 0; j0 < NB; j0 += NT) {
-        const int j = j0 + (int)threadIdx.x;
-        if (NB % NT != 0 && j >= NB) break;
-        const int k = j & (NS - 1);
-        cpx<T> v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = in[bidx<IN_PAD>(j + r * STRIDE)];
-        if (NS > 1 && k > 0) {
-            // w^r for r = 1..R-1 from two table loads (w and w^4 for radix 8): a few complex
-            // products instead of R-1 dependent loads
-            cpx<T> wp[R];
-            wp[1] = ldtw(tw, (TSTEP * k) & (M - 1));
-            if constexpr (R >= 4) {
-                wp[2] = cmul(wp[1], wp[1]);
-                wp[3] = cmul(wp[2], wp[1]);
-            }
-            if constexpr (R == 8) {
-                wp[4] = ldtw(tw, (4 * TSTEP * k) & (M - 1));
-                wp[5] = cmul(wp[4], wp[1]);
-                wp[6] = cmul(wp[4], wp[2]);
-                wp[7] = cmul(wp[4], wp[3]);
-            }
-#pragma unroll
-            for (int r = 1; r < R; ++r) v[r] = INV ? cmulc(v[r], wp[r]) : cmul(v[r], wp[r]);
-        }
-        dftR<T, R, INV>(v);
-        const int base = (j - k) * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[bidx<OUT_PAD>(base + r * NS)] = v[r];
-    }
-}
-
-// All passes: radix-8 while 8 divides the remaining length, then a radix-4 or radix-2 pass.
-// Returns (through the template recursion) the parity of the pass count: the result lies in
-// B when the number of passes is odd, in A when it is even.
-// in0: the unpadded input of pass 0 (may be A itself, or a separate staging buffer that is
-// free again once pass 0 is done, so that the next row can be loaded into it meanwhile).
-// on_pass0_done() runs right after the barrier that ends pass 0.
-template <typename T, int M, int NS, int P, bool INV, int NT, typename F>
-__device__ __forceinline__ void fft_passes(const cpx<T>* in0, cpx<T>* A, cpx<T>* B, const cpx<T>* tw,
-                                           F&& on_pass0_done) {
-    if constexpr (NS < M) {
-        constexpr int REM = M / NS;
-        constexpr int R = (REM % 8 == 0) ? 8 : REM;   // REM is 4 or 2 in the last pass
-        constexpr bool IN_PAD = (P % 2 == 1);         // pass P reads what pass P-1 wrote
-        constexpr bool OUT_PAD = (P % 2 == 0);
-        const cpx<T>* in = (P == 0) ? in0 : ((P % 2 == 0) ? A : B);
-        cpx<T>* out = (P % 2 == 0) ? B : A;
-        fft_pass<T, M, R, NS, INV, IN_PAD, OUT_PAD, NT>(in, out, tw);
-        __syncthreads();
-        if constexpr (P == 0) on_pass0_done();
-        fft_passes<T, M, NS * R, P + 1, INV, NT>(in0, A, B, tw, on_pass0_done);
-    }
-}
-
+// Number of passes of an M-point transform: radix 8 while 8 divides what is left, then 4 or 2.
 template <int M> struct fft_npass {
     template <int NS> static constexpr int count() {
         if constexpr (NS >= M) return 0;
@@ -102,7 +32,90 @@ template <int M> struct fft_npass {
     static constexpr int v = count<1>();
 };
 
-// Result buffer of an M-point transform run by fft_passes: B (padded) if the pass count is odd.
-template <int M> struct fft_out { static constexpr bool in_B = (fft_npass<M>::v % 2) == 1; };
+// ---------------------------------------------------------------------------------------
+// In-place decimation-in-time FFT of M points in ONE shared buffer.
+//
+// Pass p (radix R_p, sub-transform length L' = R_0 ... R_{p-1} before it, L = R_p L'):
+//   for every group g (start g L) and m in [0, L'):  x_r = buf[g L + m + r L'] * W_L^{r m},
+//   y = DFT_R(x), buf[g L + m + s L'] = y_s.
+// The input must sit in mixed-radix digit-reversed order: element n of the sequence goes to
+// position dit_pos(n); the output is then in natural order. With the radix list
+// (R_0, .., R_{P-1}) written most-significant-last, position p = sum d_q (R_0..R_{q-1})
+// holds element n = d_{P-1} + R_{P-1} (d_{P-2} + R_{P-2} (...)). Radices: 8 while 8 divides
+// what is left, then one 4 or 2.
+//
+// Shared-memory layout: ip_idx(i) = i + i/8 + i/512 (16-byte units) spreads the stride-8 and
+// stride-512 accesses of the first pass and of the digit-reversed scatter over the banks.
+// ---------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int ip_idx(int i) { return i + (i >> 3) + (i >> 9); }
+__host__ __device__ constexpr int ip_size(int M) { return M + (M >> 3) + (M >> 9) + 1; }
+
+// Radices are powers of two, so digits are bit groups: pass q has 3 bits (radix 8) except a
+// last pass of 1 or 2 bits. Digit d_q sits at bit offset 3q of the position p and is taken from
+// n starting at its least significant end in the order q = P-1, P-2, ..., 0.
+template <int M> struct ip_plan {
+    static constexpr int m = ilog2<M>::v;
+    static constexpr int P = fft_npass<M>::v;
+    static constexpr int bits(int q) { return (q < m / 3) ? 3 : m % 3; }
+};
+
+template <int M> __host__ __device__ __forceinline__ int dit_pos(int n) {
+    constexpr int P = ip_plan<M>::P;
+    int p = 0, sn = 0;
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q) {
+        const int b = ip_plan<M>::bits(q);
+        p |= ((n >> sn) & ((1 << b) - 1)) << (3 * q);
+        sn += b;
+    }
+    return p;
+}
+
+template <typename T, int M, int R, int LP, bool INV, int NT>
+__device__ __forceinline__ void ip_pass(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw) {
+    constexpr int NB = M / R;            // butterflies
+    constexpr int L = R * LP;
+    constexpr int TSTEP = M / L;         // W_L^{m} = W_M^{m TSTEP}
+#pragma unroll
+    for (int b0 = 0; b0 < NB; b0 += NT) {
+        const int b = b0 + (int)threadIdx.x;
+        if (NB % NT != 0 && b >= NB) break;
+        const int m = b & (LP - 1);
+        const int base = (b - m) * R + m;            // g L + m with g = b / LP
+        cpx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = buf[ip_idx(base + r * LP)];
+        if (LP > 1 && m > 0) {
+            cpx<T> wp[R];
+            wp[1] = ldtw(tw, (TSTEP * m) & (M - 1));
+            if constexpr (R >= 4) {
+                wp[2] = cmul(wp[1], wp[1]);
+                wp[3] = cmul(wp[2], wp[1]);
+            }
+            if constexpr (R == 8) {
+                wp[4] = ldtw(tw, (4 * TSTEP * m) & (M - 1));
+                wp[5] = cmul(wp[4], wp[1]);
+                wp[6] = cmul(wp[4], wp[2]);
+                wp[7] = cmul(wp[4], wp[3]);
+            }
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = INV ? cmulc(v[r], wp[r]) : cmul(v[r], wp[r]);
+        }
+        dftR<T, R, INV>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[ip_idx(base + r * LP)] = v[r];
+    }
+}
+
+template <typename T, int M, int LP, bool INV, int NT>
+__device__ __forceinline__ void ip_passes(cpx<T>* buf, const cpx<T>* tw) {
+    if constexpr (LP < M) {
+        constexpr int REM = M / LP;
+        constexpr int R = (REM % 8 == 0) ? 8 : REM;
+        ip_pass<T, M, R, LP, INV, NT>(buf, tw);
+        __syncthreads();
+        ip_passes<T, M, LP * R, INV, NT>(buf, tw);
+    }
+}
 
 }  // namespace nse2d

@@ -313,11 +313,6 @@ void context_destroy(Context* c) {
 }
 
 // ---- launchers ----
-static int rows_per_cta(int rows, int grid_target) {
-    const int g = std::max(1, std::min(rows, grid_target));
-    return (rows + g - 1) / g;
-}
-
 static StageParams stage_params(Context* c) {
     StageParams p{};
     p.psi = c->psi; p.rt = c->rt; p.ctl = c->ctl;
@@ -339,7 +334,7 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
     return 0;
 }
 
-static size_t fft_smem(int M) { return (size_t)fft_smem_elems(M) * sizeof(cpx<double>); }
+static size_t fft_smem(int M) { return fft_smem_bytes(M); }
 
 static FftParams fft_params(Context* c) {
     FftParams p{};
@@ -349,22 +344,24 @@ static FftParams fft_params(Context* c) {
     return p;
 }
 
+// Forward transforms: one row per CTA (many small CTAs per SM hide each other's load latency).
 template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) {
     const size_t sm = fft_smem(M);
     NSE_CUDA_TRY(cudaFuncSetAttribute(k_fft_fwd<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    p.rows_per_cta = rows_per_cta(c->Ni, 3 * c->num_sms);
-    const int grid = (c->Ni + p.rows_per_cta - 1) / p.rows_per_cta;
-    k_fft_fwd<M><<<grid, FFT_NT, sm, s>>>(p);
+    p.rows_per_cta = 1;
+    k_fft_fwd<M><<<c->Ni, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
+// Inverse transforms: bands of at least 3 rows (the Thom closure needs rows 1-2 and Ny-3..Ny-2
+// in one CTA each).
 template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
     const size_t sm = fft_smem(M);
     NSE_CUDA_TRY(cudaFuncSetAttribute(k_ifft_thom<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    p.rows_per_cta = std::max(3, rows_per_cta(c->Ny, 3 * c->num_sms));
+    p.rows_per_cta = 3;
     const int grid = std::max(1, c->Ny / p.rows_per_cta);   // the last band takes the remainder
-    k_ifft_thom<M><<<grid, FFT_NT, sm, s>>>(p);
+    k_ifft_thom<M><<<grid, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -208,7 +208,6 @@ struct FftParams {
     double psi_bot, psi_top, invA_full;
 };
 
-constexpr int FFT_NT = 256;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -216,40 +215,34 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Shared memory of the row FFT kernels: S (staging, M + 8 entries, unpadded), A (M, unpadded)
-// and B (padded_size(M)).
-__host__ __device__ constexpr int fft_smem_elems(int M) { return (M + 8) + M + (M + (M >> 3) + 1); }
+// Row FFT kernels: one CTA of IP_NT threads transforms one row at a time in ONE shared buffer
+// (in-place decimation-in-time passes, fft_rows.cuh), so that 5 CTAs fit on an SM and the
+// load latency of one row is hidden behind the passes of the others.
+constexpr int IP_NT = 128;
+__host__ __device__ constexpr size_t fft_smem_bytes(int M) { return (size_t)ip_size(M) * 16; }
 
 // Forward real FFT of rows 1..Ny-2 (the reference's pack + cuFFT forward, src/poisson.cuh:93-96):
-// a row is read as M complex points z_n = x_2n + i x_2n+1 into S by cp.async; pass 0 reads S,
-// after which the next row is loaded into S while the remaining passes run; the split step
-// then writes X_k, k = 0..M.
+// a row is read as M complex points z_n = x_2n + i x_2n+1, scattered by cp.async into the
+// digit-reversed layout; after the passes the split step writes X_k, k = 0..M:
+//   E_k = (Z_k + conj Z_{M-k}) / 2,  O_k = -i (Z_k - conj Z_{M-k}) / 2,  X_k = E_k + W_{2M}^k O_k.
 template <int M>
-static __global__ void __launch_bounds__(FFT_NT, 2) k_fft_fwd(FftParams p) {
+static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<double>* S = reinterpret_cast<cpx<double>*>(smem_raw);
-    cpx<double>* A = S + (M + 8);
-    cpx<double>* B = A + M;
-    constexpr bool OUTB = fft_out<M>::in_B;
+    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const int jb = 1 + blockIdx.x * p.rows_per_cta;
     const int je = min(p.Ny - 1, jb + p.rows_per_cta);
-    auto stage_row = [&](int j) {
-        const cpx<double>* row = reinterpret_cast<const cpx<double>*>(p.src + (size_t)j * p.Nx);
-        for (int n = threadIdx.x; n < M; n += FFT_NT) cp_async16(&S[n], &row[n]);
-    };
-    if (jb < je) stage_row(jb);
     for (int j = jb; j < je; ++j) {
+        const cpx<double>* row = reinterpret_cast<const cpx<double>*>(p.src + (size_t)j * p.Nx);
+        for (int n = threadIdx.x; n < M; n += IP_NT) cp_async16(&buf[ip_idx(dit_pos<M>(n))], &row[n]);
         cp_async_wait_all();
         __syncthreads();
-        fft_passes<double, M, 1, 0, false, FFT_NT>(S, A, B, p.tw, [&]() {
-            if (j + 1 < je) stage_row(j + 1);
-        });
-        const cpx<double>* Z = OUTB ? B : A;
+        ip_passes<double, M, 1, false, IP_NT>(buf, p.tw);
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-        for (int k = threadIdx.x; k <= M; k += FFT_NT) {
+#pragma unroll 4
+        for (int k = threadIdx.x; k <= M; k += IP_NT) {
             const int ka = (k == M ? 0 : k), kb = (k == 0 ? 0 : M - k);
-            const cpx<double> a = Z[OUTB ? pad_idx(ka) : ka];
-            const cpx<double> b0 = Z[OUTB ? pad_idx(kb) : kb];
+            const cpx<double> a = buf[ip_idx(ka)];
+            const cpx<double> b0 = buf[ip_idx(kb)];
             const cpx<double> b = {b0.x, -b0.y};
             const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
             const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
@@ -262,6 +255,7 @@ static __global__ void __launch_bounds__(FFT_NT, 2) k_fft_fwd(FftParams p) {
 
 // Thom wall vorticity of one wall (src/ops.cu:114-151) from the psi rows this CTA just wrote,
 // with the closure_diag enstrophy jump of the wall row (src/main.cu:271-298).
+template <int NT>
 __device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
     const int Nx = p.Nx, Ny = p.Ny;
     const double d1 = top ? p.dy_edge[Ny - 2] : p.dy_edge[0];
@@ -274,7 +268,7 @@ __device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
     double* wr = p.w + (size_t)(top ? Ny - 1 : 0) * Nx;
     const double wq = p.closure ? p.w_node[top ? Ny - 1 : 0] : 0.0;
     double sb = 0.0, sa = 0.0;
-    for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
+    for (int i = threadIdx.x; i < Nx; i += NT) {
         double nv = 0.0;
         if (!p.free_slip) nv = -(A * (__ldcg(&r1[i]) - pw) + B * (__ldcg(&r2[i]) - pw));
         const double ov = wr[i];
@@ -283,10 +277,10 @@ __device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
         sa += wq * nv * nv;
     }
     if (!p.closure) return;
-    __shared__ double rb[FFT_NT], ra[FFT_NT];
+    __shared__ double rb[NT], ra[NT];
     rb[threadIdx.x] = sb; ra[threadIdx.x] = sa;
     __syncthreads();
-    for (int s = FFT_NT / 2; s > 0; s >>= 1) {
+    for (int s = NT / 2; s > 0; s >>= 1) {
         if ((int)threadIdx.x < s) { rb[threadIdx.x] += rb[threadIdx.x + s]; ra[threadIdx.x] += ra[threadIdx.x + s]; }
         __syncthreads();
     }
@@ -301,56 +295,46 @@ __host__ __device__ __forceinline__ void band_of(int b, int nb, int L, int Ny, i
     j1 = (b == nb - 1) ? Ny : min(Ny, (b + 1) * L);
 }
 
-// Inverse real FFT of every row (the reference's cuFFT inverse + scale, src/poisson.cuh:110-114)
-// and the Thom closure of omega^(s+1) by the first and the last CTA. The half spectrum of a
-// row is staged into S by cp.async; after the merge step S is free and the next row is
-// loaded into it while the passes run.
+// Inverse real FFT of every row (the reference's cuFFT inverse + scale, src/poisson.cuh:110-114):
+// the merge step forms Z_k = E_k + i O_k, E_k = (X_k + conj X_{M-k}) / 2,
+// O_k = (X_k - conj X_{M-k}) W_{2M}^{-k} / 2, straight from HBM into the digit-reversed layout;
+// the passes give z_n = x_2n + i x_2n+1 (times M). Then the Thom closure of omega^(s+1) by the
+// first and the last CTA, and, in the stage-3 launch, the time advance by the last CTA.
 template <int M>
-static __global__ void __launch_bounds__(FFT_NT, 2) k_ifft_thom(FftParams p) {
+static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<double>* S = reinterpret_cast<cpx<double>*>(smem_raw);
-    cpx<double>* A = S + (M + 8);
-    cpx<double>* B = A + M;
-    constexpr bool OUTB = fft_out<M>::in_B;
+    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const int Nx = p.Nx, Ny = p.Ny;
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr double scale = 1.0 / (double)M;
-    auto stage_row = [&](int j) {
-        const cpx<double>* row = p.hat + (size_t)j * p.Hp;
-        for (int k = threadIdx.x; k <= M; k += FFT_NT) cp_async16(&S[k], &row[k]);
-    };
-    int jn = (j0 < 1) ? 1 : j0;                     // next interior row to stage
-    if (jn < j1 && jn < Ny - 1) stage_row(jn);
     for (int j = j0; j < j1; ++j) {
         double* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {
             const double v = (j == 0) ? p.psi_bot : p.psi_top;
-            for (int i = threadIdx.x; i < Nx; i += FFT_NT) dst[i] = v;
+            for (int i = threadIdx.x; i < Nx; i += IP_NT) dst[i] = v;
             continue;
         }
-        cp_async_wait_all();
-        __syncthreads();
-        for (int k = threadIdx.x; k < M; k += FFT_NT) {
-            const cpx<double> a = S[k], b0 = S[M - k];
-            const cpx<double> b = {b0.x, -b0.y};
+        const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
+#pragma unroll 4
+        for (int k = threadIdx.x; k < M; k += IP_NT) {
+            const double2 av = __ldcs(X + k), bv = __ldcs(X + (M - k));
+            const cpx<double> a = {av.x, av.y}, b = {bv.x, -bv.y};
             const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
             const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
-            A[k] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, k))));
+            buf[ip_idx(dit_pos<M>(k))] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, k))));
         }
         __syncthreads();
-        if (j + 1 < j1 && j + 1 < Ny - 1) stage_row(j + 1);
-        fft_passes<double, M, 1, 0, true, FFT_NT>(A, A, B, p.tw, []() {});
-        const cpx<double>* Z = OUTB ? B : A;
-        for (int n = threadIdx.x; n < M; n += FFT_NT) {
-            const cpx<double> z = Z[OUTB ? pad_idx(n) : n];
+        ip_passes<double, M, 1, true, IP_NT>(buf, p.tw);
+        for (int n = threadIdx.x; n < M; n += IP_NT) {
+            const cpx<double> z = buf[ip_idx(n)];
             reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
         }
         __syncthreads();
     }
     if (p.do_thom) {
-        if (j0 <= 1 && j1 >= 3) thom_row(p, false);
-        if (j0 <= Ny - 3 && j1 >= Ny - 1) thom_row(p, true);
+        if (j0 <= 1 && j1 >= 3) thom_row<IP_NT>(p, false);
+        if (j0 <= Ny - 3 && j1 >= Ny - 1) thom_row<IP_NT>(p, true);
     }
     if (p.advance) {
         // the last CTA to finish advances the time: t += dt and the output snap
