@@ -137,6 +137,21 @@ int  nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, doub
 int  nse2d_poisson_solve(nse2d_ctx* ctx, const double* d_w, double* d_psi, cudaStream_t s);
 /* max |u|, |v|, |v| a of the context's psi (src/diag.cu:821-866). Synchronous. */
 int  nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s);
+/* The same max |u|, |v|, |v| a of a caller-owned psi [Ny][Nx] and a_node [Ny] (device
+ * pointers), without a context and without allocating any device memory. No counterpart in
+ * the reference. It is for callers that may not allocate: code whose device memory is all
+ * handed out by its own pool, or that cannot afford the device-wide synchronisation of a
+ * cudaMalloc/cudaFree pair in its loop. The reduction's scratch is a fixed array inside the
+ * library, room for NSE2D_MAXUV_NOALLOC_MAX_BLOCKS per-CTA partials (24 KiB) plus a small
+ * control block; the launch uses at most that many CTAs, which stride over the rows, so
+ * every Ny fits. Nx must be in [2, 2^30] and Ny >= 3; other sizes are rejected with an error.
+ * The first call on a device (with that device current) looks up the scratch address and
+ * should come before any stream capture on that device. Every call clears the control block
+ * on stream s first. One scratch serves all callers on a device: calls that overlap in time
+ * on the same device race. Synchronous: out3 (host) holds the result on return. */
+#define NSE2D_MAXUV_NOALLOC_MAX_BLOCKS 1024
+int  nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node, int Nx, int Ny,
+                          double inv_dx, double inv_deta, double* out3, cudaStream_t s);
 /* One diagnostics.csv row at the current state, columns umax .. Re_tau (16) followed by
  * the 13 closure_diag columns (nan when not computed), as src/main.cu:566-692
  * (t0_row = 0) or the t = 0 row of src/main.cu:325-421 (t0_row = 1). Synchronous. */

@@ -1,0 +1,107 @@
+// max |u|, |v|, |v| a of a caller-owned streamfunction, computed without allocating device
+// memory. Written for this project; the reference has no such entry point.
+//
+// Who needs it: a caller that already holds psi and the a_node metric on the device but may
+// not allocate, either because its device memory is carved up in advance by its own pool (a
+// solver embedded in a larger code that owns all of HBM), or because it runs under a
+// memory budget where a cudaMalloc/cudaFree pair would synchronise the device and stall
+// its other streams. The context API cannot serve it: nse2d_create allocates the fields and
+// the workspace of the whole time step.
+//
+// How: the reduction kernel is the time step's own k_maxuv_dt (one partial triple per CTA,
+// the last CTA folds them). Its partials and its control block live in g_maxuv_scratch, a
+// fixed file-scope device array, instead of the context's buffers. The first call on a
+// device, with that device current, looks up the array's address with cudaGetSymbolAddress
+// and caches it; that first call should come before any stream capture on the device.
+// Every call clears the control block (the last-CTA counter and the non-finite flag must
+// start at zero) with cudaMemsetAsync. One scratch array serves every caller on a device,
+// so calls that overlap in time on one device, from two streams or two host threads, race.
+#include <cstdio>
+#include <mutex>
+
+#include "nse2d_internal.h"
+#include "step_kernels.cuh"
+#include "../../include/nse2d.h"
+
+namespace nse2d {
+
+namespace {
+constexpr int kMaxUvNoAllocBlocks = NSE2D_MAXUV_NOALLOC_MAX_BLOCKS;
+struct MaxUvScratch {
+    Ctl ctl;                                     // last-CTA counter, non-finite flag, results
+    double blocks[3 * kMaxUvNoAllocBlocks];      // per-CTA partial maxima
+};
+constexpr int kMaxDevices = 64;
+
+struct DeviceSlot {
+    MaxUvScratch* scratch = nullptr;
+    int num_sms = 0;
+};
+std::mutex g_slot_mutex;
+DeviceSlot g_slots[kMaxDevices];
+}  // namespace
+
+static __device__ __align__(256) MaxUvScratch g_maxuv_scratch;
+
+// Address of this device's scratch and its SM count, looked up once per device.
+static int device_slot(DeviceSlot& out) {
+    int dev = -1;
+    NSE_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("nse2d_max_uv_noalloc: device %d outside the %d devices this entry point serves",
+                  dev, kMaxDevices);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lock(g_slot_mutex);
+    DeviceSlot& slot = g_slots[dev];
+    if (!slot.scratch) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_maxuv_scratch);
+        if (e != cudaSuccess || !ptr) {
+            set_error("nse2d_max_uv_noalloc: cudaGetSymbolAddress of the scratch failed on device %d: %s",
+                      dev, cudaGetErrorString(e));
+            return -1;
+        }
+        int sms = 0;
+        NSE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        slot.num_sms = sms > 0 ? sms : 1;
+        slot.scratch = static_cast<MaxUvScratch*>(ptr);
+    }
+    out = slot;
+    return 0;
+}
+
+}  // namespace nse2d
+
+extern "C" int nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node, int Nx, int Ny,
+                                    double inv_dx, double inv_deta, double* out3, cudaStream_t s) {
+    using namespace nse2d;
+    if (!d_psi || !d_a_node || !out3) {
+        set_error("nse2d_max_uv_noalloc: null pointer argument");
+        return -1;
+    }
+    if (Nx < 2 || Ny < 3) {
+        set_error("nse2d_max_uv_noalloc: grid %d x %d too small (need Nx >= 2, Ny >= 3)", Nx, Ny);
+        return -1;
+    }
+    if (Nx > (1 << 30)) {
+        set_error("nse2d_max_uv_noalloc: Nx = %d exceeds the maximum %d (32-bit column index)", Nx, 1 << 30);
+        return -1;
+    }
+    DeviceSlot slot;
+    if (device_slot(slot)) return -1;
+    // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, one partial slot each; the CTAs stride over
+    // the interior rows, so every Ny is covered by that fixed number of slots.
+    const int grid = std::max(1, std::min(std::min(4 * slot.num_sms, Ny - 2), kMaxUvNoAllocBlocks));
+    MaxUvScratch* sc = slot.scratch;
+    NSE_CUDA_TRY(cudaMemsetAsync(&sc->ctl, 0, sizeof(Ctl), s));
+    MaxParams p{};
+    p.psi = d_psi; p.a_node = d_a_node; p.blocks = sc->blocks; p.ctl = &sc->ctl;
+    p.Nx = Nx; p.Ny = Ny; p.adapt = 0; p.set_dt = 0;
+    p.inv_dx = inv_dx; p.inv_deta = inv_deta;
+    k_maxuv_dt<<<grid, 256, 0, s>>>(p);
+    NSE_CUDA_TRY(cudaGetLastError());
+    NSE_CUDA_TRY(cudaMemcpyAsync(out3, &sc->ctl.umax, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}

@@ -80,6 +80,7 @@ def load(path=LIB_PATH):
         "nse2d_get_time": (I, [P, P, P, P, P, P]),
         "nse2d_poisson_solve": (I, [P, P, P, P]),
         "nse2d_max_uv": (I, [P, P, P]),
+        "nse2d_max_uv_noalloc": (I, [P, P, I, I, D, D, P, P]),
         "nse2d_diagnostics": (I, [P, I, P, P]),
         "nse2d_rhs_at_state": (I, [P, D, P]),
         "nse2d_uv": (I, [P, P, P, P]),
@@ -135,6 +136,18 @@ def _stream(s):
     if hasattr(s, "cuda_stream"):
         return ctypes.c_void_p(s.cuda_stream)
     return ctypes.c_void_p(int(s))
+
+
+def max_uv_noalloc(psi_dev, a_node_dev, Nx, Ny, inv_dx, inv_deta, stream=None):
+    """max |u|, |v|, |v| a of a caller-owned psi [Ny, Nx] and a_node [Ny] (CUDA float64)
+    through nse2d_max_uv_noalloc, which allocates no device memory. psi_dev and a_node_dev may
+    also be raw device addresses (int), such as Solver.field_ptr returns."""
+    def dev(a):
+        return ctypes.c_void_p(a) if isinstance(a, int) else _ptr(a)
+    out = (ctypes.c_double * 3)()
+    _check(load().nse2d_max_uv_noalloc(dev(psi_dev), dev(a_node_dev), int(Nx), int(Ny), float(inv_dx),
+                                       float(inv_deta), out, _stream(stream)))
+    return tuple(out)
 
 
 class Solver:
