@@ -103,6 +103,19 @@ def kernel_bytes(name, stage, Nx, Ny):
     return 0
 
 
+def read_traffic(Nx, Ny):
+    """DRAM bytes (read + write) per launch of each kernel from the committed ncu summary of
+    this grid (lines `kernel bytes`), or {} when there is none."""
+    path = os.path.join(ROOT, "profiles", f"traffic_step_{Nx}x{Ny}.txt")
+    out = {}
+    if os.path.isfile(path):
+        for ln in open(path):
+            parts = ln.split()
+            if len(parts) == 2 and not ln.startswith("#"):
+                out[parts[0]] = int(parts[1])
+    return out
+
+
 def hbm_peak():
     try:
         d = json.load(open(MEASURED_PEAKS))
@@ -270,13 +283,7 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": int(a["bytes"] / a["launches"])}
     dom = max(agg, key=lambda k: agg[k]["ms"])
     dk = kernels[dom]
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.isfile(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(dom)
-        except Exception:
-            traffic = None
+    traffic = read_traffic(Nx, Ny).get(dom)
     step_gbs = B_step / (step_ms * 1e-3) / 1e9
     h2d = N * 8 / args.steps + 8 * 3
     d2h = 2 * N * 8 / args.steps + 128
