@@ -8,7 +8,7 @@ seeded (seed 1) random vorticity over streamwise modes 1-64 of amplitude 0.05 Ub
 the walls (see initial_vorticity()).
 
 One "step" = one SSPRK(3,3) step: device-side adaptive dt, three stages of (stage + forward FFT,
-cluster Thomas solve, inverse FFT, Thom closure), time advance.
+segmented Thomas solve, inverse FFT, Thom closure), time advance.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -94,8 +94,11 @@ def kernel_bytes(name, stage, Nx, Ny):
         return 8 * N * (2 if stage == 1 else 3) + 8 * N          # psi, omega^(s) [, omega^n] -> omega^(s+1)
     if name == "k_fft_fwd":
         return 8 * Nx * Ni + 16 * H * Ni                         # omega^(s+1) rows -> omega-hat
-    if name == "k_thomas":
-        return 16 * H * Ni * 2 + 8 * H * Ni                      # omega-hat, cp -> psi-hat
+    if name == "k_thomas_maps":
+        return 16 * H * Ni + 8 * H * Ni                          # omega-hat, cp read once
+    if name == "k_thomas_apply":
+        return 16 * H * Ni                                       # psi-hat written (its re-read of
+                                                                 # omega-hat and cp is not counted)
     if name == "k_ifft_thom":
         return 16 * H * Ni + 8 * N + 8 * 6 * Nx                  # psi-hat -> psi, + Thom rows
     if name == "k_maxuv_dt":

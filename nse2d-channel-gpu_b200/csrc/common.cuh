@@ -106,8 +106,13 @@ struct Context {
     // launch shapes
     int fft_threads = 256;
     int stage_grid = 0, ifft_grid = 0;
-    int thomas_C = 1, thomas_R = 0, thomas_groups = 0;
-    size_t thomas_smem = 0;
+    // segmented Thomas solve: 16-column groups, segments of TS_ROWS rows, blocks of TS_NW segments (one CTA)
+    int thomas_groups = 0, thomas_nseg = 0, thomas_nsb = 0;
+    double* tconst = nullptr;      // [nseg][3][Hp] segment products P, V, Q
+    double* tmaps = nullptr;       // [nseg][2][2 Hp] segment maps D, U
+    double* tblk = nullptr;        // [groups][nsb][5][32] block aggregates
+    double* tbcarry = nullptr;     // [groups][nsb][2][32] block carries c, X
+    unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
     int num_sms = 0;
     cudaStream_t cap_stream = nullptr;     // private stream used only for graph capture
     cudaGraphExec_t graph_exec = nullptr;  // one captured step

@@ -59,6 +59,16 @@ int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>
     return 0;
 }
 
+static ThomasParams thomas_params(const Context* c) {
+    ThomasParams p{};
+    p.hat = c->hat; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
+    p.tconst = c->tconst; p.tmaps = c->tmaps; p.tblk = c->tblk; p.tbcarry = c->tbcarry; p.tcount = c->tcount;
+    p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni;
+    p.nseg = c->thomas_nseg; p.nsb = c->thomas_nsb;
+    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
+    return p;
+}
+
 // ---- device setup kernels ----
 // Elimination table, one thread per kx: src/poisson.cu:16-22 (kx^2) and :38-68 (cp), the
 // same expressions; stored [Ni][Hp] so that a warp reads consecutive kx.
@@ -217,6 +227,17 @@ int context_create(const Config& cfg, Context** out) {
     if (dalloc(&c->hat, (size_t)Ny * c->Hp) || dalloc(&c->cp, (size_t)c->Ni * c->Hp) ||
         dalloc(&c->tw, (size_t)c->M) || dalloc(&c->wN, (size_t)c->M + 1))
         return fail();
+    c->thomas_nseg = (c->Ni + TS_ROWS - 1) / TS_ROWS;
+    c->thomas_nsb = (c->thomas_nseg + TS_NW - 1) / TS_NW;
+    if (dalloc(&c->tconst, (size_t)c->thomas_nseg * 3 * c->Hp) || dalloc(&c->tmaps, (size_t)c->thomas_nseg * 4 * c->Hp) ||
+        dalloc(&c->tblk, (size_t)c->thomas_groups * c->thomas_nsb * 5 * 32) ||
+        dalloc(&c->tbcarry, (size_t)c->thomas_groups * c->thomas_nsb * 2 * 32))
+        return fail();
+    if (cudaMalloc((void**)&c->tcount, sizeof(unsigned int) * c->thomas_groups) != cudaSuccess ||
+        cudaMemset(c->tcount, 0, sizeof(unsigned int) * c->thomas_groups) != cudaSuccess) {
+        set_error("cudaMalloc of the Thomas counters failed");
+        return fail();
+    }
     // one buffer for the block partials of the max reduction (3 per block) and the per-row
     // partials of the diagnostics (32 per row); never reallocated (graphs keep its address)
     c->red_nblocks = 2 * c->num_sms;
@@ -249,42 +270,17 @@ int context_create(const Config& cfg, Context** out) {
         set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail();
     }
-    // Thomas launch shape: clusters of C CTAs splitting the Ni interior rows, R rows per CTA,
-    // aiming at R ~ 128 (54 KB of shared memory, 4 CTAs per SM). Clusters of more than 8 CTAs
-    // are used only when the occupancy query says they can be scheduled.
+    if (cudaFuncSetAttribute(k_thomas_maps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes()) ||
+        cudaFuncSetAttribute(k_thomas_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes())) {
+        set_error("cudaFuncSetAttribute (Thomas shared memory) failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail();
+    }
     {
-        auto shape = [&](int C) {
-            c->thomas_C = C;
-            c->thomas_R = (c->Ni + C - 1) / C;
-            c->thomas_smem = thomas_smem_doubles(c->thomas_R, C) * sizeof(double);
-        };
-        int C = std::min(16, std::max(1, (c->Ni + 127) / 128));
-        if (C > 8) {
-            shape(C);
-            int nclusters = 0;
-            cudaLaunchConfig_t lc{};
-            lc.gridDim = dim3(C * c->thomas_groups);
-            lc.blockDim = dim3(KT_NW * 32);
-            lc.dynamicSmemBytes = c->thomas_smem;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-            lc.attrs = at;
-            lc.numAttrs = 1;
-            if (cudaFuncSetAttribute(k_thomas, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-                cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem) != cudaSuccess ||
-                cudaOccupancyMaxActiveClusters(&nclusters, k_thomas, &lc) != cudaSuccess || nclusters < 1) {
-                cudaGetLastError();
-                C = 8;
-            }
-        }
-        shape(C);
-        if (c->thomas_smem > 220 * 1024) {
-            set_error("Ny = %d too large for the cluster Thomas solve (R = %d rows per CTA)", Ny, c->thomas_R);
-            return fail();
-        }
-        if (cudaFuncSetAttribute(k_thomas, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->thomas_smem)) {
-            set_error("cudaFuncSetAttribute failed: %s", cudaGetErrorString(cudaGetLastError()));
+        ThomasParams tp = thomas_params(c);
+        dim3 grid((c->Hp + 127) / 128, c->thomas_nseg);
+        k_thomas_consts<<<grid, 128>>>(tp);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+            set_error("Thomas table setup failed: %s", cudaGetErrorString(cudaGetLastError()));
             return fail();
         }
     }
@@ -303,6 +299,11 @@ void context_destroy(Context* c) {
                       c->psi, c->rhs, c->J, c->cp, c->red_blocks, c->red_out})
         if (p) cudaFree(p);
     if (c->hat) cudaFree(c->hat);
+    if (c->tconst) cudaFree(c->tconst);
+    if (c->tmaps) cudaFree(c->tmaps);
+    if (c->tblk) cudaFree(c->tblk);
+    if (c->tbcarry) cudaFree(c->tbcarry);
+    if (c->tcount) cudaFree(c->tcount);
     if (c->tw) cudaFree(c->tw);
     if (c->wN) cudaFree(c->wN);
     if (c->ctl) cudaFree(c->ctl);
@@ -396,26 +397,19 @@ int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom
     NSE_FFT_DISPATCH(fft_inv_t)
 }
 
-int launch_thomas(Context* c, cudaStream_t s) {
-    ThomasParams p{};
-    p.hat = c->hat; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
-    p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni; p.C = c->thomas_C; p.R = c->thomas_R;
-    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(c->thomas_C * c->thomas_groups);
-    cfg.blockDim = dim3(KT_NW * 32);
-    cfg.dynamicSmemBytes = c->thomas_smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = c->thomas_C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    NSE_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_thomas, p));
+// The two passes of the segmented Thomas solve: the segment maps (and, in the last CTA of each
+// column group, the carries), then the rerun of every segment from its carries.
+static int launch_thomas_maps(Context* c, cudaStream_t s) {
+    k_thomas_maps<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c));
+    NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
+static int launch_thomas_apply(Context* c, cudaStream_t s) {
+    k_thomas_apply<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c));
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+int launch_thomas(Context* c, cudaStream_t s) { return (launch_thomas_maps(c, s) || launch_thomas_apply(c, s)) ? -1 : 0; }
 
 // the reference's standalone Thom launcher (src/ops.cu:270-276)
 int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s) {
@@ -466,7 +460,8 @@ static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev
         if (launch_stage(c, st, win[st - 1], c->w, wst[st - 1], s, (store_rhs && st == 3) ? c->rhs : nullptr) || mark())
             return -1;
         if (launch_fft_fwd(c, wst[st - 1], s) || mark()) return -1;
-        if (launch_thomas(c, s) || mark()) return -1;
+        if (launch_thomas_maps(c, s) || mark()) return -1;
+        if (launch_thomas_apply(c, s) || mark()) return -1;
         // the stage-3 transform also advances the time (its last CTA)
         if (launch_ifft_thom(c, c->psi, wst[st - 1], st, true, c->closure_diag, s, st == 3) || mark()) return -1;
     }
@@ -478,15 +473,15 @@ int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev) { return ste
 
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
-    static const char* stage[4] = {"k_stage", "k_fft_fwd", "k_thomas", "k_ifft_thom"};
+    static const char* stage[5] = {"k_stage", "k_fft_fwd", "k_thomas_maps", "k_thomas_apply", "k_ifft_thom"};
     if (c->cfg.adapt) {
         if (k == 0) return "k_maxuv_dt";
         --k;
     }
-    return (k < 12) ? stage[k % 4] : "";
+    return (k < 15) ? stage[k % 5] : "";
 }
 
-int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 4; }
+int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 5; }
 
 // nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.
 int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs) {

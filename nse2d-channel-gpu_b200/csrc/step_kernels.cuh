@@ -14,7 +14,6 @@
 // Per step: k_maxuv_dt (max|u|,|v|,|v|a -> adaptive dt on the device) before stage 1; the
 // last CTA of the stage-3 k_ifft_thom advances the time.
 #pragma once
-#include <cooperative_groups.h>
 #include "common.cuh"
 #include "fft_rows.cuh"
 
@@ -213,6 +212,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Row FFT kernels: one CTA of IP_NT threads transforms one row at a time in ONE shared buffer
@@ -353,175 +356,322 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
 }
 
 struct ThomasParams {
-    cpx<double>* hat;        // [Ny][Hp], in place
+    cpx<double>* hat;        // [Ny][Hp], in place: omega-hat in, psi-hat out
     const double* cp;        // [Ni][Hp]
-    const double* asub;
-    const double* inv_csup;
-    const double* csup;
-    int Nx, Ny, Hp, H, Ni, C, R;
+    const double* asub;      // [Ny]
+    const double* inv_csup;  // [Ny]
+    const double* csup;      // [Ny]
+    double* tconst;          // [nseg][3][Hp]: P, V, Q of every segment (data independent)
+    double* tmaps;           // [nseg][2][2 Hp]: D, U of every segment and real column
+    double* tblk;            // [groups][nsb][5][32]: block aggregates P, D, B0, B1, Q
+    double* tbcarry;         // [groups][nsb][2][32]: carries c (from below) and X (from above) of every block
+    unsigned int* tcount;    // [groups]: arrival counters of the map pass
+    int Nx, Ny, Hp, H, Ni, nseg, nsb;
     double psi_bot, psi_top;
 };
 
-constexpr int KT_NW = 8;     // warps per CTA
-
-// Thomas sweeps of the reference (src/poisson.cu:70-133) split into segments. A segment maps
-// the value entering it to d + P c (forward elimination) and x + Q X (back substitution);
-// the maps of consecutive segments compose, so every warp sweeps its own rows and only the
-// maps travel between warps (shared memory) and CTAs (distributed shared memory).
+// Thomas sweeps of the reference (src/poisson.cu:70-133), split into segments of TS_ROWS rows.
 //
-// Shared memory of a CTA with R rows: data [R][32] (16 kx, re/im interleaved as in HBM),
-// cp [R][16], the row coefficients asub and 1/csup [R] each, per-warp maps and the maps of
-// all CTAs of the cluster.
-__host__ __device__ constexpr size_t thomas_smem_doubles(int R, int C) {
-    return (size_t)R * 32 + (size_t)R * 16 + 2 * (size_t)R + 2 * KT_NW * 32 + 2 * 64 + (size_t)C * 64;
+// Forward elimination dp_j = (r_j - a_j dp_{j-1}) / (b_j - a_j cp_{j-1}) is written
+// dp_j = alpha_j r_j + beta_j dp_{j-1} with alpha_j = cp_j / c_j, beta_j = -a_j alpha_j, and the
+// back substitution is x_j = dp_j - cp_j x_{j+1}. Both are affine in the value entering a
+// segment, so a segment of rows a..b with incoming carries c (dp_{a-1}) and X (x_{b+1}) gives
+//   dp_b = D + P c,   x_a = U + V c + Q X,
+// where D, U come from running the segment with zero carries, P = prod beta, Q = prod (-cp) and
+// V = the back substitution of the partial products of beta (P, V, Q do not depend on the data
+// and are tabulated once). A block of TS_NW consecutive segments composes in the same way:
+//   dp_last = D_blk + P_blk c_blk,   x_first = B0 + B1 c_blk + Q_blk X_blk.
+// One warp owns one segment of one 16-column group (32 real columns, re/im interleaved as in
+// HBM); one CTA owns a block. The map pass (k_thomas_maps) writes D, U of every segment and the
+// block aggregates; the last CTA of a column group to finish folds that group's block
+// aggregates into the carries of every block. The apply pass (k_thomas_apply) resolves the
+// carries of the block's segments from the block carries and reruns each segment from them.
+constexpr int TS_ROWS = 16;  // rows per segment
+constexpr int TS_NW = 8;     // warps (segments) per CTA
+
+// Right-hand side of interior row j (0-based interior index r = j - 1): -omega-hat, with the
+// k = 0 Dirichlet wall terms of src/poisson.cu:91-95,109-114 on the real part.
+__device__ __forceinline__ double thomas_rhs(const ThomasParams& p, double w, int j, bool kx0re) {
+    double v = -w;
+    if (kx0re) {
+        if (j == 1) v -= p.asub[1] * p.psi_bot * (double)p.Nx;
+        if (j == p.Ny - 2) v -= p.csup[p.Ny - 2] * p.psi_top * (double)p.Nx;
+    }
+    return v;
 }
 
-static __global__ void __launch_bounds__(KT_NW * 32) k_thomas(ThomasParams p) {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// One-time table of P, V, Q per (segment, kx), one thread per (segment, kx).
+static __global__ void k_thomas_consts(ThomasParams p) {
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (kx >= p.Hp) return;
+    const int r0 = s * TS_ROWS, n = min(TS_ROWS, p.Ni - r0);
+    double Pc[TS_ROWS], cpr[TS_ROWS];
+    double P = 1.0;
+    for (int t = 0; t < n; ++t) {
+        const int j = r0 + t + 1;
+        cpr[t] = p.cp[(size_t)(r0 + t) * p.Hp + kx];
+        const double alpha = cpr[t] * p.inv_csup[j];
+        P = (-p.asub[j] * alpha) * P;
+        Pc[t] = P;
+    }
+    double V = 0.0, Q = 1.0;
+    for (int t = n - 1; t >= 0; --t) {
+        V = Pc[t] - cpr[t] * V;
+        Q = -cpr[t] * Q;
+    }
+    double* o = p.tconst + (size_t)s * 3 * p.Hp;
+    o[kx] = P;
+    o[p.Hp + kx] = V;
+    o[2 * p.Hp + kx] = Q;
+}
+
+// Shared memory of the map and apply passes: per warp, its segment's values [TS_ROWS][32]
+// (16 kx, re/im interleaved as in HBM) and cp [TS_ROWS][16]; per CTA, asub and 1/csup of its rows.
+__host__ __device__ constexpr size_t thomas_smem_bytes() {
+    return sizeof(double) * ((size_t)TS_NW * TS_ROWS * 32 + (size_t)TS_NW * TS_ROWS * 16 + 2 * (size_t)TS_NW * TS_ROWS);
+}
+
+struct ThomasTile {
+    double* v;               // [TS_ROWS][32] of this warp
+    double* cp;              // [TS_ROWS][16] of this warp
+    const double* sa;        // asub of the warp's rows
+    const double* sic;       // 1/csup of the warp's rows
+};
+
+__device__ __forceinline__ ThomasTile thomas_tile(unsigned char* smem_raw, int warp) {
+    double* base = reinterpret_cast<double*>(smem_raw);
+    ThomasTile tl;
+    tl.v = base + (size_t)warp * TS_ROWS * 32;
+    tl.cp = base + (size_t)TS_NW * TS_ROWS * 32 + (size_t)warp * TS_ROWS * 16;
+    double* rows = base + (size_t)TS_NW * TS_ROWS * 48;
+    tl.sa = rows + warp * TS_ROWS;
+    tl.sic = rows + TS_NW * TS_ROWS + warp * TS_ROWS;
+    return tl;
+}
+
+// asub and 1/csup of one warp's rows (8-byte cp.async), and the warp's tile by 16-byte
+// cp.async copies (the padding columns kx >= H of omega-hat and of cp hold zeros, so every chunk of a
+// valid row is a valid address); rows past the end are left unread and never used.
+__device__ __forceinline__ void thomas_stage_warp_rows(const ThomasParams& p, unsigned char* smem_raw, int s) {
+    double* rows = reinterpret_cast<double*>(smem_raw) + (size_t)TS_NW * TS_ROWS * 48;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = (int)cluster.block_rank();
-    const int C = p.C;
-    const int g = blockIdx.x / C;                     // kx group of 16 columns
-    const int R = p.R;
-    double* data = reinterpret_cast<double*>(smem_raw);          // [R][32]
-    double* cpv = data + (size_t)R * 32;                         // [R][16]
-    double* sasub = cpv + (size_t)R * 16;                        // [R]
-    double* sinvc = sasub + R;                                   // [R]
-    double* aggP = sinvc + R;                                    // [NW][32]
-    double* aggD = aggP + KT_NW * 32;                            // [NW][32]
-    double* ctaF = aggD + KT_NW * 32;                            // [64]  (P, d) of this CTA
-    double* ctaB = ctaF + 64;                                    // [64]  (Q, x) of this CTA
-    double* allc = ctaB + 64;                                    // [C][64] maps of the cluster's CTAs
-    const int kx = g * 16 + (lane >> 1);
-    const int part = lane & 1;
-    const bool valid = kx < p.H;
-    const int r0 = q * R;                                         // first interior row index (0-based)
-    const int r1 = min(p.Ni, r0 + R);
-    const int nr = max(0, r1 - r0);
-    const int RW = (R + KT_NW - 1) / KT_NW;
-    const int wa = min(r1, r0 + warp * RW), wb = min(r1, r0 + (warp + 1) * RW);   // [wa, wb)
+    for (int t = lane; t < 2 * TS_ROWS; t += 32) {
+        const int tt = t % TS_ROWS, j = s * TS_ROWS + tt + 1;
+        if (j <= p.Ni) {
+            if (t < TS_ROWS) cp_async8(&rows[warp * TS_ROWS + tt], &p.asub[j]);
+            else cp_async8(&rows[TS_NW * TS_ROWS + warp * TS_ROWS + tt], &p.inv_csup[j]);
+        }
+    }
+}
+
+__device__ __forceinline__ void thomas_issue_loads(const ThomasParams& p, int r0, int n, int g, const ThomasTile& tl) {
     const double* hatd = reinterpret_cast<const double*>(p.hat);
     const size_t rowstride = (size_t)p.Hp * 2;
-    // ---- stage the CTA's tile: 16-byte chunks, all in flight (the padding columns kx >= H of
-    //      the spectral buffer and of cp hold zeros, so every chunk is a valid address)
-    for (int ch = threadIdx.x; ch < nr * 16; ch += blockDim.x) {
-        const int rr = ch >> 4, cc = (ch & 15) * 2;
-        cp_async16(&data[(size_t)rr * 32 + cc], &hatd[(size_t)(r0 + rr + 1) * rowstride + (size_t)g * 32 + cc]);
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < TS_ROWS / 2; ++i) {             // 16 chunks of 16 bytes per row
+        const int ch = lane + 32 * i, row = ch >> 4, part = ch & 15;
+        if (row < n) cp_async16(&tl.v[row * 32 + part * 2], &hatd[(size_t)(r0 + row + 1) * rowstride + (size_t)g * 32 + part * 2]);
     }
-    for (int ch = threadIdx.x; ch < nr * 8; ch += blockDim.x) {
-        const int rr = ch >> 3, cc = (ch & 7) * 2;
-        cp_async16(&cpv[(size_t)rr * 16 + cc], &p.cp[(size_t)(r0 + rr) * p.Hp + (size_t)g * 16 + cc]);
+#pragma unroll
+    for (int i = 0; i < TS_ROWS / 4; ++i) {             // 8 chunks per row
+        const int ch = lane + 32 * i, row = ch >> 3, part = ch & 7;
+        if (row < n) cp_async16(&tl.cp[row * 16 + part * 2], &p.cp[(size_t)(r0 + row) * p.Hp + (size_t)g * 16 + part * 2]);
     }
-    for (int rr = threadIdx.x; rr < nr; rr += blockDim.x) {
-        sasub[rr] = p.asub[r0 + rr + 1];
-        sinvc[rr] = p.inv_csup[r0 + rr + 1];
+}
+
+// Forward elimination over the segment from the carry d, in place in the tile; returns dp at
+// the last row.
+__device__ __forceinline__ double thomas_forward(const ThomasParams& p, int r0, int n, bool kx0re, double d,
+                                                 const ThomasTile& tl) {
+    const int lane = threadIdx.x & 31, k16 = lane >> 1;
+#pragma unroll 8
+    for (int t = 0; t < n; ++t) {
+        const double alpha = tl.cp[t * 16 + k16] * tl.sic[t];
+        const double beta = -tl.sa[t] * alpha;
+        d = alpha * thomas_rhs(p, tl.v[t * 32 + lane], r0 + t + 1, kx0re) + beta * d;
+        tl.v[t * 32 + lane] = d;
     }
+    return d;
+}
+
+// Copies the per-segment maps (P, V, Q from the table, D, U of this solve) of segment s into
+// e[5][32] (one warp, cp.async): slots 0 P, 1 D, 2 V, 3 Q, 4 U.
+__device__ __forceinline__ void thomas_seg_maps(const ThomasParams& p, int s, int kx, int col, int lane, double* e) {
+    const int cols = 2 * p.Hp;
+    cp_async8(&e[0 * 32 + lane], &p.tconst[((size_t)s * 3 + 0) * p.Hp + kx]);
+    cp_async8(&e[2 * 32 + lane], &p.tconst[((size_t)s * 3 + 1) * p.Hp + kx]);
+    cp_async8(&e[3 * 32 + lane], &p.tconst[((size_t)s * 3 + 2) * p.Hp + kx]);
+    cp_async8(&e[1 * 32 + lane], &p.tmaps[((size_t)s * 2 + 0) * cols + col]);
+    cp_async8(&e[4 * 32 + lane], &p.tmaps[((size_t)s * 2 + 1) * cols + col]);
+}
+
+static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = blockIdx.x / p.nsb, sb = blockIdx.x - g * p.nsb;
+    const int kx = g * 16 + (lane >> 1), col = g * 32 + lane;
+    const bool kx0re = (kx == 0) && ((lane & 1) == 0);
+    const int cols = 2 * p.Hp;
+    const int s = sb * TS_NW + warp;
+    const ThomasTile tl = thomas_tile(smem_raw, warp);
+    double* e = tl.v;                                  // [5][32] maps of this warp's segment, after use of the tile
+    const int r0 = s * TS_ROWS, n = (s < p.nseg) ? min(TS_ROWS, p.Ni - r0) : 0;
+    double Ps = 0.0, Vs = 0.0, Qs = 0.0;
+    if (s < p.nseg) {
+        thomas_issue_loads(p, r0, n, g, tl);
+        thomas_stage_warp_rows(p, smem_raw, s);
+        Ps = __ldg(&p.tconst[((size_t)s * 3 + 0) * p.Hp + kx]);
+        Vs = __ldg(&p.tconst[((size_t)s * 3 + 1) * p.Hp + kx]);
+        Qs = __ldg(&p.tconst[((size_t)s * 3 + 2) * p.Hp + kx]);
+        cp_async_wait_all();
+        __syncwarp();
+        const double D = thomas_forward(p, r0, n, kx0re, 0.0, tl);
+        double U = 0.0;
+#pragma unroll 8
+        for (int t = n - 1; t >= 0; --t) U = tl.v[t * 32 + lane] - tl.cp[t * 16 + (lane >> 1)] * U;
+        p.tmaps[((size_t)s * 2 + 0) * cols + col] = D;
+        p.tmaps[((size_t)s * 2 + 1) * cols + col] = U;
+        __syncwarp();
+        e[0 * 32 + lane] = Ps;
+        e[1 * 32 + lane] = D;
+        e[2 * 32 + lane] = Vs;
+        e[3 * 32 + lane] = Qs;
+        e[4 * 32 + lane] = U;
+    }
+    __syncthreads();
+    double* blk = p.tblk + ((size_t)g * p.nsb + sb) * 5 * 32;
+    if (warp == 0) {
+        // block aggregate: forward carries c_s = c0_s + Pp_s c_blk inside the block, then the
+        // backward maps B_s = (U_s + V_s c0_s) + (V_s Pp_s) c_blk composed from the top down
+        const int ns = min(TS_NW, p.nseg - sb * TS_NW);
+        double c0[TS_NW], Pp[TS_NW];
+        double Pa = 1.0, Da = 0.0;
+#pragma unroll
+        for (int w = 0; w < TS_NW; ++w) {
+            if (w < ns) {
+                const double* ew = thomas_tile(smem_raw, w).v;
+                c0[w] = Da;
+                Pp[w] = Pa;
+                Da = ew[1 * 32 + lane] + ew[0 * 32 + lane] * Da;
+                Pa = ew[0 * 32 + lane] * Pa;
+            }
+        }
+        double B0 = 0.0, B1 = 0.0, Qb = 1.0;
+#pragma unroll
+        for (int w = TS_NW - 1; w >= 0; --w) {
+            if (w < ns) {
+                const double* ew = thomas_tile(smem_raw, w).v;
+                const double Vs = ew[2 * 32 + lane], Qs = ew[3 * 32 + lane], Us = ew[4 * 32 + lane];
+                B0 = (Us + Vs * c0[w]) + Qs * B0;
+                B1 = Vs * Pp[w] + Qs * B1;
+                Qb = Qs * Qb;
+            }
+        }
+        blk[0 * 32 + lane] = Pa;
+        blk[1 * 32 + lane] = Da;
+        blk[2 * 32 + lane] = B0;
+        blk[3 * 32 + lane] = B1;
+        blk[4 * 32 + lane] = Qb;
+        __threadfence();                               // the aggregate before the arrival count
+    }
+    // the last CTA of this column group folds the block aggregates into block carries
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(&p.tcount[g], 1u) == (unsigned)(p.nsb - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double* fb = reinterpret_cast<double*>(smem_raw);  // [nsb][5][32], the tiles are free now
+    const double* gblk = p.tblk + (size_t)g * p.nsb * 5 * 32;
+    const int nfit = (int)(thomas_smem_bytes() / sizeof(double)) / (5 * 32);
+    double* bc = p.tbcarry + (size_t)g * p.nsb * 2 * 32;
+    if (p.nsb <= nfit) {
+        for (int i = threadIdx.x; i < p.nsb * 5 * 32; i += blockDim.x) fb[i] = __ldcg(&gblk[i]);
+        __syncthreads();
+        if (warp == 0) {
+            double c = 0.0;
+            for (int b = 0; b < p.nsb; ++b) {
+                bc[(size_t)b * 64 + lane] = c;
+                c = fb[b * 160 + 32 + lane] + fb[b * 160 + lane] * c;
+            }
+            double X = 0.0;
+            for (int b = p.nsb - 1; b >= 0; --b) {
+                bc[(size_t)b * 64 + 32 + lane] = X;
+                const double cb = bc[(size_t)b * 64 + lane];
+                X = fb[b * 160 + 64 + lane] + fb[b * 160 + 96 + lane] * cb + fb[b * 160 + 128 + lane] * X;
+            }
+        }
+    } else if (warp == 0) {
+        double c = 0.0;
+        for (int b = 0; b < p.nsb; ++b) {
+            bc[(size_t)b * 64 + lane] = c;
+            c = __ldcg(&gblk[b * 160 + 32 + lane]) + __ldcg(&gblk[b * 160 + lane]) * c;
+        }
+        double X = 0.0;
+        for (int b = p.nsb - 1; b >= 0; --b) {
+            bc[(size_t)b * 64 + 32 + lane] = X;
+            const double cb = bc[(size_t)b * 64 + lane];
+            X = __ldcg(&gblk[b * 160 + 64 + lane]) + __ldcg(&gblk[b * 160 + 96 + lane]) * cb +
+                __ldcg(&gblk[b * 160 + 128 + lane]) * X;
+        }
+    }
+    if (threadIdx.x == 0) p.tcount[g] = 0;      // ready for the next solve
+}
+
+static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double segm[TS_NW][5 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = blockIdx.x / p.nsb, sb = blockIdx.x - g * p.nsb;
+    const int kx = g * 16 + (lane >> 1), col = g * 32 + lane;
+    const bool kx0re = (kx == 0) && ((lane & 1) == 0);
+    const bool valid = kx < p.H;
+    const int s = sb * TS_NW + warp;
+    const int ns = min(TS_NW, p.nseg - sb * TS_NW);
+    const ThomasTile tl = thomas_tile(smem_raw, warp);
+    const int r0 = s * TS_ROWS, n = (s < p.nseg) ? min(TS_ROWS, p.Ni - r0) : 0;
+    if (s < p.nseg) {
+        thomas_issue_loads(p, r0, n, g, tl);
+        thomas_stage_warp_rows(p, smem_raw, s);
+        thomas_seg_maps(p, s, kx, col, lane, segm[warp]);
+    }
+    const double* bcar = p.tbcarry + ((size_t)g * p.nsb + sb) * 2 * 32;
+    const double cblk = __ldcg(&bcar[lane]), Xblk = __ldcg(&bcar[32 + lane]);
     cp_async_wait_all();
     __syncthreads();
-    // ---- phase 1: local forward elimination, dp_j = alpha_j r_j + beta_j dp_{j-1}, with
-    //      r_j = -omega-hat_j plus the k = 0 wall terms (poisson.cu:91-95,109-114),
-    //      alpha_j = 1/den_j = cp_j / csup_j, beta_j = -asub_j alpha_j (poisson.cu:97-119)
-    double d = 0.0, P = 1.0;
-#pragma unroll 4
-    for (int r = wa; r < wb; ++r) {
-        const int jrow = r + 1, rr = r - r0;
-        double v = -data[(size_t)rr * 32 + lane];
-        if (kx == 0 && part == 0) {
-            if (jrow == 1) v -= p.asub[1] * p.psi_bot * (double)p.Nx;
-            if (jrow == p.Ny - 2) v -= p.csup[p.Ny - 2] * p.psi_top * (double)p.Nx;
-        }
-        const double alpha = cpv[(size_t)rr * 16 + (lane >> 1)] * sinvc[rr];
-        const double beta = -sasub[rr] * alpha;
-        d = alpha * v + beta * d;
-        P = beta * P;
-        data[(size_t)rr * 32 + lane] = d;
+    if (s >= p.nseg) return;
+    // carries of this warp's segment from the block carries: forward through the lower
+    // segments of the block, then backward from the top of the block down to this one
+    double cs[TS_NW];
+    double c = cblk;
+#pragma unroll
+    for (int w = 0; w < TS_NW; ++w) {
+        cs[w] = c;
+        if (w < ns) c = segm[w][32 + lane] + segm[w][lane] * c;
     }
-    aggP[warp * 32 + lane] = P;
-    aggD[warp * 32 + lane] = d;
-    __syncthreads();
-    if (warp == 0) {
-        double cP = 1.0, cD = 0.0;                    // identity map
-        for (int w = 0; w < KT_NW; ++w) {
-            const double Pw = aggP[w * 32 + lane], Dw = aggD[w * 32 + lane];
-            cD = Dw + Pw * cD;
-            cP = Pw * cP;
-        }
-        ctaF[lane] = cP;
-        ctaF[32 + lane] = cD;
-    }
-    cluster.sync();
-    // gather the maps of all CTAs of the cluster in one parallel pass over DSMEM
-    for (int idx = threadIdx.x; idx < C * 64; idx += blockDim.x) {
-        const int qq = idx >> 6;
-        allc[idx] = cluster.map_shared_rank(ctaF, qq)[idx & 63];
-    }
-    __syncthreads();
-    // incoming carry of this warp: the maps of the lower-ranked CTAs, then of the lower warps
-    double c = 0.0;
-    for (int qq = 0; qq < q; ++qq) c = allc[qq * 64 + 32 + lane] + allc[qq * 64 + lane] * c;
-    for (int w = 0; w < warp; ++w) c = aggD[w * 32 + lane] + aggP[w * 32 + lane] * c;
-    // ---- phase 2: dp_j = dtilde_j + P_j c
-    P = 1.0;
-#pragma unroll 4
-    for (int r = wa; r < wb; ++r) {
-        const int rr = r - r0;
-        const double alpha = cpv[(size_t)rr * 16 + (lane >> 1)] * sinvc[rr];
-        P = (-sasub[rr] * alpha) * P;
-        data[(size_t)rr * 32 + lane] += P * c;
-    }
-    // ---- phase 3: local back substitution x_j = dp_j - cp_j x_{j+1} (poisson.cu:121-129)
-    double x = 0.0, Q = 1.0;
-#pragma unroll 4
-    for (int r = wb - 1; r >= wa; --r) {
-        const int rr = r - r0;
-        const double cpj = cpv[(size_t)rr * 16 + (lane >> 1)];
-        x = data[(size_t)rr * 32 + lane] - cpj * x;
-        Q = -cpj * Q;
-        data[(size_t)rr * 32 + lane] = x;
-    }
-    __syncthreads();                                   // forward maps no longer needed
-    aggP[warp * 32 + lane] = Q;
-    aggD[warp * 32 + lane] = x;
-    __syncthreads();
-    if (warp == 0) {
-        double cQ = 1.0, cX = 0.0;
-        for (int w = KT_NW - 1; w >= 0; --w) {
-            const double Qw = aggP[w * 32 + lane], Xw = aggD[w * 32 + lane];
-            cX = Xw + Qw * cX;
-            cQ = Qw * cQ;
-        }
-        ctaB[lane] = cQ;
-        ctaB[32 + lane] = cX;
-    }
-    cluster.sync();
-    for (int idx = threadIdx.x; idx < C * 64; idx += blockDim.x) {
-        const int qq = idx >> 6;
-        allc[idx] = cluster.map_shared_rank(ctaB, qq)[idx & 63];
-    }
-    __syncthreads();
-    double X = 0.0;                                    // x at the row above this warp
-    for (int qq = C - 1; qq > q; --qq) X = allc[qq * 64 + 32 + lane] + allc[qq * 64 + lane] * X;
-    for (int w = KT_NW - 1; w > warp; --w) X = aggD[w * 32 + lane] + aggP[w * 32 + lane] * X;
-    // ---- phase 4: x_j = xtilde_j + Q_j X, Q_j = prod_{i=j}^{top} (-cp_i); store psi-hat
+    double x = Xblk;
+#pragma unroll
+    for (int w = TS_NW - 1; w >= 0; --w)
+        if (w > warp && w < ns) x = (segm[w][128 + lane] + segm[w][64 + lane] * cs[w]) + segm[w][96 + lane] * x;
+    double cw = cblk;
+#pragma unroll
+    for (int w = 0; w < TS_NW; ++w)
+        if (w == warp) cw = cs[w];
+    thomas_forward(p, r0, n, kx0re, cw, tl);
     double* hatw = reinterpret_cast<double*>(p.hat);
-    Q = 1.0;
-#pragma unroll 4
-    for (int r = wb - 1; r >= wa; --r) {
-        const int rr = r - r0;
-        Q = -cpv[(size_t)rr * 16 + (lane >> 1)] * Q;
-        const double xv = data[(size_t)rr * 32 + lane] + Q * X;
-        if (valid) hatw[(size_t)(r + 1) * rowstride + (size_t)g * 32 + lane] = xv;
+    const size_t rowstride = (size_t)p.Hp * 2;
+#pragma unroll 8
+    for (int t = n - 1; t >= 0; --t) {
+        x = tl.v[t * 32 + lane] - tl.cp[t * 16 + (lane >> 1)] * x;
+        if (valid) hatw[(size_t)(r0 + t + 1) * rowstride + col] = x;
     }
     // wall rows of psi-hat: Nx psi_bot / Nx psi_top at kx = 0, else 0 (poisson.cu:130-132)
-    if (warp == 0 && valid) {
-        if (q == 0) hatw[(size_t)g * 32 + lane] = (kx == 0 && part == 0) ? (double)p.Nx * p.psi_bot : 0.0;
-        if (q == C - 1)
-            hatw[(size_t)(p.Ny - 1) * rowstride + (size_t)g * 32 + lane] =
-                (kx == 0 && part == 0) ? (double)p.Nx * p.psi_top : 0.0;
+    if (valid) {
+        if (s == 0) hatw[col] = kx0re ? (double)p.Nx * p.psi_bot : 0.0;
+        if (s == p.nseg - 1) hatw[(size_t)(p.Ny - 1) * rowstride + col] = kx0re ? (double)p.Nx * p.psi_top : 0.0;
     }
-    cluster.sync();                                    // keep smem alive for remote readers
 }
 
 // Thom wall vorticity alone (the reference's launcher, src/ops.cu:102-158,270-276).
