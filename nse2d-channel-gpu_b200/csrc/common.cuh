@@ -94,7 +94,7 @@ struct Context {
     // spectral buffer [Ny][Hp] complex, FP64 (in place: omega-hat in, psi-hat out)
     cpx<double>* hat = nullptr;
     double* cp = nullptr;          // elimination table [Ni][Hp]
-    cpx<double>* tw = nullptr;     // M twiddles e^{-2 pi i t/M}
+    cpx<double>* tw = nullptr;     // per-pass twiddle pairs of the Nx/2-point transform
     cpx<double>* wN = nullptr;     // M+1 twiddles e^{-2 pi i k/Nx}
     // reductions
     double* red_blocks = nullptr;  // per-block partials (max and diagnostics)

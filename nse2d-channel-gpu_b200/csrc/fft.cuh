@@ -20,7 +20,9 @@
 
 namespace nse2d {
 
-template <typename T> struct cpx { T x, y; };
+// Aligned to its full size, so that a complex element moves as one 16-byte (FP64) or 8-byte
+// (FP32) access to shared or global memory.
+template <typename T> struct alignas(2 * sizeof(T)) cpx { T x, y; };
 
 template <typename T> NSE_HD cpx<T> cmul(cpx<T> a, cpx<T> b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
 template <typename T> NSE_HD cpx<T> cmulc(cpx<T> a, cpx<T> b) { return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y}; }  // a * conj(b)

@@ -2,6 +2,8 @@
 // this project. With M a template constant every index is a shift or a mask and the pass
 // schedule unrolls.
 #pragma once
+#include <vector>
+
 #include "fft.cuh"
 
 namespace nse2d {
@@ -46,6 +48,11 @@ template <int M> struct fft_npass {
 //
 // Shared-memory layout: ip_idx(i) = i + i/8 + i/512 (16-byte units) spreads the stride-8 and
 // stride-512 accesses of the first pass and of the digit-reversed scatter over the banks.
+//
+// Twiddles: a pass with sub-transform length LP > 1 (always a power of 8) reads the pairs
+// (W_L^m, W_L^{4m}), L = R LP, m < LP, from a per-pass table, contiguous in m and stored as
+// consecutive complex pairs from pair (LP - 8) / 7 on (pass_twiddle_table builds it), so a
+// warp's twiddle loads cover consecutive addresses.
 // ---------------------------------------------------------------------------------------
 __host__ __device__ __forceinline__ int ip_idx(int i) { return i + (i >> 3) + (i >> 9); }
 __host__ __device__ constexpr int ip_size(int M) { return M + (M >> 3) + (M >> 9) + 1; }
@@ -71,11 +78,24 @@ template <int M> __host__ __device__ __forceinline__ int dit_pos(int n) {
     return p;
 }
 
+// Per-pass twiddle table of an M-point transform from the full table tw[t] = W_M^t: for each
+// pass with LP > 1, the pairs (W_L^m, W_L^{4m}) = (tw[m M/L], tw[4 m M/L mod M]), m < LP.
+template <typename C>
+inline void pass_twiddle_table(int M, const C* tw, std::vector<C>& out) {
+    out.clear();
+    for (int LP = 8; LP < M; LP *= 8) {
+        const int rem = M / LP, R = (rem % 8 == 0) ? 8 : rem, L = R * LP, step = M / L;
+        for (int m = 0; m < LP; ++m) {
+            out.push_back(tw[(step * m) & (M - 1)]);
+            out.push_back(tw[(4 * step * m) & (M - 1)]);
+        }
+    }
+    if (out.empty()) out.push_back(tw[0]);
+}
+
 template <typename T, int M, int R, int LP, bool INV, int NT>
 __device__ __forceinline__ void ip_pass(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw) {
     constexpr int NB = M / R;            // butterflies
-    constexpr int L = R * LP;
-    constexpr int TSTEP = M / L;         // W_L^{m} = W_M^{m TSTEP}
 #pragma unroll
     for (int b0 = 0; b0 < NB; b0 += NT) {
         const int b = b0 + (int)threadIdx.x;
@@ -86,14 +106,17 @@ __device__ __forceinline__ void ip_pass(cpx<T>* __restrict__ buf, const cpx<T>* 
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = buf[ip_idx(base + r * LP)];
         if (LP > 1 && m > 0) {
+            // this pass's pair (W_L^m, W_L^{4m}) sits at 2 (off + m) of the per-pass table
+            static_assert(LP == 1 || (ilog2<LP>::v % 3 == 0), "passes with twiddles start at a power of 8");
+            constexpr int OFF = (LP - 8) / 7;
             cpx<T> wp[R];
-            wp[1] = ldtw(tw, (TSTEP * m) & (M - 1));
+            wp[1] = ldtw(tw, 2 * (OFF + m));
             if constexpr (R >= 4) {
                 wp[2] = cmul(wp[1], wp[1]);
                 wp[3] = cmul(wp[2], wp[1]);
             }
             if constexpr (R == 8) {
-                wp[4] = ldtw(tw, (4 * TSTEP * m) & (M - 1));
+                wp[4] = ldtw(tw, 2 * (OFF + m) + 1);
                 wp[5] = cmul(wp[4], wp[1]);
                 wp[6] = cmul(wp[4], wp[2]);
                 wp[7] = cmul(wp[4], wp[3]);

@@ -225,7 +225,7 @@ int context_create(const Config& cfg, Context** out) {
         dalloc(&c->rhs, c->N) || dalloc(&c->J, c->N))
         return fail();
     if (dalloc(&c->hat, (size_t)Ny * c->Hp) || dalloc(&c->cp, (size_t)c->Ni * c->Hp) ||
-        dalloc(&c->tw, (size_t)c->M) || dalloc(&c->wN, (size_t)c->M + 1))
+        dalloc(&c->wN, (size_t)c->M + 1))
         return fail();
     c->thomas_nseg = (c->Ni + TS_ROWS - 1) / TS_ROWS;
     c->thomas_nsb = (c->thomas_nseg + TS_NW - 1) / TS_NW;
@@ -254,8 +254,10 @@ int context_create(const Config& cfg, Context** out) {
         set_error("metric upload failed");
         return fail();
     }
-    std::vector<cpx<double>> tw, wN;
-    twiddles(c->M, tw, wN);
+    std::vector<cpx<double>> tw_full, tw, wN;
+    twiddles(c->M, tw_full, wN);
+    pass_twiddle_table(c->M, tw_full.data(), tw);
+    if (dalloc(&c->tw, tw.size())) return fail();
     if (cudaMemcpy(c->tw, tw.data(), tw.size() * sizeof(tw[0]), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->wN, wN.data(), wN.size() * sizeof(wN[0]), cudaMemcpyHostToDevice)) {
         set_error("twiddle upload failed");

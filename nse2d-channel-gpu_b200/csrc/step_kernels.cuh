@@ -195,7 +195,7 @@ struct FftParams {
     const double* src;       // forward: real rows [Ny][Nx]
     cpx<double>* hat;        // [Ny][Hp]
     double* psi;             // inverse output [Ny][Nx]
-    const cpx<double>* tw;   // M twiddles e^{-2 pi i t/M}
+    const cpx<double>* tw;   // per-pass twiddle pairs of the M-point transform (pass_twiddle_table)
     const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
     int Nx, Ny, Hp, rows_per_cta;
     // inverse only: Thom closure (src/ops.cu:102-158) and the closure_diag wall bookkeeping
