@@ -90,7 +90,7 @@ def kernel_bytes(name, stage, Nx, Ny):
     """Algorithmic bytes of one launch of each kernel of this implementation (inputs read
     once, outputs written once)."""
     N, H, Ni = Nx * Ny, Nx // 2 + 1, Ny - 2
-    if name == "k_stage":
+    if name.startswith("k_stage"):
         return 8 * N * (2 if stage == 1 else 3) + 8 * N          # psi, omega^(s) [, omega^n] -> omega^(s+1)
     if name == "k_fft_fwd":
         return 8 * Nx * Ni + 16 * H * Ni                         # omega^(s+1) rows -> omega-hat
@@ -142,7 +142,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -269,7 +269,7 @@ def run_ours(args, world, rank, local):
     agg = {}
     stage = 0
     for name, tot in per_kernel:
-        if name == "k_stage":
+        if name.startswith("k_stage"):
             stage += 1
         b = kernel_bytes(name, stage, Nx, Ny)
         a = agg.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0})
@@ -383,7 +383,7 @@ def main():
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=3)

@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "fft.cuh"
 
 namespace nse2d {
@@ -66,6 +68,9 @@ struct RowTables {
     double* w_node;     // trapezoid weights
     double* wt_node;    // deta / a_node on interior rows, 0 at walls
     double* frow;       // vorticity forcing f(y_j)
+    double* st_cj;      // stage stencil: a_j inv_dx inv_deta / 12 (the Arakawa factor a / (4 dx deta) / 3)
+    double* st_ap;      // stage stencil: nu a_j a_{j+1/2} / deta^2
+    double* st_am;      // stage stencil: nu a_j a_{j-1/2} / deta^2
     double* asub;       // Thomas sub-diagonal a_j a_{j-1/2} / deta^2
     double* csup;       // Thomas super-diagonal a_j a_{j+1/2} / deta^2
     double* inv_csup;   // 1 / csup
@@ -114,6 +119,10 @@ struct Context {
     double* tbcarry = nullptr;     // [groups][nsb][2][32] block carries c, X
     unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
     int num_sms = 0;
+    // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
+    bool stage_tma = false;
+    int stage_tma_grid = 0;
+    CUtensorMap tm_psi{}, tm_w[3]{}, tm_wn{};
     cudaStream_t cap_stream = nullptr;     // private stream used only for graph capture
     cudaGraphExec_t graph_exec = nullptr;  // one captured step
     bool closure_diag = false;

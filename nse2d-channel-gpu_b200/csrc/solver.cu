@@ -7,6 +7,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cudaTypedefs.h>
+
 #include "nse2d_internal.h"
 #include "step_kernels.cuh"
 
@@ -101,7 +103,7 @@ __global__ void k_setup_cp(double* cp, const double* a_node, const double* a_edg
 // Row tables: Thomas coefficients (poisson.cu:86-88), forcing f(y) (ops.cu:526-531), trapezoid
 // weights wt (main.cu:252-254) and the MMS row factors (ops.cu:587-603).
 __global__ void k_setup_rows(RowTables rt, int Ny, double inv_deta2, double deta, double F0, int nforce,
-                             double h, double mms_k, double mms_c) {
+                             double h, double mms_k, double mms_c, double inv4dxde, double nu) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= Ny) return;
     if (j >= 1 && j <= Ny - 2) {
@@ -110,8 +112,12 @@ __global__ void k_setup_rows(RowTables rt, int Ny, double inv_deta2, double deta
         rt.csup[j] = an * rt.a_edge[j] * inv_deta2;
         rt.inv_csup[j] = 1.0 / rt.csup[j];
         rt.wt_node[j] = deta / an;
+        rt.st_cj[j] = an * (inv4dxde * (1.0 / 3.0));
+        rt.st_ap[j] = nu * (an * rt.a_edge[j] * inv_deta2);
+        rt.st_am[j] = nu * (an * rt.a_edge[j - 1] * inv_deta2);
     } else {
         rt.asub[j] = 0.0; rt.csup[j] = 0.0; rt.inv_csup[j] = 0.0; rt.wt_node[j] = 0.0;
+        rt.st_cj[j] = 0.0; rt.st_ap[j] = 0.0; rt.st_am[j] = 0.0;
     }
     double f = 0.0;
     if (F0 != 0.0) {
@@ -158,6 +164,33 @@ static void twiddles(int M, std::vector<cpx<double>>& tw, std::vector<cpx<double
     wN[0] = {1.0, 0.0};
     wN[M] = {-1.0, 0.0};
     if (M % 2 == 0) wN[M / 2] = {0.0, -1.0};
+}
+
+// 2-D tensor map of one [Ny][Nx] FP64 field with a box of bw x bh elements.
+static int encode_field_map(CUtensorMap* map, const double* base, int Nx, int Ny, int bw = SB_W, int bh = SB_H) {
+    static PFN_cuTensorMapEncodeTiled encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return -1;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)Nx, (cuuint64_t)Ny};
+    const cuuint64_t strides[1] = {(cuuint64_t)Nx * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
+        return -1;
+    }
+    return 0;
 }
 
 template <typename T> static int dalloc(T** p, size_t n) {
@@ -213,7 +246,8 @@ int context_create(const Config& cfg, Context** out) {
     auto fail = [&]() { context_destroy(c); return -1; };
     RowTables& rt = c->rt;
     if (dalloc(&rt.y, Ny) || dalloc(&rt.a_node, Ny) || dalloc(&rt.a_edge, Ny) || dalloc(&rt.dy_edge, Ny) ||
-        dalloc(&rt.w_node, Ny) || dalloc(&rt.wt_node, Ny) || dalloc(&rt.frow, Ny) || dalloc(&rt.asub, Ny) ||
+        dalloc(&rt.w_node, Ny) || dalloc(&rt.wt_node, Ny) || dalloc(&rt.frow, Ny) || dalloc(&rt.st_cj, Ny) ||
+        dalloc(&rt.st_ap, Ny) || dalloc(&rt.st_am, Ny) || dalloc(&rt.asub, Ny) ||
         dalloc(&rt.csup, Ny) || dalloc(&rt.inv_csup, Ny))
         return fail();
     if (cfg.mms) {
@@ -265,7 +299,8 @@ int context_create(const Config& cfg, Context** out) {
     }
     const double mms_k = 2.0 * kPiD * (double)cfg.mms_kx / cfg.Lx;
     const double mms_c = kPiD / (2.0 * cfg.h);
-    k_setup_rows<<<(Ny + 127) / 128, 128>>>(rt, Ny, c->inv_deta2, c->deta, cfg.F0, cfg.nforce, cfg.h, mms_k, mms_c);
+    k_setup_rows<<<(Ny + 127) / 128, 128>>>(rt, Ny, c->inv_deta2, c->deta, cfg.F0, cfg.nforce, cfg.h, mms_k, mms_c,
+                                            0.25 * c->inv_dx * c->inv_deta, c->nu);
     if (cfg.mms) k_setup_mms_cols<<<(c->Nx + 127) / 128, 128>>>(rt.mms_sk, rt.mms_s2k, c->Nx, c->dx, mms_k);
     k_setup_cp<<<(c->H + 127) / 128, 128>>>(c->cp, rt.a_node, rt.a_edge, c->Nx, Ny, c->Hp, c->H, cfg.Lx, c->inv_deta2);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
@@ -286,6 +321,23 @@ int context_create(const Config& cfg, Context** out) {
             return fail();
         }
     }
+    // stage kernel: persistent TMA variant when every tile row holds two or more tiles
+    c->stage_tma = (c->Nx >= 2 * ST_TX);
+    if (c->stage_tma) {
+        if (encode_field_map(&c->tm_psi, c->psi, c->Nx, Ny) || encode_field_map(&c->tm_w[0], c->w, c->Nx, Ny) ||
+            encode_field_map(&c->tm_w[1], c->w1, c->Nx, Ny) || encode_field_map(&c->tm_w[2], c->w2, c->Nx, Ny) ||
+            encode_field_map(&c->tm_wn, c->w, c->Nx, Ny, ST_TX, ST_TY))
+            return fail();
+        int per_sm = 0;
+        if (cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem_bytes()) ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tma, 256, stage_tma_smem_bytes()) ||
+            per_sm < 1) {
+            set_error("k_stage_tma cannot be resident: %s", cudaGetErrorString(cudaGetLastError()));
+            return fail();
+        }
+        const int ntiles = (c->Nx / ST_TX) * ((Ny + ST_TY - 1) / ST_TY);
+        c->stage_tma_grid = std::min(ntiles, per_sm * c->num_sms);
+    }
     Ctl h{};
     h.t = 0.0; h.dt = cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     if (cudaMemcpy(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess) { set_error("ctl upload"); return fail(); }
@@ -296,7 +348,7 @@ int context_create(const Config& cfg, Context** out) {
 void context_destroy(Context* c) {
     if (!c) return;
     RowTables& rt = c->rt;
-    for (double* p : {rt.y, rt.a_node, rt.a_edge, rt.dy_edge, rt.w_node, rt.wt_node, rt.frow, rt.asub, rt.csup,
+    for (double* p : {rt.y, rt.a_node, rt.a_edge, rt.dy_edge, rt.w_node, rt.wt_node, rt.frow, rt.st_cj, rt.st_ap, rt.st_am, rt.asub, rt.csup,
                       rt.inv_csup, rt.mms_g, rt.mms_gpp, rt.mms_sin2, rt.mms_sk, rt.mms_s2k, c->w, c->w1, c->w2,
                       c->psi, c->rhs, c->J, c->cp, c->red_blocks, c->red_out})
         if (p) cudaFree(p);
@@ -331,8 +383,20 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
                  double* rhs_out) {
     StageParams p = stage_params(c);
     p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out; p.stage = stage;
-    const dim3 grid((c->Nx + ST_TX - 1) / ST_TX, (c->Ny + ST_TY - 1) / ST_TY);
-    k_stage<<<grid, 256, 0, s>>>(p);
+    if (c->stage_tma) {
+        if (stage > 1 && w_n != c->w) { set_error("launch_stage: omega^n is not the context's omega"); return -1; }
+        StageMaps maps;
+        maps.psi = c->tm_psi;
+        maps.wn = c->tm_wn;
+        if (w_in == c->w) maps.w = c->tm_w[0];
+        else if (w_in == c->w1) maps.w = c->tm_w[1];
+        else if (w_in == c->w2) maps.w = c->tm_w[2];
+        else { set_error("launch_stage: omega^(s) is not a context buffer"); return -1; }
+        k_stage_tma<<<c->stage_tma_grid, 256, stage_tma_smem_bytes(), s>>>(maps, p);
+    } else {
+        const dim3 grid((c->Nx + ST_TX - 1) / ST_TX, (c->Ny + ST_TY - 1) / ST_TY);
+        k_stage<<<grid, 256, 0, s>>>(p);
+    }
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -480,7 +544,9 @@ const char* step_kernel_name(const Context* c, int k) {
         if (k == 0) return "k_maxuv_dt";
         --k;
     }
-    return (k < 15) ? stage[k % 5] : "";
+    if (k >= 15) return "";
+    if (k % 5 == 0 && c->stage_tma) return "k_stage_tma";
+    return stage[k % 5];
 }
 
 int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 5; }

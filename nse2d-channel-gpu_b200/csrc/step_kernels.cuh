@@ -14,6 +14,9 @@
 // Per step: k_maxuv_dt (max|u|,|v|,|v|a -> adaptive dt on the device) before stage 1; the
 // last CTA of the stage-3 k_ifft_thom advances the time.
 #pragma once
+#include <cuda.h>
+#include <cstdint>
+
 #include "common.cuh"
 #include "fft_rows.cuh"
 
@@ -92,11 +95,112 @@ __device__ __forceinline__ double point_rhs(const StageParams& p, int j, int i, 
     return rhs;
 }
 
-// ---- k_stage: 2-D tile of TX x TY points, halo staged in shared memory ----
+// ---- stage kernels: 2-D tiles of ST_TX x ST_TY points, halo of psi and omega^(s) in shared memory ----
 // 256 threads = 64 columns x 4 row groups; a thread sweeps 8 consecutive rows of one column
 // with a sliding 3-row window of psi and omega in registers (6 shared loads per point).
 constexpr int ST_TX = 64, ST_TY = 32, ST_RPT = 8, ST_W = ST_TX + 2, ST_H = ST_TY + 2;
 
+// Stage constants of one launch: dt, and the MMS amplitude at the stage time (main.cu:487-528).
+struct StageTime {
+    double dt, mA, mAp;
+};
+__device__ __forceinline__ StageTime stage_time(const StageParams& p) {
+    StageTime st;
+    st.dt = p.ctl->dt;
+    const double t = p.ctl->t;
+    const double ts = (p.stage == 1) ? t : (p.stage == 2 ? t + st.dt : t + 0.5 * st.dt);
+    st.mA = 0.0;
+    st.mAp = 0.0;
+    if (p.mms) {
+        st.mA = p.mms_A0 * (1.0 + p.mms_eps * sin(p.mms_Om * ts));
+        st.mAp = p.mms_A0 * (p.mms_eps * p.mms_Om * cos(p.mms_Om * ts));
+    }
+    return st;
+}
+
+// The points of one tile from its halo in shared memory: sp/so[r * ld + c] holds row y0 - 1 + r,
+// column x0 - 1 - coff + c.
+//
+// The arithmetic is the reference's rhs = -J + nu lap + f - r omega (src/ops.cu:532) with the
+// Arakawa Jacobian (src/ops.cu:305-325) and the mapped Laplacian (src/ops.cu:488-498), regrouped
+// for fewer FP64 operations: every term of J1 + J2 + J3 carries the factor a_j / (4 dx deta), so
+//   J = -c_j S,  c_j = a_j / (12 dx deta),
+//   S = Dx psi_j Dy om_i - Dy psi_i Dx om_j
+//     + psi_{i+1,j} Dy om_{i+1} - psi_{i-1,j} Dy om_{i-1} - psi_{i,j+1} Dx om_{j+1} + psi_{i,j-1} Dx om_{j-1}
+//     - om_{i+1,j} Dy psi_{i+1} + om_{i-1,j} Dy psi_{i-1} + om_{i,j+1} Dx psi_{j+1} - om_{i,j-1} Dx psi_{j-1},
+// with Dx f_j = f_{i+1,j} - f_{i-1,j} and Dy f_i = f_{i,j+1} - f_{i,j-1}, the very differences the
+// reference forms; the x differences of rows j-1 and j are carried down the sliding window.
+// nu lap = nu/dx^2 (om_{i+1} + om_{i-1} - 2 om) + A+_j (om_{j+1} - om) - A-_j (om - om_{j-1}),
+// A+-_j = nu a_j a_{j+-1/2} / deta^2 from the row tables. The regrouping moves the result by a few
+// ulps of its terms; the stage parity bounds hold with margin.
+__device__ __forceinline__ void stage_tile(const StageParams& p, const StageTime& st, const double* sp,
+                                           const double* so, int ld, int coff, int x0, int y0,
+                                           const double* swn = nullptr) {
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int lx = threadIdx.x & (ST_TX - 1), g = threadIdx.x / ST_TX;
+    const int i = x0 + lx;
+    if (i >= Nx) return;
+    const int ly0 = g * ST_RPT;                         // first local row (tile row ly0 <-> smem row ly0 + 1)
+    const int cb = lx + coff;
+    const double nu_dx2 = p.nu * p.inv_dx2;
+    double ps[3][3], om[3][3], dxp[3], dxo[3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { ps[r + 1][c] = sp[(ly0 + r) * ld + cb + c]; om[r + 1][c] = so[(ly0 + r) * ld + cb + c]; }
+        dxp[r + 1] = ps[r + 1][2] - ps[r + 1][0];
+        dxo[r + 1] = om[r + 1][2] - om[r + 1][0];
+    }
+#pragma unroll
+    for (int q = 0; q < ST_RPT; ++q) {
+        const int ly = ly0 + q, j = y0 + ly;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ps[0][c] = ps[1][c]; ps[1][c] = ps[2][c]; ps[2][c] = sp[(ly + 2) * ld + cb + c];
+            om[0][c] = om[1][c]; om[1][c] = om[2][c]; om[2][c] = so[(ly + 2) * ld + cb + c];
+        }
+        dxp[0] = dxp[1]; dxp[1] = dxp[2]; dxp[2] = ps[2][2] - ps[2][0];
+        dxo[0] = dxo[1]; dxo[1] = dxo[2]; dxo[2] = om[2][2] - om[2][0];
+        if (j >= Ny) break;
+        const double wc = om[1][1];
+        double rhs = fma(-p.lin_drag, wc, __ldg(&p.rt.frow[j]));                        // f - r omega
+        if (j != 0 && j != Ny - 1) {
+            const double dyo_m = om[2][0] - om[0][0], dyo_c = om[2][1] - om[0][1], dyo_p = om[2][2] - om[0][2];
+            const double dyp_m = ps[2][0] - ps[0][0], dyp_c = ps[2][1] - ps[0][1], dyp_p = ps[2][2] - ps[0][2];
+            double s1 = dxp[1] * dyo_c;
+            s1 = fma(-dyp_c, dxo[1], s1);
+            s1 = fma(ps[1][2], dyo_p, s1);
+            s1 = fma(-ps[1][0], dyo_m, s1);
+            s1 = fma(-ps[2][1], dxo[2], s1);
+            s1 = fma(ps[0][1], dxo[0], s1);
+            double s2 = -om[1][2] * dyp_p;
+            s2 = fma(om[1][0], dyp_m, s2);
+            s2 = fma(om[2][1], dxp[2], s2);
+            s2 = fma(-om[0][1], dxp[0], s2);
+            const double lapx = fma(-2.0, wc, om[1][2] + om[1][0]);
+            const double ap = __ldg(&p.rt.st_ap[j]), am = __ldg(&p.rt.st_am[j]), cj = __ldg(&p.rt.st_cj[j]);
+            rhs = fma(nu_dx2, lapx, rhs);
+            rhs = fma(ap, om[2][1] - wc, rhs);
+            rhs = fma(-am, wc - om[0][1], rhs);
+            rhs = fma(cj, s1 + s2, rhs);                                                  // -J = c_j S
+        }
+        if (p.mms) rhs += mms_term(p, j, i, st.mA, st.mAp);
+        const size_t id = (size_t)j * Nx + i;
+        if (p.rhs_out) p.rhs_out[id] = rhs;
+        double wnew;
+        const double dt = st.dt;
+        if (p.stage == 1) {
+            wnew = wc + dt * rhs;                                                          // ops.cu:646
+        } else {
+            const double wn = swn ? swn[ly * ST_TX + lx] : p.w_n[id];
+            if (p.stage == 2) wnew = 0.75 * wn + 0.25 * (wc + dt * rhs);                   // ops.cu:650
+            else wnew = (1.0 / 3.0) * wn + (2.0 / 3.0) * (wc + dt * rhs);                 // ops.cu:654
+        }
+        p.w_out[id] = wnew;
+    }
+}
+
+// One CTA per tile, halo loaded with plain loads (used when Nx < 2 ST_TX).
 static __global__ void __launch_bounds__(256) k_stage(StageParams p) {
     __shared__ double sp[ST_H][ST_W + 1];
     __shared__ double so[ST_H][ST_W + 1];
@@ -133,46 +237,118 @@ static __global__ void __launch_bounds__(256) k_stage(StageParams p) {
         }
     }
     __syncthreads();
-    const double dt = p.ctl->dt, t = p.ctl->t;
-    const double ts = (p.stage == 1) ? t : (p.stage == 2 ? t + dt : t + 0.5 * dt);   // main.cu:487-528
-    double mA = 0.0, mAp = 0.0;
-    if (p.mms) {
-        mA = p.mms_A0 * (1.0 + p.mms_eps * sin(p.mms_Om * ts));
-        mAp = p.mms_A0 * (p.mms_eps * p.mms_Om * cos(p.mms_Om * ts));
+    stage_tile(p, stage_time(p), &sp[0][0], &so[0][0], ST_W + 1, 0, x0, y0);
+}
+
+// ---- k_stage_tma: persistent, with the halos moved by the tensor memory accelerator ----
+// A CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the halo of the next tile is
+// in flight (cp.async.bulk.tensor into the other of two buffers) while the current one is
+// computed, together with the tile of omega^n in stages 2 and 3 (a third box, 64 x 32). The
+// halo box starts at column x0 - 2 so that its x coordinate is a multiple of 16 bytes
+// (68 columns x 34 rows, FP64); rows outside [0, Ny) and columns outside [0, Nx) arrive as
+// zeros, and the periodic columns -1 and Nx of the first and last tile column are patched
+// with plain loads once the box has landed. A wait that does not complete within
+// kTmaWaitLimit polls sets bit 1 of the control block's error flags and ends the CTA (after
+// waiting, again bounded, for its other copy in flight).
+constexpr int SB_W = ST_TX + 4, SB_H = ST_TY + 2;
+constexpr int SB_FIELD = ((SB_H * SB_W * 8 + 127) / 128) * 128;     // bytes per field, 128-byte aligned
+constexpr int SB_WN = ST_TX * ST_TY * 8;                          // omega^n tile (128-byte multiple)
+constexpr int SB_BUF = 2 * SB_FIELD + SB_WN;                       // psi + omega halos, omega^n tile
+constexpr unsigned SB_TX_BYTES = 2u * SB_H * SB_W * 8;             // bytes the two halo boxes deliver
+constexpr unsigned kTmaWaitLimit = 1u << 22;
+__host__ __device__ constexpr size_t stage_tma_smem_bytes() { return 2 * (size_t)SB_BUF + 128; }   // + alignment slack
+
+struct StageMaps {
+    CUtensorMap psi, w;      // halo boxes (SB_W x SB_H)
+    CUtensorMap wn;          // omega^n tile box (ST_TX x ST_TY), stages 2 and 3
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* ptr) { return (unsigned)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    for (unsigned it = 0; it < kTmaWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
+}
+
+static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_constant__ StageMaps maps, StageParams p) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    __shared__ __align__(8) uint64_t bars[2];
+    // the boxes land at 128-byte aligned shared addresses
+    unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int tiles_x = Nx / ST_TX, ntiles = tiles_x * ((Ny + ST_TY - 1) / ST_TY);
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async_smem();
     }
-    const int lx = threadIdx.x & (ST_TX - 1), g = threadIdx.x / ST_TX;
-    const int i = x0 + lx;
-    if (i >= Nx) return;
-    const int ly0 = g * ST_RPT;                         // first local row (tile row ly0 <-> smem row ly0 + 1)
-    double ps[3][3], om[3][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) { ps[r + 1][c] = sp[ly0 + r][lx + c]; om[r + 1][c] = so[ly0 + r][lx + c]; }
-#pragma unroll
-    for (int q = 0; q < ST_RPT; ++q) {
-        const int ly = ly0 + q, j = y0 + ly;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            ps[0][c] = ps[1][c]; ps[1][c] = ps[2][c]; ps[2][c] = sp[ly + 2][lx + c];
-            om[0][c] = om[1][c]; om[1][c] = om[2][c]; om[2][c] = so[ly + 2][lx + c];
+    __syncthreads();
+    auto issue = [&](int tile, int b) {
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        unsigned char* dst = smem_raw + b * SB_BUF;
+        mbar_expect_tx(&bars[b], SB_TX_BYTES + (p.stage > 1 ? (unsigned)SB_WN : 0u));
+        tma_load_2d(dst, &maps.psi, tx * ST_TX - 2, ty * ST_TY - 1, &bars[b]);
+        tma_load_2d(dst + SB_FIELD, &maps.w, tx * ST_TX - 2, ty * ST_TY - 1, &bars[b]);
+        if (p.stage > 1) tma_load_2d(dst + 2 * SB_FIELD, &maps.wn, tx * ST_TX, ty * ST_TY, &bars[b]);
+    };
+    const StageTime st = stage_time(p);
+    int k = 0;
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+        const int b = k & 1;
+        const int next = tile + gridDim.x;
+        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
+        const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
+        if (!ok) {
+            if (threadIdx.x == 0) {
+                atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
+                if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+            }
+            return;
         }
-        if (j >= Ny) break;
-        const double fj = __ldg(&p.rt.frow[j]);
-        const double wc = om[1][1];
-        double J = 0.0, lap = 0.0;
-        if (j != 0 && j != Ny - 1)
-            stencil_J_lap(ps, om, __ldg(&p.rt.a_node[j]), __ldg(&p.rt.a_edge[j]), __ldg(&p.rt.a_edge[j - 1]),
-                          p.inv_dx, p.inv_deta, p.inv_dx2, p.inv_deta2, J, lap);
-        double rhs = -J + p.nu * lap + fj - p.lin_drag * wc;                             // ops.cu:532
-        if (p.mms) rhs += mms_term(p, j, i, mA, mAp);
-        const size_t id = (size_t)j * Nx + i;
-        if (p.rhs_out) p.rhs_out[id] = rhs;
-        double wnew;
-        if (p.stage == 1) wnew = wc + dt * rhs;                                            // ops.cu:646
-        else if (p.stage == 2) wnew = 0.75 * p.w_n[id] + 0.25 * (wc + dt * rhs);           // ops.cu:650
-        else wnew = (1.0 / 3.0) * p.w_n[id] + (2.0 / 3.0) * (wc + dt * rhs);              // ops.cu:654
-        p.w_out[id] = wnew;
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        const int x0 = tx * ST_TX, y0 = ty * ST_TY;
+        double* sp = reinterpret_cast<double*>(smem_raw + b * SB_BUF);
+        double* so = reinterpret_cast<double*>(smem_raw + b * SB_BUF + SB_FIELD);
+        if (tx == 0 || tx == tiles_x - 1) {
+            // periodic halo columns: box column 1 is x = -1, box column ST_TX + 2 is x = Nx
+            for (int r = threadIdx.x; r < SB_H; r += blockDim.x) {
+                const int gy = y0 - 1 + r;
+                if (gy < 0 || gy >= Ny) continue;
+                if (tx == 0) {
+                    sp[r * SB_W + 1] = __ldg(&p.psi[(size_t)gy * Nx + Nx - 1]);
+                    so[r * SB_W + 1] = __ldg(&p.w_in[(size_t)gy * Nx + Nx - 1]);
+                }
+                if (tx == tiles_x - 1) {
+                    sp[r * SB_W + ST_TX + 2] = __ldg(&p.psi[(size_t)gy * Nx]);
+                    so[r * SB_W + ST_TX + 2] = __ldg(&p.w_in[(size_t)gy * Nx]);
+                }
+            }
+        }
+        __syncthreads();
+        stage_tile(p, st, sp, so, SB_W, 1, x0, y0,
+                   reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD));
+        fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
+        __syncthreads();
     }
 }
 
