@@ -119,6 +119,7 @@ struct Context {
     double* tbcarry = nullptr;     // [groups][nsb][2][32] block carries c, X
     unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
     int num_sms = 0;
+    int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false;
     int stage_tma_grid = 0;

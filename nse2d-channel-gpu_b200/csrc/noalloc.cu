@@ -36,6 +36,7 @@ constexpr int kMaxDevices = 64;
 struct DeviceSlot {
     MaxUvScratch* scratch = nullptr;
     int num_sms = 0;
+    int per_sm = 0;          // resident CTAs of the reduction kernel per SM
 };
 std::mutex g_slot_mutex;
 DeviceSlot g_slots[kMaxDevices];
@@ -43,7 +44,8 @@ DeviceSlot g_slots[kMaxDevices];
 
 static __device__ __align__(256) MaxUvScratch g_maxuv_scratch;
 
-// Address of this device's scratch and its SM count, looked up once per device.
+// Address of this device's scratch, its SM count and the reduction's occupancy, looked up once
+// per device.
 static int device_slot(DeviceSlot& out) {
     int dev = -1;
     NSE_CUDA_TRY(cudaGetDevice(&dev));
@@ -64,7 +66,10 @@ static int device_slot(DeviceSlot& out) {
         }
         int sms = 0;
         NSE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        int per_sm = 0;
+        NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt, 256, 0));
         slot.num_sms = sms > 0 ? sms : 1;
+        slot.per_sm = per_sm > 0 ? per_sm : 1;
         slot.scratch = static_cast<MaxUvScratch*>(ptr);
     }
     out = slot;
@@ -92,7 +97,7 @@ extern "C" int nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node,
     if (device_slot(slot)) return -1;
     // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, one partial slot each; the CTAs stride over
     // the interior rows, so every Ny is covered by that fixed number of slots.
-    const int grid = std::max(1, std::min(std::min(4 * slot.num_sms, Ny - 2), kMaxUvNoAllocBlocks));
+    const int grid = std::max(1, std::min(std::min(slot.per_sm * slot.num_sms, Ny - 2), kMaxUvNoAllocBlocks));
     MaxUvScratch* sc = slot.scratch;
     NSE_CUDA_TRY(cudaMemsetAsync(&sc->ctl, 0, sizeof(Ctl), s));
     MaxParams p{};

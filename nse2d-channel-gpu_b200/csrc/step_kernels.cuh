@@ -888,39 +888,60 @@ struct MaxParams {
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
-static __global__ void __launch_bounds__(256) k_maxuv_dt(MaxParams p) {
+// max |u|, |v|, |v| a over the interior (src/diag.cu:702-866). One row per CTA at a time; a
+// thread takes 4 adjacent columns (16-byte loads of rows j-1, j, j+1). The maxima of
+// |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| over a row are scaled once per row: for
+// positive factors, rounding is monotone, so max_i |a (d_i c)| = a (max_i |d_i| c) exactly and the
+// result is the reference's per-point maximum to the bit. A running sum of the differences
+// turns NaN or Inf anywhere into a non-finite flag.
+static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
-    double um = 0.0, vm = 0.0, vmm = 0.0;
-    int nonfinite = 0;
-    constexpr int U = 4;                       // independent points per thread and iteration
+    double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;
+    const double cy = 0.5 * p.inv_deta, cx = 0.5 * p.inv_dx;
     for (int j = 1 + blockIdx.x; j < Ny - 1; j += gridDim.x) {
-        const double a = __ldg(&p.a_node[j]);
         const double* rm = p.psi + (size_t)(j - 1) * Nx;
         const double* r0 = p.psi + (size_t)j * Nx;
         const double* rp = p.psi + (size_t)(j + 1) * Nx;
-        for (int i0 = threadIdx.x; i0 < Nx; i0 += U * blockDim.x) {
-            double up[U], dn[U], xp[U], xm[U];
+        double dym = 0.0, dxm = 0.0;
+        constexpr int U = 2;                           // column quads per thread and iteration
+        for (int q0 = threadIdx.x; 4 * q0 < Nx; q0 += U * blockDim.x) {
+            double2 a0[U], a1[U], u0[U], u1[U], d0[U], d1[U];
+            double xl[U], xr[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int i = i0 + u * blockDim.x;
-                if (i < Nx) {
-                    const int ip = (i + 1 < Nx) ? i + 1 : 0, im = (i > 0) ? i - 1 : Nx - 1;
-                    up[u] = __ldg(&rp[i]); dn[u] = __ldg(&rm[i]); xp[u] = __ldg(&r0[ip]); xm[u] = __ldg(&r0[im]);
+                const int c = 4 * (q0 + u * (int)blockDim.x);
+                if (c < Nx) {
+                    a0[u] = __ldg(reinterpret_cast<const double2*>(r0 + c));
+                    a1[u] = __ldg(reinterpret_cast<const double2*>(r0 + c + 2));
+                    u0[u] = __ldg(reinterpret_cast<const double2*>(rp + c));
+                    u1[u] = __ldg(reinterpret_cast<const double2*>(rp + c + 2));
+                    d0[u] = __ldg(reinterpret_cast<const double2*>(rm + c));
+                    d1[u] = __ldg(reinterpret_cast<const double2*>(rm + c + 2));
+                    xl[u] = __ldg(r0 + (c > 0 ? c - 1 : Nx - 1));
+                    xr[u] = __ldg(r0 + (c + 4 < Nx ? c + 4 : 0));
                 } else {
-                    up[u] = dn[u] = xp[u] = xm[u] = 0.0;
+                    a0[u] = a1[u] = u0[u] = u1[u] = d0[u] = d1[u] = make_double2(0.0, 0.0);
+                    xl[u] = xr[u] = 0.0;
                 }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double dpsideta = (up[u] - dn[u]) * (0.5 * p.inv_deta);
-                const double dpsidx = (xp[u] - xm[u]) * (0.5 * p.inv_dx);
-                const double uu = a * dpsideta, v = -dpsidx;
-                const double au = fabs(uu), av = fabs(v), avm = av * a;
-                if (!(au <= 1e300) || !(av <= 1e300)) nonfinite = 1;
-                um = fmax(um, au); vm = fmax(vm, av); vmm = fmax(vmm, avm);
+                const double e0 = u0[u].x - d0[u].x, e1 = u0[u].y - d0[u].y;
+                const double e2 = u1[u].x - d1[u].x, e3 = u1[u].y - d1[u].y;
+                const double f0 = a0[u].y - xl[u], f1 = a1[u].x - a0[u].x;
+                const double f2 = a1[u].y - a0[u].y, f3 = xr[u] - a1[u].x;
+                dym = fmax(dym, fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))));
+                dxm = fmax(dxm, fmax(fmax(fabs(f0), fabs(f1)), fmax(fabs(f2), fabs(f3))));
+                probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
             }
         }
+        const double a = __ldg(&p.a_node[j]);
+        const double av = dxm * cx;
+        um = fmax(um, a * (dym * cy));
+        vm = fmax(vm, av);
+        vmm = fmax(vmm, av * a);
     }
+    const int nonfinite = !(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300);
     __shared__ double s[3][256];
     __shared__ int snf;
     __shared__ bool last;
