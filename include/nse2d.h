@@ -107,6 +107,8 @@ int  nse2d_set_state(nse2d_ctx* ctx, const double* w, const double* psi, int whe
 int  nse2d_get_fields(nse2d_ctx* ctx, double* w, double* psi, int where, cudaStream_t s);
 /* Device pointer of a context field: 0 omega, 1 psi, 2 omega1, 3 omega2, 4 rhs, 5 J. */
 int  nse2d_field_ptr(nse2d_ctx* ctx, int which, double** d_ptr);
+/* Copy context field `which` (numbered as for nse2d_field_ptr) to a host array. Synchronous. */
+int  nse2d_get_field(nse2d_ctx* ctx, int which, double* host, cudaStream_t s);
 
 /* Advance nsteps SSPRK(3,3) steps, asynchronously. With adapt, dt is computed on the
  * device before every step (max |u|, |v|, |v| a, CFL and viscous limits, trimming to
@@ -121,6 +123,12 @@ int  nse2d_step_store_rhs(nse2d_ctx* ctx, int nsteps, cudaStream_t s);
  * receives the summed duration of the k-th kernel of a step over the nsteps steps
  * (nse2d_launches_per_step entries). Synchronous. */
 int  nse2d_step_timed(nse2d_ctx* ctx, int nsteps, double* kernel_ms, cudaStream_t s);
+/* One step (storing its stage-3 rhs, as nse2d_step_store_rhs) with CUDA events around every
+ * kernel: the step's device time, the time of its row transforms and of its tridiagonal
+ * solves, in ms (the step_ms, fft_ms and tridiag_ms columns of the reference's timing.csv,
+ * src/main.cu:746-753; any output may be NULL). Synchronous. */
+int  nse2d_step_profiled(nse2d_ctx* ctx, double* step_ms, double* fft_ms, double* tridiag_ms,
+                         cudaStream_t s);
 /* Name of the k-th kernel of a step. */
 const char* nse2d_step_kernel_name(nse2d_ctx* ctx, int k);
 /* Number of kernels one step launches. */
@@ -131,6 +139,34 @@ int  nse2d_set_schedule(nse2d_ctx* ctx, double next_snap, double next_diag, cuda
 /* Read t, dt, step count and the last max |u|, |v|, |v| a (any may be NULL). Synchronous. */
 int  nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, double* umax3,
                     cudaStream_t s);
+
+/* Run the time loop on the device (src/main.cu:434-551) until something needs the host:
+ * steps are taken inside one CUDA graph launch (a WHILE node around the captured step) and
+ * the run stops after the step at which
+ *   NSE2D_HALT_OUTPUT     t has reached min(next_snap, next_diag) (within the snap tolerance),
+ *   NSE2D_HALT_STATS      the step count is a multiple of stats_every (0: never),
+ *   NSE2D_HALT_END        t >= t_end - dt/2 (the reference's loop test),
+ *   NSE2D_HALT_NONFINITE  a reduction saw NaN/Inf (or a bounded wait timed out),
+ *   NSE2D_HALT_BUDGET     max_steps steps were taken;
+ * *reason receives those bits. dt is trimmed to the output times as in the reference. At least
+ * one step is taken. Synchronous. */
+#define NSE2D_HALT_OUTPUT    1
+#define NSE2D_HALT_STATS     2
+#define NSE2D_HALT_END       4
+#define NSE2D_HALT_NONFINITE 8
+#define NSE2D_HALT_BUDGET    16
+int  nse2d_run(nse2d_ctx* ctx, double next_snap, double next_diag, int stats_every, double t_end,
+               long long max_steps, int* reason, cudaStream_t s);
+/* Row sums over x of u, v, u^2, v^2 and u v of the current psi (src/diag.cu:468-499), neighbours
+ * clamped at the walls: out5 = [5][Ny] host array. Synchronous. */
+int  nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s);
+/* Add one sample of the 1-D spectra E_u(k), E_v(k) of the current psi (src/diag.cuh:123-191,
+ * src/diag.cu:868-898), with the project's own row FFT. Overwrites the stage buffers (fields 2
+ * and 3); call between steps. */
+int  nse2d_spectra_accumulate(nse2d_ctx* ctx, cudaStream_t s);
+/* kx = 2 pi k / Lx and the sample-averaged spectra, k = 0..Nx/2 (Nx/2+1 values each; any
+ * output may be NULL); *samples receives the sample count. Synchronous. */
+int  nse2d_spectra(nse2d_ctx* ctx, double* kx, double* Eu, double* Ev, int* samples, cudaStream_t s);
 
 /* Poisson solve of the reference (src/poisson.cuh:83-118): psi from omega, Dirichlet
  * psi = 0 / 2 h Ub at the walls on kx = 0. Device pointers, asynchronous. */

@@ -1,4 +1,6 @@
 // C ABI of the solver context (include/nse2d.h, group 2). Written for this project.
+#include <cstddef>
+#include <string>
 #include <cstring>
 #include <vector>
 
@@ -97,6 +99,16 @@ int nse2d_field_ptr(nse2d_ctx* ctx, int which, double** d_ptr) {
     return 0;
 }
 
+int nse2d_get_field(nse2d_ctx* ctx, int which, double* host, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    double* d = nullptr;
+    if (nse2d_field_ptr(ctx, which, &d)) return -1;
+    if (!host) { set_error("nse2d_get_field: null output"); return -1; }
+    NSE_CUDA_TRY(cudaMemcpyAsync(host, d, ctx->c->N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
 int nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s) {
     CHECK_CTX(ctx);
     return run_steps(ctx->c, nsteps, use_graph != 0, s, false);
@@ -124,6 +136,32 @@ int nse2d_step_timed(nse2d_ctx* ctx, int nsteps, double* kernel_ms, cudaStream_t
                 cudaEventElapsedTime(&ms, ev[(size_t)i * (nk + 1) + k], ev[(size_t)i * (nk + 1) + k + 1]);
                 kernel_ms[k] += ms;
             }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int nse2d_step_profiled(nse2d_ctx* ctx, double* step_ms, double* fft_ms, double* tridiag_ms, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const int nk = launches_per_step(c);
+    std::vector<cudaEvent_t> ev((size_t)nk + 1);
+    for (auto& e : ev) NSE_CUDA_TRY(cudaEventCreate(&e));
+    int rc = enqueue_step_timed(c, s, ev.data(), true);
+    if (rc == 0) {
+        NSE_CUDA_TRY(cudaStreamSynchronize(s));
+        double tot = 0.0, fft = 0.0, tri = 0.0;
+        for (int k = 0; k < nk; ++k) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            const std::string name = step_kernel_name(c, k);
+            tot += ms;
+            if (name.rfind("k_fft_fwd", 0) == 0 || name.rfind("k_ifft", 0) == 0) fft += ms;
+            if (name.rfind("k_thomas", 0) == 0) tri += ms;
+        }
+        if (step_ms) *step_ms = tot;
+        if (fft_ms) *fft_ms = fft;
+        if (tridiag_ms) *tridiag_ms = tri;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     return rc;
@@ -164,6 +202,63 @@ int nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, doubl
     if (dt) *dt = c->h_ctl->dt;
     if (step) *step = c->h_ctl->step;
     if (umax3) { umax3[0] = c->h_ctl->umax; umax3[1] = c->h_ctl->vmax; umax3[2] = c->h_ctl->vmaxm; }
+    return 0;
+}
+
+int nse2d_run(nse2d_ctx* ctx, double next_snap, double next_diag, int stats_every, double t_end,
+              long long max_steps, int* reason, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    if (max_steps <= 0) { set_error("nse2d_run: max_steps must be positive"); return -1; }
+    if (stats_every < 0) { set_error("nse2d_run: stats_every must be >= 0"); return -1; }
+    double sched[3] = {std::min(next_snap, next_diag), next_snap, next_diag};
+    NSE_CUDA_TRY(cudaMemcpyAsync(&c->ctl->next_out, sched, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    // the run fields form the tail of the control block, from run to t_end
+    Ctl* h = c->h_ctl;
+    h->run = 1; h->halt = 0; h->halt_reason = 0; h->stats_every = stats_every;
+    h->run_budget = max_steps; h->t_end = t_end;
+    const size_t off = offsetof(Ctl, run), len = offsetof(Ctl, t_end) + sizeof(double) - off;
+    NSE_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c->ctl) + off, reinterpret_cast<char*>(h) + off, len,
+                                 cudaMemcpyHostToDevice, s));
+    if (run_until_halt(c, s)) return -1;
+    NSE_CUDA_TRY(cudaMemcpyAsync(h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    if (reason) *reason = h->halt_reason;
+    const int zero = 0;
+    NSE_CUDA_TRY(cudaMemcpyAsync(&c->ctl->run, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    if (!out5) { set_error("nse2d_row_moments: null output"); return -1; }
+    return row_moments(ctx->c, out5, s);
+}
+
+int nse2d_spectra_accumulate(nse2d_ctx* ctx, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return spectra_accumulate(ctx->c, s);
+}
+
+int nse2d_spectra(nse2d_ctx* ctx, double* kx, double* Eu, double* Ev, int* samples, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    Context* c = ctx->c;
+    const int H = c->H;
+    std::vector<double> acc(2 * (size_t)c->Hp, 0.0);
+    if (c->spec_acc) {
+        NSE_CUDA_TRY(cudaMemcpyAsync(acc.data(), c->spec_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    const int n = c->spec_samples;
+    for (int k = 0; k < H; ++k) {
+        if (kx) kx[k] = (2.0 * 3.141592653589793 * (double)k) / c->cfg.Lx;   // fill_kx_array_kernel, diag.cu:868-873
+        double eu = acc[k], ev = acc[(size_t)c->Hp + k];
+        if (n > 0) { eu /= n; ev /= n; }
+        if (Eu) Eu[k] = eu;
+        if (Ev) Ev[k] = ev;
+    }
+    if (samples) *samples = n;
     return 0;
 }
 

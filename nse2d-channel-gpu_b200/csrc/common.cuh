@@ -56,7 +56,14 @@ struct Ctl {
     long long step;
     unsigned int blocks_done;      // last-block-done counter of the max reduction
     unsigned int ifft_done;        // last-block-done counter of the stage-3 inverse transform
-    int nonfinite;                 // set when a reduction saw NaN/Inf
+    int nonfinite;                 // bit 0: a reduction saw NaN/Inf; bit 1: a bounded wait timed out
+    // run mode (nse2d_run): stop stepping when an output, a statistics step or the end is due
+    int run;                       // 1 while a run is active
+    int halt;                      // set at the end of the step after which the run stops
+    int halt_reason;               // NSE2D_HALT_* bits
+    int stats_every;               // steps between statistics samples (0: none)
+    long long run_budget;          // steps a run may still take (a hard bound on the device loop)
+    double t_end;                  // the loop runs while t < t_end - dt/2 (src/main.cu:434)
 };
 
 // Row-constant tables (device), length Ny unless noted.
@@ -126,6 +133,10 @@ struct Context {
     CUtensorMap tm_psi{}, tm_w[3]{}, tm_wn{};
     cudaStream_t cap_stream = nullptr;     // private stream used only for graph capture
     cudaGraphExec_t graph_exec = nullptr;  // one captured step
+    cudaGraphExec_t run_exec = nullptr;    // WHILE(no halt) { step } for nse2d_run
+    double* spec_acc = nullptr;            // [2][Hp] accumulated E_u, E_v of the 1-D spectra
+    double* moments = nullptr;             // [5][Ny] row sums of u, v, u^2, v^2, u v
+    int spec_samples = 0;
     bool closure_diag = false;
 };
 

@@ -5,6 +5,7 @@
 // so its last digits depend on block scheduling. Here every row is reduced by one CTA into
 // per-row partials (fixed tree order), and the rows are then summed in row order with a
 // compensated (Neumaier) sum: the result is deterministic and at least as accurate.
+#include <algorithm>
 #include <cmath>
 #include <limits>
 
@@ -231,6 +232,89 @@ int diagnostics_row(Context* c, int t0_row, double* o, cudaStream_t s) {
     o[26] = C[S_T2_P] * iA;
     o[27] = nu * C[S_T2_ETA] * iA;
     o[28] = nu * C[S_T2_PHI] * iA;
+    return 0;
+}
+
+// ---- time-averaged profiles: row sums of u, v, u^2, v^2, u v (src/diag.cu:468-499) ----
+// One CTA per row (grid-stride over rows); u and v as the reference forms them, with the
+// neighbouring rows clamped at the walls; a fixed-order reduction, so the sums are
+// deterministic.
+static __global__ void __launch_bounds__(256) k_row_moments(const double* __restrict__ psi, const double* __restrict__ a_node,
+                                                           int Nx, int Ny, double inv_dx, double inv_deta,
+                                                           double* __restrict__ out) {
+    __shared__ double red[5][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int iy = blockIdx.x; iy < Ny; iy += gridDim.x) {
+        const int ym = (iy == 0 ? 0 : iy - 1), yp = (iy == Ny - 1 ? Ny - 1 : iy + 1);
+        const double a = a_node[iy];
+        double lu = 0.0, lv = 0.0, lu2 = 0.0, lv2 = 0.0, luv = 0.0;
+        for (int ix = threadIdx.x; ix < Nx; ix += blockDim.x) {
+            const int xm = (ix == 0 ? Nx - 1 : ix - 1), xp = (ix == Nx - 1 ? 0 : ix + 1);
+            const double u = (psi[(size_t)yp * Nx + ix] - psi[(size_t)ym * Nx + ix]) * 0.5 * inv_deta * a;
+            const double v = -(psi[(size_t)iy * Nx + xp] - psi[(size_t)iy * Nx + xm]) * 0.5 * inv_dx;
+            lu += u; lv += v; lu2 += u * u; lv2 += v * v; luv += u * v;
+        }
+        double vals[5] = {lu, lv, lu2, lv2, luv};
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
+        if (lane == 0)
+            for (int q = 0; q < 5; ++q) red[q][warp] = vals[q];
+        __syncthreads();
+        if (threadIdx.x < 5) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+            out[(size_t)threadIdx.x * Ny + iy] = t;
+        }
+        __syncthreads();
+    }
+}
+
+int row_moments(Context* c, double* out5, cudaStream_t s) {
+    if (!c->moments) {
+        NSE_CUDA_TRY(cudaMalloc((void**)&c->moments, sizeof(double) * 5 * (size_t)c->Ny));
+    }
+    const int grid = std::min(c->Ny, 8 * c->num_sms);
+    k_row_moments<<<grid, 256, 0, s>>>(c->psi, c->rt.a_node, c->Nx, c->Ny, c->inv_dx, c->inv_deta, c->moments);
+    NSE_CUDA_TRY(cudaGetLastError());
+    NSE_CUDA_TRY(cudaMemcpyAsync(out5, c->moments, sizeof(double) * 5 * (size_t)c->Ny, cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// ---- 1-D energy spectra in x (src/diag.cuh:123-191, src/diag.cu:868-898) ----
+// E(k) += w_k / (Nx^2 Ny) sum_j |f-hat_j(k)|^2 for k = 0..Nx/2, w_k = 2 inside the half
+// spectrum and 1 at k = 0 and Nx/2, summed over the rows in row order (one thread per k).
+static __global__ void k_spectra_reduce(const cpx<double>* __restrict__ hat, int Ny, int Hp, int H, double norm,
+                                        double* __restrict__ acc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= H) return;
+    const double wx = (k > 0 && k < H - 1) ? 2.0 : 1.0;
+    double sum = 0.0;
+    for (int j = 0; j < Ny; ++j) {
+        const cpx<double> z = hat[(size_t)j * Hp + k];
+        sum += (z.x * z.x + z.y * z.y);
+    }
+    acc[k] += norm * wx * sum;
+}
+
+// One spectra sample of the current psi: u and v (into the stage buffers, free between steps),
+// the row transforms of each (into the spectral buffer), and the row reduction.
+int spectra_accumulate(Context* c, cudaStream_t s) {
+    if (!c->spec_acc) {
+        NSE_CUDA_TRY(cudaMalloc((void**)&c->spec_acc, sizeof(double) * 2 * (size_t)c->Hp));
+        NSE_CUDA_TRY(cudaMemsetAsync(c->spec_acc, 0, sizeof(double) * 2 * (size_t)c->Hp, s));
+        c->spec_samples = 0;
+    }
+    if (uv_from_psi(c, c->psi, c->w1, c->w2, s)) return -1;
+    const double norm = 1.0 / ((double)c->Nx * (double)c->Nx * (double)c->Ny);
+    const int tb = 128, gb = (c->H + tb - 1) / tb;
+    for (int q = 0; q < 2; ++q) {
+        if (launch_fft_all_rows(c, q == 0 ? c->w1 : c->w2, s)) return -1;
+        k_spectra_reduce<<<gb, tb, 0, s>>>(c->hat, c->Ny, c->Hp, c->H, norm, c->spec_acc + (size_t)q * c->Hp);
+        NSE_CUDA_TRY(cudaGetLastError());
+    }
+    c->spec_samples += 1;
     return 0;
 }
 

@@ -18,11 +18,15 @@ int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s);
 int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s);
 int enqueue_step(Context* c, cudaStream_t s, bool store_rhs);
 int launches_per_step(const Context* c);
-int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev);
+int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev, bool store_rhs = false);
 const char* step_kernel_name(const Context* c, int k);
 int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs);
 int set_initial_omega(Context* c, cudaStream_t s);
 int diagnostics_row(Context* c, int t0_row, double* out29, cudaStream_t s);
 int rhs_at_state(Context* c, const double* w, const double* psi, double* J, double* rhs, double tm, cudaStream_t s);
 int uv_from_psi(Context* c, const double* psi, double* u, double* v, cudaStream_t s);
+int launch_fft_all_rows(Context* c, const double* src, cudaStream_t s);
+int run_until_halt(Context* c, cudaStream_t s);
+int row_moments(Context* c, double* out5, cudaStream_t s);
+int spectra_accumulate(Context* c, cudaStream_t s);
 }  // namespace nse2d

@@ -371,6 +371,9 @@ void context_destroy(Context* c) {
     if (c->ctl) cudaFree(c->ctl);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->run_exec) cudaGraphExecDestroy(c->run_exec);
+    if (c->spec_acc) cudaFree(c->spec_acc);
+    if (c->moments) cudaFree(c->moments);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
@@ -424,7 +427,7 @@ template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) 
     const size_t sm = fft_smem(M);
     NSE_CUDA_TRY(cudaFuncSetAttribute(k_fft_fwd<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     p.rows_per_cta = 1;
-    k_fft_fwd<M><<<c->Ni, IP_NT, sm, s>>>(p);
+    k_fft_fwd<M><<<p.nrows, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -460,6 +463,21 @@ int launch_fft_fwd(Context* c, const double* src, cudaStream_t s) {
     }
     FftParams p = fft_params(c);
     p.src = src;
+    p.row0 = 1;
+    p.nrows = c->Ni;
+    NSE_FFT_DISPATCH(fft_fwd_t)
+}
+
+// Forward transform of every row 0..Ny-1 of src into the spectral buffer (1-D spectra).
+int launch_fft_all_rows(Context* c, const double* src, cudaStream_t s) {
+    if (reinterpret_cast<uintptr_t>(src) % 16 != 0) {
+        set_error("the field must be 16-byte aligned for the row transform (got %p)", (const void*)src);
+        return -1;
+    }
+    FftParams p = fft_params(c);
+    p.src = src;
+    p.row0 = 0;
+    p.nrows = c->Ny;
     NSE_FFT_DISPATCH(fft_fwd_t)
 }
 
@@ -542,7 +560,9 @@ static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev
 }
 
 int enqueue_step(Context* c, cudaStream_t s, bool store_rhs) { return step_impl(c, s, store_rhs, nullptr); }
-int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev) { return step_impl(c, s, false, ev); }
+int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev, bool store_rhs) {
+    return step_impl(c, s, store_rhs, ev);
+}
 
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
@@ -579,6 +599,60 @@ int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store
         NSE_CUDA_TRY(e2);
     }
     for (int i = 0; i < nsteps; ++i) NSE_CUDA_TRY(cudaGraphLaunch(c->graph_exec, s));
+    return 0;
+}
+
+// Last node of the run loop's body: keep looping while no halt was requested and the step
+// budget lasts (the budget bounds the device loop whatever the schedule says).
+static __global__ void k_loop_cond(Ctl* ctl, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    ctl->run_budget -= 1;
+    if (!ctl->halt && ctl->run_budget <= 0) {
+        ctl->halt = 1;
+        ctl->halt_reason |= 16;
+    }
+    cudaGraphSetConditional(h, ctl->halt ? 0u : 1u);
+}
+
+// Steps on the device until advance_time or the budget requests a halt: one graph launch holds
+// a WHILE node whose body is one captured step followed by k_loop_cond. The run fields of the
+// control block must be set (run = 1, halt = 0, run_budget > 0) before the launch.
+int run_until_halt(Context* c, cudaStream_t s) {
+    if (!c->run_exec) {
+        if (!c->cap_stream) NSE_CUDA_TRY(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        NSE_CUDA_TRY(cudaGraphCreate(&g, 0));
+        auto fail = [&](const char* what, cudaError_t e) {
+            set_error("run graph: %s: %s", what, cudaGetErrorString(e));
+            cudaGraphDestroy(g);
+            return -1;
+        };
+        cudaGraphConditionalHandle h;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return fail("conditional handle", e);
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+        if (e != cudaSuccess) return fail("conditional node", e);
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(c->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail("capture", e);
+        // the step stores its stage-3 rhs, which the diagnostics row after a run pairs with omega
+        int rc = enqueue_step(c, c->cap_stream, true);
+        if (rc == 0) k_loop_cond<<<1, 32, 0, c->cap_stream>>>(c->ctl, h);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(c->cap_stream, &captured);
+        if (rc != 0) { cudaGraphDestroy(g); return -1; }
+        if (e != cudaSuccess) return fail("end capture", e);
+        e = cudaGraphInstantiate(&c->run_exec, g, 0);
+        cudaGraphDestroy(g);
+        NSE_CUDA_TRY(e);
+    }
+    NSE_CUDA_TRY(cudaGraphLaunch(c->run_exec, s));
     return 0;
 }
 

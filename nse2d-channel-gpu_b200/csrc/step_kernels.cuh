@@ -364,6 +364,20 @@ __device__ __forceinline__ void advance_time(Ctl* ctl) {
     if (nd < 1e299 && fabs(t - nd) <= fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)))) t = nd;
     ctl->t = t;
     ctl->step += 1;
+    if (ctl->run) {
+        // the host's output and loop tests of src/main.cu:434,553-566,695 after this step
+        // (with the wider snapshot tolerance, so that no due output is missed)
+        const double tol = fmax(time_tol_d(t), 1e-6 * fmax(1e-300, fabs(dt)));
+        int r = 0;
+        if (fmin(ns, nd) < 1e299 && t + tol >= fmin(ns, nd)) r |= 1;
+        if (ctl->stats_every > 0 && (ctl->step % ctl->stats_every) == 0) r |= 2;
+        if (!(t < ctl->t_end - 0.5 * dt)) r |= 4;
+        if (ctl->nonfinite & 2) r |= 8;     // a bounded wait gave up; NaN alone runs on, as in the reference
+        if (r) {
+            ctl->halt = 1;
+            ctl->halt_reason = r;
+        }
+    }
 }
 
 // ---- row FFT kernels ----
@@ -374,6 +388,7 @@ struct FftParams {
     const cpx<double>* tw;   // per-pass twiddle pairs of the M-point transform (pass_twiddle_table)
     const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
     int Nx, Ny, Hp, rows_per_cta;
+    int row0, nrows;         // forward: transform rows row0 .. row0 + nrows - 1
     // inverse only: Thom closure (src/ops.cu:102-158) and the closure_diag wall bookkeeping
     double* w;               // omega^(s+1): wall rows rewritten
     const double* dy_edge;
@@ -400,7 +415,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int IP_NT = 128;
 __host__ __device__ constexpr size_t fft_smem_bytes(int M) { return (size_t)ip_size(M) * 16; }
 
-// Forward real FFT of rows 1..Ny-2 (the reference's pack + cuFFT forward, src/poisson.cuh:93-96):
+// Forward real FFT of rows row0 .. row0 + nrows - 1: rows 1..Ny-2 in the Poisson solve (the
+// reference's pack + cuFFT forward, src/poisson.cuh:93-96), all rows for the 1-D spectra:
 // a row is read as M complex points z_n = x_2n + i x_2n+1, scattered by cp.async into the
 // digit-reversed layout; after the passes the split step writes X_k, k = 0..M:
 //   E_k = (Z_k + conj Z_{M-k}) / 2,  O_k = -i (Z_k - conj Z_{M-k}) / 2,  X_k = E_k + W_{2M}^k O_k.
@@ -408,8 +424,8 @@ template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
-    const int jb = 1 + blockIdx.x * p.rows_per_cta;
-    const int je = min(p.Ny - 1, jb + p.rows_per_cta);
+    const int jb = p.row0 + blockIdx.x * p.rows_per_cta;
+    const int je = min(p.row0 + p.nrows, jb + p.rows_per_cta);
     for (int j = jb; j < je; ++j) {
         const cpx<double>* row = reinterpret_cast<const cpx<double>*>(p.src + (size_t)j * p.Nx);
         for (int n = threadIdx.x; n < M; n += IP_NT) cp_async16(&buf[ip_idx(dit_pos<M>(n))], &row[n]);

@@ -70,16 +70,22 @@ def load(path=LIB_PATH):
         "nse2d_set_state": (I, [P, P, P, I, D, P]),
         "nse2d_get_fields": (I, [P, P, P, I, P]),
         "nse2d_field_ptr": (I, [P, I, ctypes.POINTER(P)]),
+        "nse2d_get_field": (I, [P, I, P, P]),
         "nse2d_step": (I, [P, I, I, P]),
         "nse2d_step_store_rhs": (I, [P, I, P]),
         "nse2d_launches_per_step": (I, [P]),
         "nse2d_step_timed": (I, [P, I, P, P]),
         "nse2d_step_kernel_name": (ctypes.c_char_p, [P, I]),
+        "nse2d_step_profiled": (I, [P, P, P, P, P]),
         "nse2d_set_dt": (I, [P, D, P]),
         "nse2d_set_schedule": (I, [P, D, D, P]),
         "nse2d_get_time": (I, [P, P, P, P, P, P]),
         "nse2d_poisson_solve": (I, [P, P, P, P]),
         "nse2d_max_uv": (I, [P, P, P]),
+        "nse2d_run": (I, [P, D, D, I, D, ctypes.c_longlong, P, P]),
+        "nse2d_row_moments": (I, [P, P, P]),
+        "nse2d_spectra_accumulate": (I, [P, P]),
+        "nse2d_spectra": (I, [P, P, P, P, P, P]),
         "nse2d_max_uv_noalloc": (I, [P, P, I, I, D, D, P, P]),
         "nse2d_diagnostics": (I, [P, I, P, P]),
         "nse2d_rhs_at_state": (I, [P, D, P]),
@@ -104,6 +110,9 @@ def load(path=LIB_PATH):
         f.argtypes = args
     _lib = lib
     return lib
+
+
+HALT_OUTPUT, HALT_STATS, HALT_END, HALT_NONFINITE, HALT_BUDGET = 1, 2, 4, 8, 16
 
 
 def _check(rc):
@@ -243,6 +252,31 @@ class Solver:
     def poisson_solve(self, w_dev, psi_dev, stream=None):
         """psi from omega (CUDA tensors [Ny,Nx] float64), the reference's Poisson2D_Z2Z::solve."""
         _check(self.lib.nse2d_poisson_solve(self.h, _ptr(w_dev), _ptr(psi_dev), _stream(stream)))
+
+    def run(self, next_snap=1e300, next_diag=1e300, stats_every=0, t_end=1e300, max_steps=1 << 40, stream=None):
+        """Step on the device until an output, statistics step, t_end, a non-finite value or
+        max_steps stops the run; returns the NSE2D_HALT_* bits."""
+        r = ctypes.c_int()
+        _check(self.lib.nse2d_run(self.h, float(next_snap), float(next_diag), int(stats_every), float(t_end),
+                                  int(max_steps), ctypes.byref(r), _stream(stream)))
+        return r.value
+
+    def row_moments(self, stream=None):
+        """Row sums over x of u, v, u^2, v^2, u v: array [5, Ny]."""
+        out = np.empty((5, self.Ny))
+        _check(self.lib.nse2d_row_moments(self.h, _ptr(out), _stream(stream)))
+        return out
+
+    def spectra_accumulate(self, stream=None):
+        _check(self.lib.nse2d_spectra_accumulate(self.h, _stream(stream)))
+
+    def spectra(self, stream=None):
+        """(kx, E_u, E_v, samples), sample-averaged, k = 0..Nx/2."""
+        H = self.Nx // 2 + 1
+        kx, eu, ev = np.empty(H), np.empty(H), np.empty(H)
+        n = ctypes.c_int()
+        _check(self.lib.nse2d_spectra(self.h, _ptr(kx), _ptr(eu), _ptr(ev), ctypes.byref(n), _stream(stream)))
+        return kx, eu, ev, n.value
 
     def max_uv(self, stream=None):
         out = (ctypes.c_double * 3)()

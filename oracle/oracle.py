@@ -76,6 +76,7 @@ def lib():
         L.or_arakawa_split.argtypes = [P, P, P, P, P, P, I, I, D, D, P]
         L.or_laplacian.argtypes = [P, P, I, I, D, D, P, P]
         L.or_grid_metrics.argtypes = [I, I, D, D, I, D, P, P, P, P, P]
+        L.or_row_moments.argtypes = [P, I, I, D, D, P, P, P, P, P, P]
         _lib = L
     return _lib
 

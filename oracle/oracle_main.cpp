@@ -5,7 +5,7 @@
 // loop with adaptive dt, output scheduling and diagnostics (src/main.cu:13-755), the
 // scheduling helpers (src/io.cu:93-178) and the profiles CSV (src/io.cu:262-312).
 // Snapshots are written in the raw side format "bin" (the reference declares SNAP_BIN
-// at src/io.cuh:28 but never implements it); see nse2d-channel-gpu_b200/host/snapshot.hpp
+// at src/io.cuh:28 but never implements it); see nse2d-channel-gpu_b200/host/snapshot.h
 // for the layout, which both writers follow.
 #include "nse2d_oracle.h"
 

@@ -34,7 +34,7 @@ def build_all():
     if not os.path.isfile(os.path.join(ORACLE, "_build", "liboracle.so")) or \
             not os.path.isfile(os.path.join(ORACLE, "_build", "nse2d_oracle")):
         subprocess.check_call(["make", "-s", "-C", ORACLE])
-    if not os.path.isfile(os.path.join(PKG, "libnse2d_b200.so")):
+    if not os.path.isfile(os.path.join(PKG, "libnse2d_b200.so")) or not os.path.isfile(os.path.join(PKG, "nse2d")):
         subprocess.check_call(["make", "-s", "-C", PKG, "-j4"])
 
 
