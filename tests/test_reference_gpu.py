@@ -1,0 +1,146 @@
+"""This build against the reference's own CUDA code, both on the same B200.
+
+oracle/_ref holds the reference compiled from its sources for sm_100a by oracle/ref.mk (its own
+flags, HDF5 off). The tests skip when it was not built (the reference's sources are not on every
+machine that runs the tests).
+
+1. The seven C-linkage operators of the reference's test API (src/test_api.cu:8-92) and this
+   library's, on the same device inputs: 1e-13 relative to the output's maximum (the same
+   formulas up to FMA contraction).
+2. The reference executable and nse2d on the same command lines: every diagnostics column of
+   every row equal to the 9 significant digits the CSV prints: 1e-8 of the value plus 2e-9 of
+   the column's scale (columns such as dOmega_rhs are small differences of O(1) sums), or 1e-13
+   absolute for columns that are round-off in both (tau_w at Ub = 0). The two
+   differ only by the order of the reductions and the FFT (cuFFT there, this project's here).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ORACLE, PKG
+
+pytestmark = pytest.mark.gpu
+
+REF_DIR = os.path.join(ORACLE, "_ref")
+REF_LIB = os.path.join(REF_DIR, "libnse2d_ref.so")
+REF_EXE = os.path.join(REF_DIR, "nse2d_ref")
+
+need_ref = pytest.mark.skipif(not (os.path.isfile(REF_LIB) and os.path.isfile(REF_EXE)),
+                              reason="the reference was not compiled here (oracle/ref.mk)")
+
+
+def ref_lib():
+    L = ctypes.CDLL(REF_LIB)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "testapi_uv_from_psi_mapped": [P, P, P, I, I, D, D, P, P],
+        "testapi_omega_from_psi_interior_mapped": [P, P, I, I, D, D, P, P, P],
+        "testapi_thom_wall_vorticity_mapped": [P, P, I, I, P, D, D, P],
+        "testapi_arakawa_J_mapped": [P, P, P, I, I, D, D, P, P],
+        "testapi_compute_adv_from_uv_mapped": [P, P, P, P, I, I, D, D, P, P],
+        "testapi_compute_adv_flux_mapped": [P, P, P, P, I, I, D, D, P, P],
+        "testapi_arakawa_J_mapped_split": [P, P, P, P, P, P, I, I, D, D, P, P],
+    }
+    for n, a in sig.items():
+        getattr(L, n).argtypes = a
+        getattr(L, n).restype = None
+    return L
+
+
+@need_ref
+def test_testapi_matches_reference(nse, cuda):
+    torch = cuda
+    mine = nse.load()
+    ref = ref_lib()
+    Nx, Ny = 256, 129
+    g = nse.Solver(Nx=Nx, Ny=Ny, Lx=2 * np.pi, stretch=1, beta=2.0)
+    an, ae, de = (torch.tensor(g.metric(k), dtype=torch.float64, device="cuda") for k in (1, 2, 3))
+    dx, deta = g.scalar(1), g.scalar(2)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    psi, w, u, v = (torch.randn(Ny, Nx, dtype=torch.float64, device="cuda", generator=gen) for _ in range(4))
+    P = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None   # noqa: E731
+    out = lambda: torch.zeros(Ny, Nx, dtype=torch.float64, device="cuda")   # noqa: E731
+
+    def both(fn):
+        a, b = fn(mine), fn(ref)
+        torch.cuda.synchronize()
+        for x, y in zip(a, b):
+            scale = float(y.abs().max())
+            assert float((x - y).abs().max()) <= 1e-13 * max(scale, 1e-300), (float((x - y).abs().max()), scale)
+
+    def uv(L):
+        a, b = out(), out()
+        L.testapi_uv_from_psi_mapped(P(psi), P(a), P(b), Nx, Ny, 1 / dx, 1 / deta, P(an), None)
+        return a, b
+
+    def om(L):
+        a = out()
+        L.testapi_omega_from_psi_interior_mapped(P(a), P(psi), Nx, Ny, 1 / dx**2, 1 / deta**2, P(an), P(ae), None)
+        return (a[1:-1],)
+
+    def thom(L):
+        a = w.clone()
+        L.testapi_thom_wall_vorticity_mapped(P(a), P(psi), Nx, Ny, P(de), 0.0, 2.0, None)
+        return (a,)
+
+    def jac(L):
+        a = out()
+        L.testapi_arakawa_J_mapped(P(psi), P(w), P(a), Nx, Ny, 1 / dx, 1 / deta, P(an), None)
+        return (a,)
+
+    def adv(L):
+        a, b = out(), out()
+        L.testapi_compute_adv_from_uv_mapped(P(u), P(v), P(w), P(a), Nx, Ny, 1 / dx, 1 / deta, P(an), None)
+        L.testapi_compute_adv_flux_mapped(P(u), P(v), P(w), P(b), Nx, Ny, 1 / dx, 1 / deta, P(an), None)
+        return a, b
+
+    def split(L):
+        r = [out() for _ in range(4)]
+        L.testapi_arakawa_J_mapped_split(P(psi), P(w), *[P(x) for x in r], Nx, Ny, 1 / dx, 1 / deta, P(an), None)
+        return r
+
+    for fn in (uv, om, thom, jac, adv, split):
+        both(fn)
+    g.close()
+
+
+CASES = {
+    "channel": ["--Nx", "512", "--Ny", "257", "--Ub", "1", "--Reb", "5000.0", "--init", "mix", "--amp", "0.05",
+                "--F0", "0.05", "--nforce", "12", "--drag", "0.001", "--stretch", "tanh", "--beta", "2",
+                "--tend", "0.2", "--diag_save", "0.05", "--closure_diag"],
+    "mms": ["--Nx", "128", "--Ny", "129", "--Ub", "0", "--nu", "0.01", "--init", "mms", "--mmsA0", "1.0",
+            "--mmsEps", "0.1", "--mmsOm", "1.0", "--mmsKx", "2", "--stretch", "tanh", "--beta", "2", "--no-adapt",
+            "--dt", "0.000125", "--tend", "0.25", "--diag_save", "0.05"],
+    "poiseuille": ["--Nx", "64", "--Ny", "129", "--Ub", "1.0", "--Reb", "500.0", "--init", "laminar", "--stretch",
+                   "tanh", "--beta", "2", "--tend", "1.0", "--diag_save", "0.25"],
+}
+
+
+def run(exe, args, out):
+    p = subprocess.run([exe] + args + ["--snap_save", "0", "--outdir", out], capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    return np.atleast_1d(np.genfromtxt(os.path.join(out, "diagnostics.csv"), delimiter=",", names=True))
+
+
+@need_ref
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_runs_match_reference_executable(cuda, tmp_path, case):
+    a = CASES[case]
+    ref = run(REF_EXE, a, str(tmp_path / "ref"))
+    mine = run(os.path.join(PKG, "nse2d"), a, str(tmp_path / "mine"))
+    assert len(mine) == len(ref) and len(ref) >= 3
+    for name in ref.dtype.names:
+        r, m = ref[name], mine[name]
+        fin = np.isfinite(r)
+        assert np.array_equal(fin, np.isfinite(m)), name
+        if name in ("utau_avg", "Cf", "Re_tau") and np.max(np.abs(ref["tauw_bot"])) < 1e-13:
+            continue
+        scale = max(float(np.max(np.abs(r[fin]))) if fin.any() else 0.0, 1e-300)
+        err = np.abs(m[fin] - r[fin])
+        # a column that is round-off in both (e.g. tau_w of a flow with Ub = 0) is held to 1e-13
+        tol = 1e-8 * np.abs(r[fin]) + max(2e-9 * scale, 1e-13)
+        assert np.all(err <= tol), (name, float(np.max(err)), scale)
