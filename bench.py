@@ -17,7 +17,10 @@ replayed K times, device events, max over ranks); `e2e` = the same metric throug
 ABI with host buffers (initial vorticity copied from pinned host memory, every step's t/dt/max
 read back to the host, final omega and psi copied back), all inside the timed region.
 --impl reference: the CPU restatement of the reference algorithm (the oracle, C++/OpenMP, all
-host threads) on the same configuration; the reference itself has no CPU path.
+host threads) on the same configuration; the reference itself has no CPU path. Where the
+reference was compiled from its sources (oracle/_ref), the line also carries
+`reference_cuda_b200`: the reference's own CUDA executable timed on this GPU, beside this
+project's executable in the same harness.
 Under torchrun (N > 1) every rank advances its own replica (the time step does not shard):
 value = steps of all ranks / max-over-ranks time.
 """
@@ -344,12 +347,53 @@ def cpu_baseline(args, sample_steps=3, max_seconds=60.0):
             "sample": f"{n} full SSPRK3 steps of the 4096x2049 workload (adaptive dt) after 1 warm-up step"}
 
 
+def exe_step_ms(exe, steps, warm=5):
+    """Median t_step_ms of the executable's --profile timing.csv (CUDA events around every step)
+    on the bench workload's grid and physics, started from --init mix (the reference's executable
+    has no way to take the seeded initial field); ~steps steps after the dt-limited start."""
+    import tempfile
+    W = WORKLOAD
+    dt_est = 5.06e-5                     # the viscous limit of this grid (cvisc 0.5), which sets dt
+    with tempfile.TemporaryDirectory() as out:
+        cmd = [exe, "--Nx", str(W["Nx"]), "--Ny", str(W["Ny"]), "--Lx", repr(W["Lx"]), "--h", "1", "--Ub", "1",
+               "--Reb", repr(W["Reb"]), "--stretch", "tanh", "--beta", repr(W["beta"]), "--F0", repr(W["F0"]),
+               "--nforce", str(W["nforce"]), "--drag", repr(W["lin_drag"]), "--cfl", repr(W["cfl"]),
+               "--dtmax", repr(W["dt_max"]), "--dt", repr(W["dt_init"]), "--init", "mix", "--amp", "0.05",
+               "--profile", "--timeEvery", "1", "--statsEvery", "100000000", "--snap_save", "0", "--diag_save", "0",
+               "--tend", repr((steps + warm) * dt_est), "--outdir", out]
+        subprocess.run(cmd, check=True, capture_output=True, timeout=900)
+        a = np.atleast_1d(np.genfromtxt(os.path.join(out, "timing.csv"), delimiter=",", names=True))
+    ms = a["t_step_ms"][warm:] if len(a) > warm else a["t_step_ms"]
+    return float(np.median(ms)), int(len(ms))
+
+
+def reference_cuda(steps):
+    """The reference's own CUDA solver compiled for sm_100a (oracle/_ref, by oracle/ref.mk) and this
+    project's nse2d executable, timed the same way on this GPU."""
+    exe = os.path.join(ORACLE, "_ref", "nse2d_ref")
+    if not os.path.isfile(exe):
+        return {"unavailable": "oracle/_ref/nse2d_ref was not built (the reference sources are not on this machine)"}
+    ref_ms, n = exe_step_ms(exe, steps)
+    ours_ms, _ = exe_step_ms(os.path.join(PKG, "nse2d"), steps)
+    return {"value": round(1e3 / ref_ms, 3), "unit": "steps/s", "ms_per_step": round(ref_ms, 4), "steps": n,
+            "ours_same_harness": {"value": round(1e3 / ours_ms, 3), "ms_per_step": round(ours_ms, 4)},
+            "how": "median t_step_ms of each executable's --profile timing.csv (CUDA events around each "
+                   "step; the reference's includes its three blocking max-reduction copies, ours the "
+                   "per-kernel events of a profiled step) at 4096x2049, --init mix, after 5 steps"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
     steps = max(1, min(args.steps, args.ref_steps))
     cb = cpu_baseline(args, sample_steps=steps, max_seconds=args.ref_seconds)
-    return {"metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
+    extra = {}
+    if args.ref_cuda_steps > 0:
+        try:
+            extra["reference_cuda_b200"] = reference_cuda(args.ref_cuda_steps)
+        except Exception as e:                                         # informational only
+            extra["reference_cuda_b200"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+    return {**extra, "metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
             "warmup": 1, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poiseuille + random vorticity)",
             "config": {"workload": "channel SSPRK3 step 4096x2049 FP64, tanh beta=2, Re_b=2e4, F0=0.05 n=12, "
@@ -389,6 +433,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-steps", type=int, default=20)
     ap.add_argument("--ref-seconds", type=float, default=120.0)
+    ap.add_argument("--ref-cuda-steps", type=int, default=40,
+                    help="reference arm: also time the reference's CUDA build (oracle/_ref) for K steps (0: off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.profile_steps > 0:
