@@ -402,6 +402,82 @@ def run_reference(args, world, rank):
             "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+ENSEMBLE_SEED = 20261203
+
+
+def ensemble_members(n=64, seed=ENSEMBLE_SEED):
+    """The survey's configuration 3: (Nx, Ny) uniform on {256, 512, 1024} x {129, 257, 513},
+    Re_b log-uniform on [2e3, 2e4], forcing mode in {4, 8, 12}; initial seeds 100 + i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        out.append(dict(Nx=int(rng.choice([256, 512, 1024])), Ny=int(rng.choice([129, 257, 513])),
+                        Reb=float(np.exp(rng.uniform(np.log(2e3), np.log(2e4)))), nforce=int(rng.choice([4, 8, 12])),
+                        seed=100 + i))
+    return out
+
+
+def run_ensemble(args):
+    """64 channels advanced by one graph launch per K steps (nse2d_ensemble, branch count chosen
+    by its autotuner) against the same 64 channels stepped one after another (each its own
+    graph replay). Metric: grid-point updates per second, sum_i Nx_i Ny_i K / time."""
+    import torch
+    nse = _load("nse2d_b200", os.path.join(PKG, "nse2d_b200.py"))
+    spec = ensemble_members()
+
+    def build():
+        sol = []
+        for m in spec:
+            W = dict(Lx=2 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, F0=0.05, lin_drag=1e-3, adapt=1, cfl=0.5,
+                     dt_max=1e-2, dt_init=1e-3, Nx=m["Nx"], Ny=m["Ny"], Reb=m["Reb"], nforce=m["nforce"])
+            s = nse.Solver(**W)
+            s.set_omega(initial_vorticity(m["Nx"], m["Ny"], W["Lx"], tanh_y(m["Ny"]), seed=m["seed"]))
+            sol.append(s)
+        return sol
+
+    K = args.steps
+    pts = sum(m["Nx"] * m["Ny"] for m in spec)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    members = build()
+    ens = nse.Ensemble(members)
+    groups, _ = ens.autotune(trial_steps=3, stream=stream)
+    ens.step(args.warmup, stream=stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    a.record(stream)
+    ens.step(K, stream=stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ens_ms = a.elapsed_time(b)
+    ens.close()
+    seq = build()
+    for s in seq:
+        s.step(args.warmup, use_graph=True, stream=stream)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for s in seq:
+        s.step(K, use_graph=True, stream=stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = a.elapsed_time(b)
+    for s in members + seq:
+        s.close()
+    return {"metric": "ensemble grid-point updates/s (64 channels, configuration 3, FP64)",
+            "value": round(pts * K / (ens_ms * 1e-3), 1), "unit": "points/s", "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "ms_per_step": round(ens_ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded laminar + random modes per member)",
+            "config": {"workload": "64 channels, (Nx,Ny) on {256,512,1024}x{129,257,513}, Re_b log-uniform "
+                                   "[2e3,2e4], nforce {4,8,12}, tanh beta=2, adaptive dt", "members": len(spec),
+                       "points": pts, "master_seed": ENSEMBLE_SEED, "branches": groups},
+            "sequential": {"value": round(pts * K / (seq_ms * 1e-3), 1), "unit": "points/s",
+                           "ms_per_step": round(seq_ms / K, 4),
+                           "how": "the same 64 channels, each replaying its own one-step graph K times, one after another"},
+            "speedup_vs_sequential": round(seq_ms / ens_ms, 3), "clocks": ck}
+
+
 def profile_steps(args):
     """A short, untimed run of the workload for profilers: initial solve, then K plain steps
     (no graph), so that every kernel launch is visible separately."""
@@ -436,9 +512,14 @@ def main():
     ap.add_argument("--ref-cuda-steps", type=int, default=40,
                     help="reference arm: also time the reference's CUDA build (oracle/_ref) for K steps (0: off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["channel", "ensemble"], default="channel",
+                    help="ensemble: the 64-channel batched ensemble (its own JSON line, 1 GPU)")
     args = ap.parse_args()
     if args.profile_steps > 0:
         profile_steps(args)
+        return
+    if args.workload == "ensemble":
+        print(json.dumps(run_ensemble(args)))
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -203,6 +203,26 @@ int  nse2d_metrics(nse2d_ctx* ctx, int which, double* out);
 /* Scalars: 0 nu, 1 dx, 2 deta, 3 invA_full, 4 meanFx_A, 5 psi_bot, 6 psi_top. */
 int  nse2d_scalar(nse2d_ctx* ctx, int which, double* out);
 
+/* ---------------------------------------------------------------------------------------
+ * 3. Batched ensembles (no counterpart in the reference, which runs one channel per process)
+ * ------------------------------------------------------------------------------------- */
+/* Many independent channels advanced by one graph launch: members are existing contexts (each
+ * with its own grid, physics, state and adaptive dt), which must outlive the ensemble. The
+ * graph's WHILE node repeats one step of every member; members are dealt round-robin onto
+ * `groups` concurrent branches. Results do not depend on the grouping. */
+typedef struct nse2d_ensemble nse2d_ensemble;
+int  nse2d_ensemble_create(nse2d_ctx* const* members, int n, nse2d_ensemble** out);
+int  nse2d_ensemble_destroy(nse2d_ensemble* e);
+/* Advance every member by nsteps steps in one graph launch, asynchronously on s. */
+int  nse2d_ensemble_step(nse2d_ensemble* e, int nsteps, cudaStream_t s);
+/* Use `groups` concurrent branches (1..n; rebuilds the graph). */
+int  nse2d_ensemble_set_groups(nse2d_ensemble* e, int groups);
+/* Time every power-of-two branch count (and n) over trial_steps steps each, keep the fastest,
+ * and report it and its time per ensemble step. The trials are real steps of every member
+ * (1 + trial_steps per candidate). Synchronous. */
+int  nse2d_ensemble_autotune(nse2d_ensemble* e, int trial_steps, int* groups_out, double* ms_per_step_out,
+                             cudaStream_t s);
+
 const char* nse2d_last_error(void);
 
 #ifdef __cplusplus

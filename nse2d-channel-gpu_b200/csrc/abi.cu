@@ -9,9 +9,6 @@
 
 using namespace nse2d;
 
-struct nse2d_ctx {
-    Context* c;
-};
 
 static Config to_config(const nse2d_config* a) {
     Config c;

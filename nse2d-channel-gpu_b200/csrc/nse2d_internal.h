@@ -30,3 +30,8 @@ int run_until_halt(Context* c, cudaStream_t s);
 int row_moments(Context* c, double* out5, cudaStream_t s);
 int spectra_accumulate(Context* c, cudaStream_t s);
 }  // namespace nse2d
+
+// The C ABI's handle: one solver context.
+struct nse2d_ctx {
+    nse2d::Context* c;
+};

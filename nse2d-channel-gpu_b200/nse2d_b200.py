@@ -77,6 +77,11 @@ def load(path=LIB_PATH):
         "nse2d_step_timed": (I, [P, I, P, P]),
         "nse2d_step_kernel_name": (ctypes.c_char_p, [P, I]),
         "nse2d_step_profiled": (I, [P, P, P, P, P]),
+        "nse2d_ensemble_create": (I, [P, I, ctypes.POINTER(P)]),
+        "nse2d_ensemble_destroy": (I, [P]),
+        "nse2d_ensemble_step": (I, [P, I, P]),
+        "nse2d_ensemble_set_groups": (I, [P, I]),
+        "nse2d_ensemble_autotune": (I, [P, I, P, P, P]),
         "nse2d_set_dt": (I, [P, D, P]),
         "nse2d_set_schedule": (I, [P, D, D, P]),
         "nse2d_get_time": (I, [P, P, P, P, P, P]),
@@ -316,3 +321,40 @@ class Testapi:
             conv = [_ptr(a) if hasattr(a, "data_ptr") or a is None else a for a in args]
             return f(*conv, _stream(stream))
         return call
+
+
+class Ensemble:
+    """Many Solver objects advanced together by one graph launch (nse2d_ensemble_*). The
+    solvers must stay alive while the ensemble exists."""
+
+    def __init__(self, solvers):
+        self.lib = load()
+        self.members = list(solvers)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = ctypes.c_void_p()
+        _check(self.lib.nse2d_ensemble_create(arr, len(self.members), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nse2d_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps=1, stream=None):
+        _check(self.lib.nse2d_ensemble_step(self.h, int(nsteps), _stream(stream)))
+
+    def set_groups(self, groups):
+        _check(self.lib.nse2d_ensemble_set_groups(self.h, int(groups)))
+
+    def autotune(self, trial_steps=5, stream=None):
+        """(branches, ms per ensemble step) of the fastest grouping, which stays selected."""
+        g, ms = ctypes.c_int(), ctypes.c_double()
+        _check(self.lib.nse2d_ensemble_autotune(self.h, int(trial_steps), ctypes.byref(g), ctypes.byref(ms),
+                                                _stream(stream)))
+        return g.value, ms.value
