@@ -43,6 +43,7 @@ ORACLE = os.path.join(ROOT, "oracle")
 WORKLOAD = dict(Nx=4096, Ny=2049, Lx=2 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, Reb=2.0e4, F0=0.05,
                 nforce=12, lin_drag=1e-3, adapt=1, cfl=0.5, dt_max=1e-2, dt_init=1e-3)
 METRIC = "SSPRK3 steps/s at 4096x2049 FP64"
+METRIC32 = "SSPRK3 steps/s at 4096x2049 FP32-bulk"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -79,20 +80,31 @@ def initial_vorticity(Nx, Ny, Lx, y, seed=1, amp=0.05, modes=64, Ub=1.0, h=1.0):
     return np.ascontiguousarray(w)
 
 
-def algorithmic_bytes_per_step(Nx, Ny, real_bytes=8):
+def algorithmic_bytes_per_step(Nx, Ny, real_bytes=8, spectral_bytes=None, table_bytes=None):
     """Algorithmic HBM bytes of one step (every input read once, every output written once):
     stage kernels read psi and omega^(s) (+ omega^n in stages 2, 3) and write omega^(s+1);
     each Poisson solve reads omega^(s+1), writes psi-hat and reads the elimination table cp;
-    each inverse transform reads psi-hat and writes psi."""
+    each inverse transform reads psi-hat and writes psi. The FP32-bulk variant has 4-byte fields
+    but keeps the spectral buffer (16 bytes per complex) and cp (8 bytes) in FP64."""
     N, H = Nx * Ny, Nx // 2 + 1
-    Rf, Cf, Tf = real_bytes, 2 * real_bytes, real_bytes
+    Rf = real_bytes
+    Cf = spectral_bytes if spectral_bytes is not None else 2 * real_bytes
+    Tf = table_bytes if table_bytes is not None else real_bytes
     return (Rf * N * (3 + 4 + 4) + 3 * (Rf * N + Cf * H * Ny + Tf * H * (Ny - 2)) + 3 * (Cf * H * Ny + Rf * N))
 
 
 def kernel_bytes(name, stage, Nx, Ny):
     """Algorithmic bytes of one launch of each kernel of this implementation (inputs read
-    once, outputs written once)."""
+    once, outputs written once); FP32-bulk kernels end in 32 (4-byte fields, FP64 spectra)."""
     N, H, Ni = Nx * Ny, Nx // 2 + 1, Ny - 2
+    if name == "k_stage32":
+        return 4 * N * (2 if stage == 1 else 3) + 4 * N
+    if name.startswith("k_fft_fwd32"):
+        return 4 * Nx * Ni + 16 * H * Ni
+    if name.startswith("k_ifft_thom32"):
+        return 16 * H * Ni + 4 * N + 4 * 6 * Nx
+    if name == "k_maxuv32":
+        return 4 * N
     if name.startswith("k_stage"):
         return 8 * N * (2 if stage == 1 else 3) + 8 * N          # psi, omega^(s) [, omega^n] -> omega^(s+1)
     if name == "k_fft_fwd":
@@ -205,6 +217,29 @@ def barrier(world):
         dist.barrier()
 
 
+def fp32_accuracy(nse, W, w0, steps=200):
+    """The FP32-bulk variant against FP64 from the same initial state after `steps` steps: relative
+    differences of the fields and of the diagnostics K, Omega, u_tau, Re_tau, C_f and the wall
+    enstrophy flux."""
+    a = nse.Solver(precision=64, **W)
+    b = nse.Solver(precision=32, **W)
+    a.set_omega(w0)
+    b.set_omega(w0)
+    a.step(steps, use_graph=True)
+    b.step(steps, use_graph=True)
+    wa, pa = a.fields()
+    wb, pb = b.fields()
+    da, db = a.diagnostics(), b.diagnostics()
+    out = {"steps": steps,
+           "omega_rel_max": float(np.max(np.abs(wb - wa)) / np.max(np.abs(wa))),
+           "psi_rel_max": float(np.max(np.abs(pb - pa)) / np.max(np.abs(pa)))}
+    for k in ("K", "Omega", "utau_avg", "Re_tau", "Cf", "BOmega_wall"):
+        out[k + "_rel"] = float(abs(db[k] - da[k]) / max(abs(da[k]), 1e-300))
+    a.close()
+    b.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -215,7 +250,8 @@ def run_ours(args, world, rank, local):
     w0 = initial_vorticity(Nx, Ny, W["Lx"], y, seed=1 + rank)
     pinned_w0 = torch.from_numpy(w0).pin_memory()
     stream = torch.cuda.Stream()
-    solver = nse.Solver(**W)
+    P = args.precision
+    solver = nse.Solver(precision=P, **W)
     solver.set_omega(pinned_w0.numpy(), stream=stream)
     with torch.cuda.stream(stream):
         solver.step(args.warmup, use_graph=True, stream=stream)
@@ -243,7 +279,7 @@ def run_ours(args, world, rank, local):
     # ---- e2e through the public API with host buffers ----
     host_w = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
     host_psi = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
-    solver2 = nse.Solver(**W)
+    solver2 = nse.Solver(precision=P, **W)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -264,8 +300,9 @@ def run_ours(args, world, rank, local):
     launches = solver.launches_per_step()
     solver.close()
 
+    accuracy = fp32_accuracy(nse, W, w0) if P == 32 else None
     N = Nx * Ny
-    B_step = algorithmic_bytes_per_step(Nx, Ny)
+    B_step = algorithmic_bytes_per_step(Nx, Ny) if P == 64 else algorithmic_bytes_per_step(Nx, Ny, 4, 16, 8)
     peak, peak_kind = hbm_peak()
     step_ms = ms_max / args.steps
     # per-kernel table; the dominant kernel carries the roofline object
@@ -294,12 +331,14 @@ def run_ours(args, world, rank, local):
     h2d = N * 8 / args.steps + 8 * 3
     d2h = 2 * N * 8 / args.steps + 128
     line = {
-        "metric": METRIC, "value": round(world * args.steps / (ms_max * 1e-3), 3), "unit": "steps/s",
+        "metric": METRIC if P == 64 else METRIC32, "value": round(world * args.steps / (ms_max * 1e-3), 3),
+        "unit": "steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if P == 64 else "f32 (FP64 base profiles, spectral buffer and tridiagonal solve)",
         "data": "synthetic (seeded Poiseuille + random vorticity over x-modes 1-64)",
-        "config": {"workload": "channel SSPRK3 step 4096x2049 FP64, tanh beta=2, Re_b=2e4, F0=0.05 n=12, "
-                               "drag 1e-3, adaptive dt CFL 0.5",
+        "config": {"workload": f"channel SSPRK3 step 4096x2049 {'FP64' if P == 64 else 'FP32-bulk'}, tanh beta=2, "
+                               "Re_b=2e4, F0=0.05 n=12, drag 1e-3, adaptive dt CFL 0.5",
                    "Nx": Nx, "Ny": Ny, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (each field 67 MB, step working set ~0.5 GB)",
                    "graph": "one CUDA graph per step, replayed"},
@@ -308,6 +347,8 @@ def run_ours(args, world, rank, local):
         "step_roofline": {"algorithmic_bytes_per_step": B_step, "achieved": round(step_gbs, 1), "peak": peak,
                           "unit": "GB/s", "frac": round(step_gbs / peak, 4), "frac_of_8TBs": round(step_gbs / 8000.0, 4)},
         "kernels": kernels,
+        **({"fp32_vs_fp64": accuracy,
+            "all_fp32_bytes_per_step": algorithmic_bytes_per_step(Nx, Ny, 4)} if P == 32 else {}),
         "e2e": {"value": round(world * args.steps / (e2e_ms * 1e-3), 3), "unit": "steps/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "wall_s": round(wall_e2e, 3)},
@@ -406,7 +447,7 @@ ENSEMBLE_SEED = 20261203
 
 
 def ensemble_members(n=64, seed=ENSEMBLE_SEED):
-    """The survey's configuration 3: (Nx, Ny) uniform on {256, 512, 1024} x {129, 257, 513},
+    """The 64-channel ensemble workload: (Nx, Ny) uniform on {256, 512, 1024} x {129, 257, 513},
     Re_b log-uniform on [2e3, 2e4], forcing mode in {4, 8, 12}; initial seeds 100 + i."""
     rng = np.random.default_rng(seed)
     out = []
@@ -512,6 +553,8 @@ def main():
     ap.add_argument("--ref-cuda-steps", type=int, default=40,
                     help="reference arm: also time the reference's CUDA build (oracle/_ref) for K steps (0: off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", type=int, choices=[64, 32], default=64,
+                    help="32: the FP32-bulk variant (its own metric line)")
     ap.add_argument("--workload", choices=["channel", "ensemble"], default="channel",
                     help="ensemble: the 64-channel batched ensemble (its own JSON line, 1 GPU)")
     args = ap.parse_args()

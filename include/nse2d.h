@@ -88,7 +88,11 @@ typedef struct nse2d_config {
     double mms_A0, mms_eps, mms_Om;
     int    mms_kx;
     int    closure_diag;      /* accumulate the wall-update enstrophy (Jwall columns) */
-    int    precision;         /* 64 */
+    int    precision;         /* 64 (FP64 throughout) or 32 (FP32 bulk with FP64 islands: the
+                                 x-mean base profiles, the spectral buffer and the tridiagonal
+                                 solve; no MMS forcing, no closure diagnostics). With 32, the
+                                 FP64 fields behind nse2d_field_ptr are refreshed only by the
+                                 calls that read them (fields, diagnostics, uv, statistics). */
 } nse2d_config;
 
 typedef struct nse2d_ctx nse2d_ctx;

@@ -21,6 +21,12 @@ static Config to_config(const nse2d_config* a) {
     return c;
 }
 
+// precision 32: refresh the FP64 fields (and the stored rhs) from the split FP32 state
+#define SYNC_FP64(ctx, with_rhs, s)                                                  \
+    do {                                                                             \
+        if ((ctx)->c->prec32 && export32((ctx)->c, (with_rhs), (s))) return -1;      \
+    } while (0)
+
 #define CHECK_CTX(ctx)                                    \
     do {                                                  \
         if (!(ctx) || !(ctx)->c) {                        \
@@ -73,12 +79,14 @@ int nse2d_set_state(nse2d_ctx* ctx, const double* w, const double* psi, int wher
     Ctl h{};
     h.t = t; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    if (c->prec32 && split32(c, s)) return -1;
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
 }
 
 int nse2d_get_fields(nse2d_ctx* ctx, double* w, double* psi, int where, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     Context* c = ctx->c;
     const cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (w) NSE_CUDA_TRY(cudaMemcpyAsync(w, c->w, c->N * sizeof(double), k, s));
@@ -98,6 +106,7 @@ int nse2d_field_ptr(nse2d_ctx* ctx, int which, double** d_ptr) {
 
 int nse2d_get_field(nse2d_ctx* ctx, int which, double* host, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, which == 4, s);
     double* d = nullptr;
     if (nse2d_field_ptr(ctx, which, &d)) return -1;
     if (!host) { set_error("nse2d_get_field: null output"); return -1; }
@@ -229,12 +238,14 @@ int nse2d_run(nse2d_ctx* ctx, double next_snap, double next_diag, int stats_ever
 
 int nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     if (!out5) { set_error("nse2d_row_moments: null output"); return -1; }
     return row_moments(ctx->c, out5, s);
 }
 
 int nse2d_spectra_accumulate(nse2d_ctx* ctx, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     return spectra_accumulate(ctx->c, s);
 }
 
@@ -275,6 +286,7 @@ int nse2d_poisson_solve(nse2d_ctx* ctx, const double* d_w, double* d_psi, cudaSt
 
 int nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     Context* c = ctx->c;
     if (launch_maxuv(c, c->psi, false, s)) return -1;
     return nse2d_get_time(ctx, nullptr, nullptr, nullptr, out3, s);
@@ -282,11 +294,13 @@ int nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s) {
 
 int nse2d_diagnostics(nse2d_ctx* ctx, int t0_row, double* out29, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, t0_row == 0, s);
     return diagnostics_row(ctx->c, t0_row, out29, s);
 }
 
 int nse2d_rhs_at_state(nse2d_ctx* ctx, double t, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     Context* c = ctx->c;
     if (rhs_at_state(c, c->w, c->psi, c->J, c->rhs, t, s)) return -1;
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
@@ -295,6 +309,7 @@ int nse2d_rhs_at_state(nse2d_ctx* ctx, double t, cudaStream_t s) {
 
 int nse2d_uv(nse2d_ctx* ctx, double* d_u, double* d_v, cudaStream_t s) {
     CHECK_CTX(ctx);
+    SYNC_FP64(ctx, false, s);
     return uv_from_psi(ctx->c, ctx->c->psi, d_u, d_v, s);
 }
 

@@ -127,6 +127,14 @@ struct Context {
     unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
     int num_sms = 0;
     int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
+    // FP32-bulk variant (precision 32): base profiles (FP64) and FP32 fluctuations
+    bool prec32 = false;
+    float *wf = nullptr, *w1f = nullptr, *w2f = nullptr, *psif = nullptr, *rhsf = nullptr;
+    double *wbar = nullptr, *psibar = nullptr;
+    float* rc32 = nullptr;                 // [RC32_N][Ny] row constants of the FP32 stage
+    cpx<float> *twf = nullptr, *wNf = nullptr;
+    double wall_bot32 = 0.0, wall_top32 = 0.0;
+    int maxuv32_grid = 0;
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false;
     int stage_tma_grid = 0;

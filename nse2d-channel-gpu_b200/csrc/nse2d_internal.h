@@ -11,6 +11,15 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
                  double* rhs_out = nullptr);
 int launch_fft_fwd(Context* c, const double* src, cudaStream_t s);
 int launch_thomas(Context* c, cudaStream_t s);
+int launch_thomas_maps(Context* c, cudaStream_t s, bool homog = false);
+int launch_thomas_apply(Context* c, cudaStream_t s, bool homog = false);
+// FP32-bulk variant (csrc/solver32.cu)
+int setup32(Context* c);
+void destroy32(Context* c);
+int split32(Context* c, cudaStream_t s);
+int export32(Context* c, bool with_rhs, cudaStream_t s);
+int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev);
+const char* step32_kernel_name(const Context* c, int k);
 int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom, bool closure, cudaStream_t s,
                      bool advance = false);
 int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s);

@@ -61,13 +61,15 @@ int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>
     return 0;
 }
 
-static ThomasParams thomas_params(const Context* c) {
+// homog: zero wall values of psi (the FP32 variant solves for psi', which vanishes on the walls)
+static ThomasParams thomas_params(const Context* c, bool homog = false) {
     ThomasParams p{};
     p.hat = c->hat; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
     p.tconst = c->tconst; p.tmaps = c->tmaps; p.tblk = c->tblk; p.tbcarry = c->tbcarry; p.tcount = c->tcount;
     p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni;
     p.nseg = c->thomas_nseg; p.nsb = c->thomas_nsb;
-    p.psi_bot = c->psi_bot; p.psi_top = c->psi_top;
+    p.psi_bot = homog ? 0.0 : c->psi_bot;
+    p.psi_top = homog ? 0.0 : c->psi_top;
     return p;
 }
 
@@ -207,7 +209,11 @@ int context_create(const Config& cfg, Context** out) {
     }
     if (cfg.Ny < 5) { set_error("Ny = %d: need Ny >= 5", cfg.Ny); return -1; }
     if (cfg.Nx > 16384) { set_error("Nx = %d exceeds 16384", cfg.Nx); return -1; }
-    if (cfg.precision != 64) { set_error("precision %d not built (64 only)", cfg.precision); return -1; }
+    if (cfg.precision != 64 && cfg.precision != 32) { set_error("precision %d: 64 or 32", cfg.precision); return -1; }
+    if (cfg.precision == 32 && (cfg.mms || cfg.closure_diag)) {
+        set_error("precision 32 (FP32 bulk) runs without the MMS forcing and the closure diagnostics");
+        return -1;
+    }
     auto* c = new Context();
     c->cfg = cfg;
     c->Nx = cfg.Nx; c->Ny = cfg.Ny; c->N = (size_t)cfg.Nx * cfg.Ny;
@@ -346,6 +352,10 @@ int context_create(const Config& cfg, Context** out) {
         const int ntiles = (c->Nx / ST_TX) * ((Ny + ST_TY - 1) / ST_TY);
         c->stage_tma_grid = std::min(ntiles, per_sm * c->num_sms);
     }
+    if (cfg.precision == 32) {
+        c->prec32 = true;
+        if (setup32(c)) return fail();
+    }
     Ctl h{};
     h.t = 0.0; h.dt = cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     if (cudaMemcpy(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess) { set_error("ctl upload"); return fail(); }
@@ -372,6 +382,7 @@ void context_destroy(Context* c) {
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->run_exec) cudaGraphExecDestroy(c->run_exec);
+    destroy32(c);
     if (c->spec_acc) cudaFree(c->spec_acc);
     if (c->moments) cudaFree(c->moments);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -491,13 +502,13 @@ int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom
 
 // The two passes of the segmented Thomas solve: the segment maps (and, in the last CTA of each
 // column group, the carries), then the rerun of every segment from its carries.
-static int launch_thomas_maps(Context* c, cudaStream_t s) {
-    k_thomas_maps<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c));
+int launch_thomas_maps(Context* c, cudaStream_t s, bool homog) {
+    k_thomas_maps<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c, homog));
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
-static int launch_thomas_apply(Context* c, cudaStream_t s) {
-    k_thomas_apply<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c));
+int launch_thomas_apply(Context* c, cudaStream_t s, bool homog) {
+    k_thomas_apply<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c, homog));
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -536,6 +547,7 @@ int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s) {
 // One SSPRK(3,3) step (src/main.cu:439-541) with dt from the control block. With ev != nullptr
 // an event is recorded before the step and after every kernel (for per-kernel timing).
 static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
+    if (c->prec32) return step32_impl(c, s, store_rhs, ev);
     int k = 0;
     auto mark = [&]() -> int {
         if (ev) NSE_CUDA_TRY(cudaEventRecord(ev[k++], s));
@@ -566,6 +578,7 @@ int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev, bool store_r
 
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
+    if (c->prec32) return step32_kernel_name(c, k);
     static const char* stage[5] = {"k_stage", "k_fft_fwd", "k_thomas_maps", "k_thomas_apply", "k_ifft_thom"};
     if (c->cfg.adapt) {
         if (k == 0) return "k_maxuv_dt";
@@ -660,6 +673,7 @@ int run_until_halt(Context* c, cudaStream_t s) {
 int set_initial_omega(Context* c, cudaStream_t s) {
     if (poisson_solve(c, c->w, c->psi, s)) return -1;
     if (launch_thom(c, c->w, c->psi, s)) return -1;
+    if (c->prec32 && split32(c, s)) return -1;
     Ctl h{};
     h.t = 0.0; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));

@@ -904,6 +904,64 @@ struct MaxParams {
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
+// The block maxima of one reduction CTA, the last-CTA fold of all CTAs' partials, and dt from
+// the reference's formula with the output trimming (src/main.cu:439-480). All threads call it.
+__device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, double vm, double vmm, int nonfinite) {
+    __shared__ double s[3][256];
+    __shared__ int snf;
+    __shared__ bool last;
+    if (threadIdx.x == 0) snf = 0;
+    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
+    __syncthreads();
+    if (nonfinite) atomicOr(&snf, 1);
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 3; ++c) p.blocks[blockIdx.x * 3 + c] = s[c][0];
+        if (snf) atomicOr(&p.ctl->nonfinite, 1);
+        __threadfence();
+        const unsigned int done = atomicAdd(&p.ctl->blocks_done, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    um = 0.0; vm = 0.0; vmm = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        um = fmax(um, __ldcg(&p.blocks[b * 3 + 0]));
+        vm = fmax(vm, __ldcg(&p.blocks[b * 3 + 1]));
+        vmm = fmax(vmm, __ldcg(&p.blocks[b * 3 + 2]));
+    }
+    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st)
+            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    Ctl* ctl = p.ctl;
+    ctl->blocks_done = 0;
+    ctl->umax = s[0][0]; ctl->vmax = s[1][0]; ctl->vmaxm = s[2][0];
+    if (!p.set_dt || !p.adapt) return;
+    const double umax = s[0][0], vmaxm = s[2][0];
+    const double dt_x = (umax > 0 ? p.cfl * (p.dx / umax) : 1e30);
+    const double dt_y = (vmaxm > 0 ? p.cfl * (p.deta / vmaxm) : 1e30);
+    const double dt_adv = fmin(dt_x, dt_y);
+    const double dt_vis = (p.nu > 0) ? p.cvisc * 0.5 / (p.nu * (p.inv_dx2 + p.inv_dymin2)) : 1e30;
+    double dt = fmin(p.dt_max, fmin(dt_adv, dt_vis));
+    const double t_next = ctl->next_out;
+    if (t_next < 1e299) {
+        const double rem = t_next - ctl->t;
+        const double tol = fmax(time_tol_d(t_next), 1e-6 * dt);
+        if (rem > tol && rem < 0.5 * dt) dt = rem;
+    }
+    ctl->dt = dt;
+}
+
 // max |u|, |v|, |v| a over the interior (src/diag.cu:702-866). One row per CTA at a time; a
 // thread takes 4 adjacent columns (16-byte loads of rows j-1, j, j+1). The maxima of
 // |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| over a row are scaled once per row: for
@@ -958,59 +1016,7 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
         vmm = fmax(vmm, av * a);
     }
     const int nonfinite = !(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300);
-    __shared__ double s[3][256];
-    __shared__ int snf;
-    __shared__ bool last;
-    if (threadIdx.x == 0) snf = 0;
-    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
-    __syncthreads();
-    if (nonfinite) atomicOr(&snf, 1);
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st)
-            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < 3; ++c) p.blocks[blockIdx.x * 3 + c] = s[c][0];
-        if (snf) atomicOr(&p.ctl->nonfinite, 1);
-        __threadfence();
-        const unsigned int done = atomicAdd(&p.ctl->blocks_done, 1u);
-        last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    um = 0.0; vm = 0.0; vmm = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        um = fmax(um, __ldcg(&p.blocks[b * 3 + 0]));
-        vm = fmax(vm, __ldcg(&p.blocks[b * 3 + 1]));
-        vmm = fmax(vmm, __ldcg(&p.blocks[b * 3 + 2]));
-    }
-    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st)
-            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
-    Ctl* ctl = p.ctl;
-    ctl->blocks_done = 0;
-    ctl->umax = s[0][0]; ctl->vmax = s[1][0]; ctl->vmaxm = s[2][0];
-    if (!p.set_dt || !p.adapt) return;
-    const double umax = s[0][0], vmaxm = s[2][0];
-    const double dt_x = (umax > 0 ? p.cfl * (p.dx / umax) : 1e30);
-    const double dt_y = (vmaxm > 0 ? p.cfl * (p.deta / vmaxm) : 1e30);
-    const double dt_adv = fmin(dt_x, dt_y);
-    const double dt_vis = (p.nu > 0) ? p.cvisc * 0.5 / (p.nu * (p.inv_dx2 + p.inv_dymin2)) : 1e30;
-    double dt = fmin(p.dt_max, fmin(dt_adv, dt_vis));
-    const double t_next = ctl->next_out;
-    if (t_next < 1e299) {
-        const double rem = t_next - ctl->t;
-        const double tol = fmax(time_tol_d(t_next), 1e-6 * dt);
-        if (rem > tol && rem < 0.5 * dt) dt = rem;
-    }
-    ctl->dt = dt;
+    maxuv_finish(p, um, vm, vmm, nonfinite);
 }
 
 }  // namespace nse2d

@@ -115,6 +115,7 @@ Args parse(int argc, char** argv) {
         else if (eq("--spectraEvery") && has()) a.spectraEvery = std::atoi(argv[++i]);
         else if (eq("--outdir") && has()) a.outdir = argv[++i];
         else if (eq("--free_slip")) c.free_slip = 1;
+        else if (eq("--fp32")) c.precision = 32;                      // FP32-bulk variant (this build)
     }
     if (a.ic.init == "laminar" && a.rand_amp > 0.0 && a.ic.amp <= 0.0) {   // init.cu:91-93
         a.ic.init = "rand";

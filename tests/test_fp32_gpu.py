@@ -1,0 +1,87 @@
+"""The FP32-bulk variant (precision 32) against the FP64 path, on a B200.
+
+The variant steps FP32 fluctuations about fixed FP64 base profiles (the x-means of the initial
+state) with the spectral buffer and the tridiagonal solve in FP64. Its error is FP32 rounding of
+the fluctuations, so the bars here are FP32-level:
+  - split and export of the initial state: 1e-6 of max |omega| / max |psi|;
+  - one step: 2e-5 of max |omega| and 1e-5 of max |psi|;
+  - 200 steps of a forced turbulent-ish channel: 1e-3 of max |omega|, and the diagnostics K,
+    Omega, u_tau, Re_tau, C_f and the wall enstrophy flux BOmega_wall within 1e-3 relative.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(Nx=256, Ny=129, Lx=2 * np.pi, stretch=1, beta=2.0, Ub=1.0, Reb=5000.0, F0=0.05, nforce=8,
+           lin_drag=1e-3, adapt=1, cfl=0.5)
+
+
+def omega0(Nx, Ny, y, seed=4, amp=0.1):
+    rng = np.random.default_rng(seed)
+    x = np.arange(Nx) * (2 * np.pi / Nx)
+    w = np.repeat((3.0 * y)[:, None], Nx, axis=1)
+    for m in range(1, 17):
+        w += amp * rng.standard_normal() * np.cos(m * x + 2 * np.pi * rng.random())[None, :] * \
+            np.sin(rng.integers(1, 7) * np.pi * (y + 1) / 2)[:, None]
+    w[0], w[-1] = 3.0 * y[0], 3.0 * y[-1]
+    return w
+
+
+def pair(nse, **kw):
+    cfg = dict(CFG, **kw)
+    a = nse.Solver(**cfg)
+    b = nse.Solver(precision=32, **cfg)
+    w0 = omega0(a.Nx, a.Ny, a.metric(0))
+    a.set_omega(w0)
+    b.set_omega(w0)
+    return a, b
+
+
+def rel(x, ref):
+    return float(np.max(np.abs(x - ref)) / np.max(np.abs(ref)))
+
+
+def test_split_and_export(nse, cuda):
+    a, b = pair(nse)
+    wa, pa = a.fields()
+    wb, pb = b.fields()
+    assert rel(wb, wa) < 1e-6 and rel(pb, pa) < 1e-6
+
+
+def test_one_step(nse, cuda):
+    a, b = pair(nse)
+    a.step(1)
+    b.step(1)
+    assert b.time()[:3] == pytest.approx(a.time()[:3], rel=1e-6)
+    wa, pa = a.fields()
+    wb, pb = b.fields()
+    assert rel(wb, wa) < 2e-5, rel(wb, wa)
+    assert rel(pb, pa) < 1e-5, rel(pb, pa)
+
+
+@pytest.mark.parametrize("walls", ["no_slip", "free_slip"])
+def test_200_steps_and_diagnostics(nse, cuda, walls):
+    a, b = pair(nse, free_slip=1 if walls == "free_slip" else 0)
+    a.step(200, use_graph=True)
+    b.step(200, use_graph=True)
+    wa, _ = a.fields()
+    wb, _ = b.fields()
+    assert rel(wb, wa) < 1e-3, rel(wb, wa)
+    da, db = a.diagnostics(), b.diagnostics()
+    for k in ("K", "Omega", "utau_avg", "Re_tau", "Cf", "BOmega_wall"):
+        if walls == "free_slip" and k in ("utau_avg", "Re_tau", "Cf"):
+            continue
+        assert abs(db[k] - da[k]) <= 1e-3 * abs(da[k]) + 1e-12, (k, db[k], da[k])
+
+
+def test_run_loop_and_ensemble(nse, cuda):
+    a, b = pair(nse)
+    r = b.run(stats_every=25)
+    assert r == nse.HALT_STATS and b.time()[2] == 25
+    c = nse.Solver(precision=32, **CFG)
+    c.set_omega(omega0(c.Nx, c.Ny, c.metric(0)))
+    e = nse.Ensemble([c])
+    e.step(25)
+    assert np.array_equal(c.fields()[0], b.fields()[0])
+    e.close()
