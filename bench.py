@@ -109,6 +109,8 @@ def kernel_bytes(name, stage, Nx, Ny):
         return 8 * N * (2 if stage == 1 else 3) + 8 * N          # psi, omega^(s) [, omega^n] -> omega^(s+1)
     if name == "k_fft_fwd":
         return 8 * Nx * Ni + 16 * H * Ni                         # omega^(s+1) rows -> omega-hat
+    if name == "k_thomas_cluster":
+        return 16 * H * Ni + 8 * H * Ni + 16 * H * Ny            # omega-hat and cp read, psi-hat written
     if name == "k_thomas_maps":
         return 16 * H * Ni + 8 * H * Ni                          # omega-hat, cp read once
     if name == "k_thomas_apply":

@@ -125,6 +125,12 @@ struct Context {
     double* tblk = nullptr;        // [groups][nsb][5][32] block aggregates
     double* tbcarry = nullptr;     // [groups][nsb][2][32] block carries c, X
     unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
+    // one-pass cluster solve (k_thomas_cluster<L>): CTAs per cluster, rows per segment, resident
+    // clusters (the persistent grid), dynamic shared memory, TMA maps of omega-hat and cp
+    bool thomas_cluster = false;
+    int tc_cluster = 0, tc_L = 0, tc_nclusters = 0;
+    size_t tc_smem = 0;
+    CUtensorMap tm_hat{}, tm_cp{};
     int num_sms = 0;
     int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
     // FP32-bulk variant (precision 32): base profiles (FP64) and FP32 fluctuations

@@ -13,6 +13,10 @@ int launch_fft_fwd(Context* c, const double* src, cudaStream_t s);
 int launch_thomas(Context* c, cudaStream_t s);
 int launch_thomas_maps(Context* c, cudaStream_t s, bool homog = false);
 int launch_thomas_apply(Context* c, cudaStream_t s, bool homog = false);
+int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog = false);
+int thomas_launches(const Context* c);
+const char* thomas_kernel_name(const Context* c, int i);
+int launch_thomas_part(Context* c, int i, cudaStream_t s, bool homog = false);
 // FP32-bulk variant (csrc/solver32.cu)
 int setup32(Context* c);
 void destroy32(Context* c);

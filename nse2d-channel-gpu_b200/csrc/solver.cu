@@ -61,6 +61,18 @@ int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>
     return 0;
 }
 
+using ThomasClusterKernel = void (*)(ThomasMaps, ThomasParams);
+static ThomasClusterKernel thomas_cluster_kernel(int L) {
+    switch (L) {
+        case 1: return k_thomas_cluster<1>;
+        case 2: return k_thomas_cluster<2>;
+        case 4: return k_thomas_cluster<4>;
+        case 8: return k_thomas_cluster<8>;
+        case 16: return k_thomas_cluster<16>;
+        default: return nullptr;
+    }
+}
+
 // homog: zero wall values of psi (the FP32 variant solves for psi', which vanishes on the walls)
 static ThomasParams thomas_params(const Context* c, bool homog = false) {
     ThomasParams p{};
@@ -68,6 +80,7 @@ static ThomasParams thomas_params(const Context* c, bool homog = false) {
     p.tconst = c->tconst; p.tmaps = c->tmaps; p.tblk = c->tblk; p.tbcarry = c->tbcarry; p.tcount = c->tcount;
     p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni;
     p.nseg = c->thomas_nseg; p.nsb = c->thomas_nsb;
+    p.ctl = c->ctl;
     p.psi_bot = homog ? 0.0 : c->psi_bot;
     p.psi_top = homog ? 0.0 : c->psi_top;
     return p;
@@ -327,6 +340,41 @@ int context_create(const Config& cfg, Context** out) {
             return fail();
         }
     }
+    // one-pass cluster solve when a cluster of at most 8 CTAs holds every interior row in
+    // registers (at most 32 x 16 rows per CTA) and such clusters can be resident; otherwise the
+    // two-pass form
+    {
+        int L = 1;
+        while (TC_NSEG * L < (c->Ni + TC_MAX_CLUSTER - 1) / TC_MAX_CLUSTER) L *= 2;
+        const int R = TC_NSEG * L, C = (c->Ni + R - 1) / R;
+        const size_t smem = tc_smem_bytes(R);
+        ThomasClusterKernel kern = thomas_cluster_kernel(L);
+        int max_smem = 0;
+        cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (kern && C <= TC_MAX_CLUSTER && smem + 4096 <= (size_t)max_smem &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            encode_field_map(&c->tm_hat, reinterpret_cast<const double*>(c->hat), 2 * c->Hp, Ny, 2 * TC_KX,
+                             std::min(R, TC_BOX)) == 0 &&
+            encode_field_map(&c->tm_cp, c->cp, c->Hp, c->Ni, TC_KX, std::min(R, TC_BOX)) == 0) {
+            cudaLaunchConfig_t lc{};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            lc.gridDim = dim3(C * (c->Hp / TC_KX));
+            lc.blockDim = dim3(TC_THREADS);
+            lc.dynamicSmemBytes = smem;
+            lc.attrs = at; lc.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &lc) == cudaSuccess && nclusters > 0) {
+                c->thomas_cluster = true;
+                c->tc_cluster = C;
+                c->tc_L = L;
+                c->tc_smem = smem;
+                c->tc_nclusters = std::min(nclusters, c->Hp / TC_KX);
+            }
+        }
+        cudaGetLastError();                         // a refused attribute or query only selects the two passes
+    }
     {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt, 256, 0) != cudaSuccess || per_sm < 1) {
@@ -512,7 +560,39 @@ int launch_thomas_apply(Context* c, cudaStream_t s, bool homog) {
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
-int launch_thomas(Context* c, cudaStream_t s) { return (launch_thomas_maps(c, s) || launch_thomas_apply(c, s)) ? -1 : 0; }
+// The one-pass form: one cluster of tc_cluster CTAs per 8-kx column group.
+int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
+    cudaLaunchConfig_t lc{};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = c->tc_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+    lc.gridDim = dim3(c->tc_cluster * c->tc_nclusters);       // persistent: the resident clusters
+    lc.blockDim = dim3(TC_THREADS);
+    lc.dynamicSmemBytes = c->tc_smem;
+    lc.stream = s;
+    lc.attrs = at; lc.numAttrs = 1;
+    ThomasMaps maps;
+    maps.hat = c->tm_hat;
+    maps.cp = c->tm_cp;
+    NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, thomas_cluster_kernel(c->tc_L), maps, thomas_params(c, homog)));
+    return 0;
+}
+
+// Launches of one tridiagonal solve: 1 (cluster form) or 2 (maps, apply); part i of them.
+int thomas_launches(const Context* c) { return c->thomas_cluster ? 1 : 2; }
+const char* thomas_kernel_name(const Context* c, int i) {
+    if (c->thomas_cluster) return "k_thomas_cluster";
+    return i == 0 ? "k_thomas_maps" : "k_thomas_apply";
+}
+int launch_thomas_part(Context* c, int i, cudaStream_t s, bool homog) {
+    if (c->thomas_cluster) return launch_thomas_cluster(c, s, homog);
+    return i == 0 ? launch_thomas_maps(c, s, homog) : launch_thomas_apply(c, s, homog);
+}
+int launch_thomas(Context* c, cudaStream_t s) {
+    for (int i = 0; i < thomas_launches(c); ++i)
+        if (launch_thomas_part(c, i, s, false)) return -1;
+    return 0;
+}
 
 // the reference's standalone Thom launcher (src/ops.cu:270-276)
 int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s) {
@@ -563,8 +643,8 @@ static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev
         if (launch_stage(c, st, win[st - 1], c->w, wst[st - 1], s, (store_rhs && st == 3) ? c->rhs : nullptr) || mark())
             return -1;
         if (launch_fft_fwd(c, wst[st - 1], s) || mark()) return -1;
-        if (launch_thomas_maps(c, s) || mark()) return -1;
-        if (launch_thomas_apply(c, s) || mark()) return -1;
+        for (int i = 0; i < thomas_launches(c); ++i)
+            if (launch_thomas_part(c, i, s, false) || mark()) return -1;
         // the stage-3 transform also advances the time (its last CTA)
         if (launch_ifft_thom(c, c->psi, wst[st - 1], st, true, c->closure_diag, s, st == 3) || mark()) return -1;
     }
@@ -579,17 +659,20 @@ int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev, bool store_r
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
     if (c->prec32) return step32_kernel_name(c, k);
-    static const char* stage[5] = {"k_stage", "k_fft_fwd", "k_thomas_maps", "k_thomas_apply", "k_ifft_thom"};
     if (c->cfg.adapt) {
         if (k == 0) return "k_maxuv_dt";
         --k;
     }
-    if (k >= 15) return "";
-    if (k % 5 == 0 && c->stage_tma) return "k_stage_tma";
-    return stage[k % 5];
+    const int per = 3 + thomas_launches(c);
+    if (k < 0 || k >= 3 * per) return "";
+    const int i = k % per;
+    if (i == 0) return c->stage_tma ? "k_stage_tma" : "k_stage";
+    if (i == 1) return "k_fft_fwd";
+    if (i == per - 1) return "k_ifft_thom";
+    return thomas_kernel_name(c, i - 2);
 }
 
-int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * 5; }
+int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * (3 + thomas_launches(c)); }
 
 // nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.
 int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs) {

@@ -177,20 +177,25 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
         NSE_CUDA_TRY(cudaGetLastError());
         if (mark()) return -1;
         if (fft32_fwd(c, wst[st - 1], s) || mark()) return -1;
-        if (launch_thomas_maps(c, s, true) || mark()) return -1;
-        if (launch_thomas_apply(c, s, true) || mark()) return -1;
+        for (int i = 0; i < thomas_launches(c); ++i)
+            if (launch_thomas_part(c, i, s, true) || mark()) return -1;
         if (fft32_inv(c, wst[st - 1], st == 3, s) || mark()) return -1;
     }
     return 0;
 }
 
 const char* step32_kernel_name(const Context* c, int k) {
-    static const char* stage[5] = {"k_stage32", "k_fft_fwd32", "k_thomas_maps", "k_thomas_apply", "k_ifft_thom32"};
     if (c->cfg.adapt) {
         if (k == 0) return "k_maxuv32";
         --k;
     }
-    return (k < 15) ? stage[k % 5] : "";
+    const int per = 3 + thomas_launches(c);
+    if (k < 0 || k >= 3 * per) return "";
+    const int i = k % per;
+    if (i == 0) return "k_stage32";
+    if (i == 1) return "k_fft_fwd32";
+    if (i == per - 1) return "k_ifft_thom32";
+    return thomas_kernel_name(c, i - 2);
 }
 
 }  // namespace nse2d

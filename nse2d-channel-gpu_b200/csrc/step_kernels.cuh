@@ -5,16 +5,18 @@
 //                 rhs = -J_arakawa + nu lap + f(y) - r omega (+ MMS forcing). psi and omega
 //                 tiles with a one-cell halo are staged in shared memory.
 //   k_fft_fwd     forward real FFT of every interior row of omega^(s+1) -> omega-hat [Ny][Hp].
-//   k_thomas      y-direction tridiagonal solve of every kx column, in place
-//                 (omega-hat -> psi-hat). One thread-block cluster owns 16 kx columns and
-//                 splits the Ny-2 rows among its CTAs; each warp sweeps a segment of rows and
-//                 the segments are joined through their affine carries (smem + DSMEM).
+//   k_thomas_cluster  y-direction tridiagonal solve of every kx column, in place
+//                 (omega-hat -> psi-hat). One thread-block cluster owns 8 kx columns and
+//                 splits the Ny-2 rows among its CTAs; each thread sweeps a segment of rows and
+//                 the segments are joined through their affine carries (smem + DSMEM). Very
+//                 tall grids use the two-pass form (k_thomas_maps, k_thomas_apply).
 //   k_ifft_thom   inverse real FFT of every row -> psi [Ny][Nx], then the Thom wall vorticity
 //                 of omega^(s+1) by the CTAs that own rows 1-2 and Ny-3..Ny-2.
 // Per step: k_maxuv_dt (max|u|,|v|,|v|a -> adaptive dt on the device) before stage 1; the
 // last CTA of the stage-3 k_ifft_thom advances the time.
 #pragma once
 #include <cuda.h>
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "common.cuh"
@@ -560,6 +562,7 @@ struct ThomasParams {
     unsigned int* tcount;    // [groups]: arrival counters of the map pass
     int Nx, Ny, Hp, H, Ni, nseg, nsb;
     double psi_bot, psi_top;
+    Ctl* ctl;                // error flags (bounded TMA waits of the cluster solve)
 };
 
 // Thomas sweeps of the reference (src/poisson.cu:70-133), split into segments of TS_ROWS rows.
@@ -864,6 +867,293 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams
         if (s == 0) hatw[col] = kx0re ? (double)p.Nx * p.psi_bot : 0.0;
         if (s == p.nseg - 1) hatw[(size_t)(p.Ny - 1) * rowstride + col] = kx0re ? (double)p.Nx * p.psi_top : 0.0;
     }
+}
+
+// ---- the same solve in one pass: thread-block clusters over 8-kx column groups ----
+//
+// The two passes above read omega-hat and cp twice and exchange block aggregates through HBM.
+// Here a cluster of C CTAs (C <= 8) splits the interior rows into C blocks of R = 32 L rows, one
+// per CTA, and walks the 8-kx column groups cid, cid + nclusters, ... (persistent). The tiles of
+// a group (omega-hat [R][8] complex, one 128-byte line per row, and cp [R][8]) arrive by TMA in
+// one of two shared-memory buffers while the previous group is solved, so the loads overlap the
+// sweeps and the exchanges. Thread (q, k) takes segment q (L consecutive rows) of kx = 8 g + k
+// into registers (re and im share every coefficient) and writes psi-hat straight back.
+// The segments and the CTAs are joined through the affine carries of the two sweeps:
+//   forward:  dp_t = dp0_t + (beta_lo ... beta_t) c,          c = dp before the segment;
+//   backward: x_t  = x0_t + ((-cp_t) ... (-cp_hi-1)) X,        X = x after the segment.
+// A segment's forward map is (D, P): dp_last = D + P c; composing a lower map a with the next
+// one b gives (D_b + P_b D_a, P_b P_a). The backward maps (U, Q) compose from the top the same
+// way. The four segments of a warp (lanes 8j + k, q = 4w + j) are scanned with shuffles, the
+// warps of a CTA through shared memory, and the CTAs of the cluster through distributed shared
+// memory after a cluster barrier; per group:
+// 1. forward sweep of every segment from c = 0;
+// 2. scans -> the carry c of every segment; carry term; backward sweep from X = 0;
+// 3. scans from the top -> the carry X of every segment; carry term; psi-hat out.
+// The CTA aggregates alternate between two slots by group parity: a slot is rewritten two groups
+// later, after cluster barriers that every CTA passes only once its reads of the slot are done.
+// The cluster barriers are hardware barriers that every thread of every CTA reaches (no early
+// return). After the last group each CTA arrives once it has read the others' aggregates and
+// waits for the rest just before it exits, so no CTA's shared memory goes away while read.
+// A TMA wait that does not complete within kTmaWaitLimit polls sets bit 1 of the control
+// block's error flags; the CTA still takes every cluster barrier (its results are then void)
+// and, before it exits, waits (bounded) for its copies in flight.
+constexpr int TC_KX = 8;                    // kx per cluster
+constexpr int TC_NSEG = 32;                 // segments per CTA
+constexpr int TC_THREADS = TC_KX * TC_NSEG;
+constexpr int TC_NW = TC_THREADS / 32;
+constexpr int TC_MAX_CLUSTER = 8;           // portable cluster size
+constexpr int TC_MAX_L = 16;                // rows per segment held in registers
+constexpr int TC_BOX = 256;                 // rows per TMA box (the box limit)
+
+struct ThomasMaps {
+    CUtensorMap hat;         // [Ny][2 Hp] doubles, box 16 x min(R, 256)
+    CUtensorMap cp;          // [Ni][Hp] doubles, box 8 x min(R, 256)
+};
+
+// bytes of one buffer (omega-hat tile [R][8] complex + cp tile [R][8]) and of the whole
+// dynamic shared memory (two buffers, the rows' asub and 1/csup, alignment slack)
+__host__ __device__ constexpr size_t tc_buf_bytes(int R) { return (size_t)R * (16 + 8) * TC_KX; }
+__host__ __device__ constexpr size_t tc_smem_bytes(int R) { return 2 * tc_buf_bytes(R) + (size_t)R * 16 + 128; }
+
+__device__ __forceinline__ void cluster_arrive_release() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// affine map (D, P) of complex D and real P
+struct AffMap {
+    double2 D;
+    double P;
+};
+// b after a
+__device__ __forceinline__ AffMap aff_after(const AffMap& b, const AffMap& a) {
+    return AffMap{make_double2(fma(b.P, a.D.x, b.D.x), fma(b.P, a.D.y, b.D.y)), b.P * a.P};
+}
+__device__ __forceinline__ AffMap aff_shfl_up(const AffMap& m, int off) {
+    return AffMap{make_double2(__shfl_up_sync(0xffffffffu, m.D.x, off), __shfl_up_sync(0xffffffffu, m.D.y, off)),
+                  __shfl_up_sync(0xffffffffu, m.P, off)};
+}
+__device__ __forceinline__ AffMap aff_shfl_down(const AffMap& m, int off) {
+    return AffMap{make_double2(__shfl_down_sync(0xffffffffu, m.D.x, off), __shfl_down_sync(0xffffffffu, m.D.y, off)),
+                  __shfl_down_sync(0xffffffffu, m.P, off)};
+}
+
+template <int L>
+static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_cluster(const __grid_constant__ ThomasMaps maps, ThomasParams p) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ double2 wD[TC_NW][TC_KX];      // per-warp aggregates of a scan
+    __shared__ double wP[TC_NW][TC_KX];
+    __shared__ double2 aggD[2][2][TC_KX];     // [slot][0 forward (D, P) | 1 backward (U, Q)][k]
+    __shared__ double aggP[2][2][TC_KX];
+    __shared__ double2 cbuf[TC_KX];           // the folded carry of the other CTAs, per kx
+    constexpr int R = TC_NSEG * L;
+    constexpr int RB = R < TC_BOX ? R : TC_BOX;
+    constexpr int NBOX = R / RB;
+    unsigned char* sm = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+    double2* rows = reinterpret_cast<double2*>(sm + 2 * tc_buf_bytes(R));   // [R] {asub, 1/csup}
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int cid = blockIdx.x / C, ncl = gridDim.x / C;
+    const int ngroups = p.Hp / TC_KX;
+    const int tid = threadIdx.x, k = tid & (TC_KX - 1), q = tid >> 3, lane = tid & 31, w = tid >> 5, j = q & 3;
+    const int r0 = rank * R;
+    const int n = max(0, min(R, p.Ni - r0));
+    const int lo = q * L;
+    const size_t Hp = (size_t)p.Hp;
+    auto issue = [&](int grp, int b) {
+        unsigned char* dst = sm + (size_t)b * tc_buf_bytes(R);
+        mbar_expect_tx(&bars[b], (unsigned)tc_buf_bytes(R));
+#pragma unroll
+        for (int bx = 0; bx < NBOX; ++bx) {
+            tma_load_2d(dst + (size_t)bx * RB * 16 * TC_KX, &maps.hat, grp * 2 * TC_KX, r0 + 1 + bx * RB, &bars[b]);
+            tma_load_2d(dst + (size_t)R * 16 * TC_KX + (size_t)bx * RB * 8 * TC_KX, &maps.cp, grp * TC_KX, r0 + bx * RB, &bars[b]);
+        }
+    };
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async_smem();
+        if (cid < ngroups) issue(cid, 0);
+        if (cid + ncl < ngroups) issue(cid + ncl, 1);
+    }
+    for (int t = tid; t < R; t += TC_THREADS)
+        rows[t] = (t < n) ? make_double2(p.asub[r0 + t + 1], p.inv_csup[r0 + t + 1]) : make_double2(0.0, 0.0);
+    __syncthreads();
+    bool failed = false;
+    int pending[2] = {-1, -1};                           // thread 0: parity of a copy whose wait timed out
+    int it = 0;
+    for (int g = cid; g < ngroups; g += ncl, ++it) {
+        const int b = it & 1, slot = it & 1;
+        const bool ok = mbar_wait_bounded(&bars[b], (it >> 1) & 1);
+        if (!ok && tid == 0 && pending[b] < 0) pending[b] = (it >> 1) & 1;
+        const int kx = g * TC_KX + k;
+        const bool valid = kx < p.H;
+        const double2* vt = reinterpret_cast<const double2*>(sm + (size_t)b * tc_buf_bytes(R));
+        const double* ct = reinterpret_cast<const double*>(sm + (size_t)b * tc_buf_bytes(R) + (size_t)R * 16 * TC_KX);
+        double2 x[L];
+        double cpv[L];
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+            x[i] = vt[(lo + i) * TC_KX + k];
+            cpv[i] = ct[(lo + i) * TC_KX + k];
+        }
+        fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
+        if (!__syncthreads_and(ok)) {
+            failed = true;
+            if (tid == 0) atomicOr(&p.ctl->nonfinite, 2);
+        }
+        if (tid == 0 && !failed && g + 2 * ncl < ngroups) issue(g + 2 * ncl, b);
+        // rhs = -omega-hat, with the k = 0 Dirichlet wall terms of src/poisson.cu:91-95,109-114
+        if (kx == 0) {
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+                const int t = lo + i;
+                if (r0 + t == 0 && t < n) x[i].x += p.asub[1] * p.psi_bot * (double)p.Nx;
+                if (r0 + t == p.Ni - 1 && t < n) x[i].x += p.csup[p.Ny - 2] * p.psi_top * (double)p.Nx;
+            }
+        }
+        // 1. forward sweep from c = 0
+        AffMap m{make_double2(0.0, 0.0), 1.0};
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+            if (lo + i < n) {
+                const double2 rc = rows[lo + i];
+                const double alpha = cpv[i] * rc.y;
+                const double beta = -rc.x * alpha;
+                m.D.x = fma(beta, m.D.x, -alpha * x[i].x);
+                m.D.y = fma(beta, m.D.y, -alpha * x[i].y);
+                x[i] = m.D;
+                m.P = beta * m.P;
+            }
+        }
+        // 2. carry c of this segment: scan of the warp's segments, of the warps below, of the CTAs below
+        AffMap s = m;
+#pragma unroll
+        for (int off = 8; off <= 16; off *= 2) {
+            const AffMap o = aff_shfl_up(s, off);
+            if (lane >= off) s = aff_after(s, o);
+        }
+        AffMap ex = aff_shfl_up(s, 8);
+        if (j == 0) ex = AffMap{make_double2(0.0, 0.0), 1.0};
+        if (j == 3) { wD[w][k] = s.D; wP[w][k] = s.P; }
+        __syncthreads();
+        AffMap A{make_double2(0.0, 0.0), 1.0};
+#pragma unroll
+        for (int v = 0; v < TC_NW - 1; ++v)
+            if (v < w) A = aff_after(AffMap{wD[v][k], wP[v][k]}, A);
+        const AffMap E = aff_after(ex, A);               // c = E.D + E.P c_blk
+        if (q == TC_NSEG - 1) {
+            const AffMap full = aff_after(s, A);
+            aggD[slot][0][k] = full.D;
+            aggP[slot][0][k] = full.P;
+        }
+        cluster_arrive_release();
+        cluster_wait_acquire();                          // also a barrier of this CTA
+        // the CTAs below: warps 0-1, lane (kx k, rank r), fold ranks 0 .. rank-1 (dp before the
+        // first interior row is 0)
+        if (w < 2) {
+            const int r = lane & 7, kk = (lane >> 3) + 4 * w;
+            AffMap a{make_double2(0.0, 0.0), 1.0};
+            if (r < rank) a = AffMap{cl.map_shared_rank(&aggD[slot][0][0], r)[kk], cl.map_shared_rank(&aggP[slot][0][0], r)[kk]};
+#pragma unroll
+            for (int off = 1; off < 8; off *= 2) {
+                const AffMap o = aff_shfl_up(a, off);
+                if (r >= off) a = aff_after(a, o);
+            }
+            if (r == rank - 1) cbuf[kk] = a.D;
+            if (rank == 0 && r == 0) cbuf[kk] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const double2 cb = cbuf[k];
+        const double2 c = make_double2(fma(E.P, cb.x, E.D.x), fma(E.P, cb.y, E.D.y));
+        {
+            double Pc = 1.0;
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+                if (lo + i < n) {
+                    const double2 rc = rows[lo + i];
+                    Pc = (-rc.x * (cpv[i] * rc.y)) * Pc;
+                    x[i].x = fma(Pc, c.x, x[i].x);
+                    x[i].y = fma(Pc, c.y, x[i].y);
+                }
+            }
+        }
+        m = AffMap{make_double2(0.0, 0.0), 1.0};         // backward sweep from X = 0: (U, Q)
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i) {
+            if (lo + i < n) {
+                m.D.x = fma(-cpv[i], m.D.x, x[i].x);
+                m.D.y = fma(-cpv[i], m.D.y, x[i].y);
+                x[i] = m.D;
+                m.P = -cpv[i] * m.P;
+            }
+        }
+        // 3. carry X of this segment: the same scans from the top
+        s = m;
+#pragma unroll
+        for (int off = 8; off <= 16; off *= 2) {
+            const AffMap o = aff_shfl_down(s, off);
+            if (lane + off < 32) s = aff_after(s, o);
+        }
+        ex = aff_shfl_down(s, 8);
+        if (j == 3) ex = AffMap{make_double2(0.0, 0.0), 1.0};
+        if (j == 0) { wD[w][k] = s.D; wP[w][k] = s.P; }  // the forward reads ended at the cluster barrier
+        __syncthreads();
+        A = AffMap{make_double2(0.0, 0.0), 1.0};
+#pragma unroll
+        for (int v = TC_NW - 1; v > 0; --v)
+            if (v > w) A = aff_after(AffMap{wD[v][k], wP[v][k]}, A);
+        const AffMap E2 = aff_after(ex, A);              // X = E2.D + E2.P X_blk
+        if (q == 0) {
+            const AffMap full = aff_after(s, A);
+            aggD[slot][1][k] = full.D;
+            aggP[slot][1][k] = full.P;
+        }
+        cluster_arrive_release();
+        cluster_wait_acquire();
+        // the CTAs above: fold ranks C-1 .. rank+1 from the top (x after the last interior row is 0)
+        if (w < 2) {
+            const int r = lane & 7, kk = (lane >> 3) + 4 * w;
+            AffMap a{make_double2(0.0, 0.0), 1.0};
+            if (r > rank && r < C) a = AffMap{cl.map_shared_rank(&aggD[slot][1][0], r)[kk], cl.map_shared_rank(&aggP[slot][1][0], r)[kk]};
+#pragma unroll
+            for (int off = 1; off < 8; off *= 2) {
+                const AffMap o = aff_shfl_down(a, off);
+                if (r + off < 8) a = aff_after(a, o);
+            }
+            if (r == rank + 1) cbuf[kk] = a.D;
+            if (rank == C - 1 && r == 0) cbuf[kk] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const double2 Xb = cbuf[k];
+        const double2 X = make_double2(fma(E2.P, Xb.x, E2.D.x), fma(E2.P, Xb.y, E2.D.y));
+        double2* hatw = reinterpret_cast<double2*>(p.hat);
+        double Qc = 1.0;
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i) {
+            const int t = lo + i;
+            if (t < n) {
+                Qc = -cpv[i] * Qc;
+                if (valid) hatw[(size_t)(r0 + t + 1) * Hp + kx] = make_double2(fma(Qc, X.x, x[i].x), fma(Qc, X.y, x[i].y));
+            }
+        }
+        // wall rows of psi-hat: Nx psi_bot / Nx psi_top at kx = 0, else 0 (poisson.cu:130-132)
+        if (valid && q == 0) {
+            if (rank == 0) hatw[kx] = make_double2(kx == 0 ? (double)p.Nx * p.psi_bot : 0.0, 0.0);
+            if (rank == C - 1) hatw[(size_t)(p.Ny - 1) * Hp + kx] = make_double2(kx == 0 ? (double)p.Nx * p.psi_top : 0.0, 0.0);
+        }
+    }
+    cluster_arrive_release();                            // done reading the others' aggregates
+    if (tid == 0) {                                      // copies still in flight after a timeout
+        for (int b = 0; b < 2; ++b)
+            if (pending[b] >= 0) mbar_wait_bounded(&bars[b], (unsigned)pending[b]);
+    }
+    cluster_wait_acquire();
 }
 
 // Thom wall vorticity alone (the reference's launcher, src/ops.cu:102-158,270-276).
