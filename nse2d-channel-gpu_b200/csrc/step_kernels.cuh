@@ -883,20 +883,23 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams
 //   backward: x_t  = x0_t + ((-cp_t) ... (-cp_hi-1)) X,        X = x after the segment.
 // A segment's forward map is (D, P): dp_last = D + P c; composing a lower map a with the next
 // one b gives (D_b + P_b D_a, P_b P_a). The backward maps (U, Q) compose from the top the same
-// way. The four segments of a warp (lanes 8j + k, q = 4w + j) are scanned with shuffles, the
-// warps of a CTA through shared memory, and the CTAs of the cluster through distributed shared
-// memory after a cluster barrier; per group:
-// 1. forward sweep of every segment from c = 0;
-// 2. scans -> the carry c of every segment; carry term; backward sweep from X = 0;
-// 3. scans from the top -> the carry X of every segment; carry term; psi-hat out.
-// The CTA aggregates alternate between two slots by group parity: a slot is rewritten two groups
-// later, after cluster barriers that every CTA passes only once its reads of the slot are done.
-// The cluster barriers are hardware barriers that every thread of every CTA reaches (no early
-// return). After the last group each CTA arrives once it has read the others' aggregates and
-// waits for the rest just before it exits, so no CTA's shared memory goes away while read.
-// A TMA wait that does not complete within kTmaWaitLimit polls sets bit 1 of the control
-// block's error flags; the CTA still takes every cluster barrier (its results are then void)
-// and, before it exits, waits (bounded) for its copies in flight.
+// way. The four segments of a warp (lanes 8j + k, q = 4w + j) are scanned with shuffles and the
+// warps of a CTA through shared memory; per group:
+// 1. forward sweep of every segment from c = 0; scans; the CTA's forward map is pushed to every
+//    CTA above it; the maps from below are folded into the carry c of every segment;
+// 2. carry term; backward sweep from X = 0; scans; the CTA's backward map is pushed to every CTA
+//    below; the maps from above are folded into the carry X of every segment;
+// 3. carry term; psi-hat out.
+// A push is st.async of the map into the receiver's shared memory, which completes bytes on the
+// receiver's mbarrier of that direction and group parity; the receiver waits on its own barrier
+// (bounded). No cluster-wide barrier is needed inside the loop, and a push carries no ordering
+// for the sender's other memory traffic. Two slots by group parity suffice: a sender finishes a
+// group only after the maps of the other direction of that group came back from its receivers,
+// so it is never two groups ahead of a receiver. One cluster barrier after the mbarriers are
+// initialised, and one before the exit, bracket the pushes.
+// A wait that does not complete within kTmaWaitLimit polls sets bit 1 of the control block's
+// error flags and the CTA goes on (its results are then void); before it exits it waits
+// (bounded) for its TMA copies still in flight.
 constexpr int TC_KX = 8;                    // kx per cluster
 constexpr int TC_NSEG = 32;                 // segments per CTA
 constexpr int TC_THREADS = TC_KX * TC_NSEG;
@@ -904,6 +907,7 @@ constexpr int TC_NW = TC_THREADS / 32;
 constexpr int TC_MAX_CLUSTER = 8;           // portable cluster size
 constexpr int TC_MAX_L = 16;                // rows per segment held in registers
 constexpr int TC_BOX = 256;                 // rows per TMA box (the box limit)
+constexpr unsigned TC_MAP_BYTES = TC_KX * (16 + 8);   // one CTA's map of one direction: 8 x (complex, real)
 
 struct ThomasMaps {
     CUtensorMap hat;         // [Ny][2 Hp] doubles, box 16 x min(R, 256)
@@ -920,6 +924,30 @@ __device__ __forceinline__ void cluster_arrive_release() {
 }
 __device__ __forceinline__ void cluster_wait_acquire() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_map_u32(unsigned saddr, int rank) {
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_async_v2f64(unsigned raddr, double2 v, unsigned rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];\n"
+                 ::"r"(raddr), "d"(v.x), "d"(v.y), "r"(rbar) : "memory");
+}
+__device__ __forceinline__ void st_async_f64(unsigned raddr, double v, unsigned rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];\n"
+                 ::"r"(raddr), "d"(v), "r"(rbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, unsigned parity) {
+    for (unsigned it = 0; it < kTmaWaitLimit; ++it)
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+    return false;
 }
 
 // affine map (D, P) of complex D and real P
@@ -945,12 +973,13 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_dyn[];
-    __shared__ __align__(8) uint64_t bars[2];
-    __shared__ double2 wD[TC_NW][TC_KX];      // per-warp aggregates of a scan
+    __shared__ __align__(8) uint64_t bars[2];            // TMA buffers
+    __shared__ __align__(8) uint64_t xbar[2][2];         // [direction 0 forward | 1 backward][group parity]
+    __shared__ double2 wD[TC_NW][TC_KX];                 // per-warp aggregates of a scan
     __shared__ double wP[TC_NW][TC_KX];
-    __shared__ double2 aggD[2][2][TC_KX];     // [slot][0 forward (D, P) | 1 backward (U, Q)][k]
-    __shared__ double aggP[2][2][TC_KX];
-    __shared__ double2 cbuf[TC_KX];           // the folded carry of the other CTAs, per kx
+    __shared__ double2 rD[2][2][TC_MAX_CLUSTER][TC_KX];  // maps pushed by the other CTAs [dir][parity][rank][k]
+    __shared__ double rP[2][2][TC_MAX_CLUSTER][TC_KX];
+    __shared__ double2 cbuf[TC_KX];                      // the folded carry of the other CTAs, per kx
     constexpr int R = TC_NSEG * L;
     constexpr int RB = R < TC_BOX ? R : TC_BOX;
     constexpr int NBOX = R / RB;
@@ -976,6 +1005,8 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        for (int d = 0; d < 2; ++d)
+            for (int par = 0; par < 2; ++par) mbar_init(&xbar[d][par], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         fence_proxy_async_smem();
         if (cid < ngroups) issue(cid, 0);
@@ -983,14 +1014,21 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     }
     for (int t = tid; t < R; t += TC_THREADS)
         rows[t] = (t < n) ? make_double2(p.asub[r0 + t + 1], p.inv_csup[r0 + t + 1]) : make_double2(0.0, 0.0);
-    __syncthreads();
+    cluster_arrive_release();                            // every CTA's mbarriers exist before any push
+    cluster_wait_acquire();
+    const unsigned nbelow = (unsigned)rank, nabove = (unsigned)(C - 1 - rank);
     bool failed = false;
     int pending[2] = {-1, -1};                           // thread 0: parity of a copy whose wait timed out
     int it = 0;
     for (int g = cid; g < ngroups; g += ncl, ++it) {
-        const int b = it & 1, slot = it & 1;
-        const bool ok = mbar_wait_bounded(&bars[b], (it >> 1) & 1);
-        if (!ok && tid == 0 && pending[b] < 0) pending[b] = (it >> 1) & 1;
+        const int b = it & 1, par = it & 1;
+        const unsigned ph = (unsigned)((it >> 1) & 1);
+        if (tid == 0) {                                  // this group's expected pushes (none: the phase ends now)
+            mbar_expect_tx(&xbar[0][par], nbelow * TC_MAP_BYTES);
+            mbar_expect_tx(&xbar[1][par], nabove * TC_MAP_BYTES);
+        }
+        const bool ok = mbar_wait_bounded(&bars[b], ph);
+        if (!ok && tid == 0 && pending[b] < 0) pending[b] = (int)ph;
         const int kx = g * TC_KX + k;
         const bool valid = kx < p.H;
         const double2* vt = reinterpret_cast<const double2*>(sm + (size_t)b * tc_buf_bytes(R));
@@ -1031,7 +1069,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
                 m.P = beta * m.P;
             }
         }
-        // 2. carry c of this segment: scan of the warp's segments, of the warps below, of the CTAs below
+        // scans: the warp's segments, then the warps below
         AffMap s = m;
 #pragma unroll
         for (int off = 8; off <= 16; off *= 2) {
@@ -1047,19 +1085,24 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         for (int v = 0; v < TC_NW - 1; ++v)
             if (v < w) A = aff_after(AffMap{wD[v][k], wP[v][k]}, A);
         const AffMap E = aff_after(ex, A);               // c = E.D + E.P c_blk
-        if (q == TC_NSEG - 1) {
+        if (q == TC_NSEG - 1) {                          // push this CTA's forward map to the CTAs above
             const AffMap full = aff_after(s, A);
-            aggD[slot][0][k] = full.D;
-            aggP[slot][0][k] = full.P;
+            const unsigned la = smem_u32(&rD[0][par][rank][k]), lp = smem_u32(&rP[0][par][rank][k]);
+            const unsigned lb = smem_u32(&xbar[0][par]);
+            for (int d = rank + 1; d < C; ++d) {
+                const unsigned rb = cluster_map_u32(lb, d);
+                st_async_v2f64(cluster_map_u32(la, d), full.D, rb);
+                st_async_f64(cluster_map_u32(lp, d), full.P, rb);
+            }
         }
-        cluster_arrive_release();
-        cluster_wait_acquire();                          // also a barrier of this CTA
-        // the CTAs below: warps 0-1, lane (kx k, rank r), fold ranks 0 .. rank-1 (dp before the
+        // the CTAs below: warps 0-1, lane (kx kk, rank r), fold ranks 0 .. rank-1 (dp before the
         // first interior row is 0)
         if (w < 2) {
+            const bool got = (nbelow == 0) || mbar_wait_cluster_bounded(&xbar[0][par], ph);
+            if (!got) atomicOr(&p.ctl->nonfinite, 2);
             const int r = lane & 7, kk = (lane >> 3) + 4 * w;
             AffMap a{make_double2(0.0, 0.0), 1.0};
-            if (r < rank) a = AffMap{cl.map_shared_rank(&aggD[slot][0][0], r)[kk], cl.map_shared_rank(&aggP[slot][0][0], r)[kk]};
+            if (r < rank) a = AffMap{rD[0][par][r][kk], rP[0][par][r][kk]};
 #pragma unroll
             for (int off = 1; off < 8; off *= 2) {
                 const AffMap o = aff_shfl_up(a, off);
@@ -1071,6 +1114,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         __syncthreads();
         const double2 cb = cbuf[k];
         const double2 c = make_double2(fma(E.P, cb.x, E.D.x), fma(E.P, cb.y, E.D.y));
+        // 2. carry term, backward sweep from X = 0: (U, Q)
         {
             double Pc = 1.0;
 #pragma unroll
@@ -1083,7 +1127,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
                 }
             }
         }
-        m = AffMap{make_double2(0.0, 0.0), 1.0};         // backward sweep from X = 0: (U, Q)
+        m = AffMap{make_double2(0.0, 0.0), 1.0};
 #pragma unroll
         for (int i = L - 1; i >= 0; --i) {
             if (lo + i < n) {
@@ -1093,7 +1137,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
                 m.P = -cpv[i] * m.P;
             }
         }
-        // 3. carry X of this segment: the same scans from the top
+        // scans from the top
         s = m;
 #pragma unroll
         for (int off = 8; off <= 16; off *= 2) {
@@ -1102,25 +1146,31 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         }
         ex = aff_shfl_down(s, 8);
         if (j == 3) ex = AffMap{make_double2(0.0, 0.0), 1.0};
-        if (j == 0) { wD[w][k] = s.D; wP[w][k] = s.P; }  // the forward reads ended at the cluster barrier
+        if (j == 0) { wD[w][k] = s.D; wP[w][k] = s.P; }  // the forward reads of wD ended at the last barrier
         __syncthreads();
         A = AffMap{make_double2(0.0, 0.0), 1.0};
 #pragma unroll
         for (int v = TC_NW - 1; v > 0; --v)
             if (v > w) A = aff_after(AffMap{wD[v][k], wP[v][k]}, A);
         const AffMap E2 = aff_after(ex, A);              // X = E2.D + E2.P X_blk
-        if (q == 0) {
+        if (q == 0) {                                    // push this CTA's backward map to the CTAs below
             const AffMap full = aff_after(s, A);
-            aggD[slot][1][k] = full.D;
-            aggP[slot][1][k] = full.P;
+            const unsigned la = smem_u32(&rD[1][par][rank][k]), lp = smem_u32(&rP[1][par][rank][k]);
+            const unsigned lb = smem_u32(&xbar[1][par]);
+            for (int d = 0; d < rank; ++d) {
+                const unsigned rb = cluster_map_u32(lb, d);
+                st_async_v2f64(cluster_map_u32(la, d), full.D, rb);
+                st_async_f64(cluster_map_u32(lp, d), full.P, rb);
+            }
         }
-        cluster_arrive_release();
-        cluster_wait_acquire();
-        // the CTAs above: fold ranks C-1 .. rank+1 from the top (x after the last interior row is 0)
+        // the CTAs above: fold ranks C-1 .. rank+1 from the top (x after the last interior row is
+        // 0); every thread read cb before the barrier after the backward scan
         if (w < 2) {
+            const bool got = (nabove == 0) || mbar_wait_cluster_bounded(&xbar[1][par], ph);
+            if (!got) atomicOr(&p.ctl->nonfinite, 2);
             const int r = lane & 7, kk = (lane >> 3) + 4 * w;
             AffMap a{make_double2(0.0, 0.0), 1.0};
-            if (r > rank && r < C) a = AffMap{cl.map_shared_rank(&aggD[slot][1][0], r)[kk], cl.map_shared_rank(&aggP[slot][1][0], r)[kk]};
+            if (r > rank && r < C) a = AffMap{rD[1][par][r][kk], rP[1][par][r][kk]};
 #pragma unroll
             for (int off = 1; off < 8; off *= 2) {
                 const AffMap o = aff_shfl_down(a, off);
@@ -1132,6 +1182,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         __syncthreads();
         const double2 Xb = cbuf[k];
         const double2 X = make_double2(fma(E2.P, Xb.x, E2.D.x), fma(E2.P, Xb.y, E2.D.y));
+        // 3. carry term; psi-hat out
         double2* hatw = reinterpret_cast<double2*>(p.hat);
         double Qc = 1.0;
 #pragma unroll
@@ -1148,11 +1199,11 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
             if (rank == C - 1) hatw[(size_t)(p.Ny - 1) * Hp + kx] = make_double2(kx == 0 ? (double)p.Nx * p.psi_top : 0.0, 0.0);
         }
     }
-    cluster_arrive_release();                            // done reading the others' aggregates
     if (tid == 0) {                                      // copies still in flight after a timeout
         for (int b = 0; b < 2; ++b)
             if (pending[b] >= 0) mbar_wait_bounded(&bars[b], (unsigned)pending[b]);
     }
+    cluster_arrive_release();                            // every push of the cluster has been issued
     cluster_wait_acquire();
 }
 
