@@ -227,6 +227,16 @@ int  nse2d_ensemble_set_groups(nse2d_ensemble* e, int groups);
 int  nse2d_ensemble_autotune(nse2d_ensemble* e, int trial_steps, int* groups_out, double* ms_per_step_out,
                              cudaStream_t s);
 
+/* ---- 4. Learned subgrid closure (no reference counterpart) ----
+ * BF16 operands on the 5th-generation tensor cores (tcgen05), FP32 accumulate. */
+
+/* C[M][ldc] = A[M][K] . B[N][K]^T (+ bias[N]), all device pointers, A and B BF16 row-major
+ * (K contiguous, 16-byte aligned). Cf (FP32, before the activation) and Cb (BF16, after it:
+ * ReLU when relu != 0) may each be NULL. M a multiple of 128, N a multiple of 16 in [16, 256],
+ * K a multiple of 64 (pad with zeros). Synchronous: returns nonzero if a bounded wait ran out. */
+int  nse2d_gemm_bf16(const void* A, const void* B, const float* bias, float* Cf, void* Cb, int M, int N, int K,
+                     int ldc, int relu, cudaStream_t s);
+
 const char* nse2d_last_error(void);
 
 #ifdef __cplusplus

@@ -98,6 +98,7 @@ def load(path=LIB_PATH):
         "nse2d_nonfinite": (I, [P, P, P]),
         "nse2d_metrics": (I, [P, I, P]),
         "nse2d_scalar": (I, [P, I, P]),
+        "nse2d_gemm_bf16": (I, [P, P, P, P, P, I, I, I, I, I, P]),
         "nse2d_last_error": (ctypes.c_char_p, []),
         "nse2d_set_abort_on_error": (V, [I]),
         "nse2d_testapi_set_free_slip": (V, [I]),
@@ -162,6 +163,20 @@ def max_uv_noalloc(psi_dev, a_node_dev, Nx, Ny, inv_dx, inv_deta, stream=None):
     _check(load().nse2d_max_uv_noalloc(dev(psi_dev), dev(a_node_dev), int(Nx), int(Ny), float(inv_dx),
                                        float(inv_deta), out, _stream(stream)))
     return tuple(out)
+
+
+def gemm_bf16(A, B, bias=None, relu=False, out_f32=True, out_bf16=False, stream=None):
+    """C = A . B^T (+ bias) on the tensor cores (nse2d_gemm_bf16): A [M, K] and B [N, K] torch
+    bfloat16 CUDA tensors (contiguous), FP32 accumulate. Returns (C_f32 or None, act(C)_bf16 or
+    None), where act is ReLU when relu is set."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    Cf = torch.empty((M, N), dtype=torch.float32, device=A.device) if out_f32 else None
+    Cb = torch.empty((M, N), dtype=torch.bfloat16, device=A.device) if out_bf16 else None
+    _check(load().nse2d_gemm_bf16(_ptr(A), _ptr(B), _ptr(bias), _ptr(Cf), _ptr(Cb), int(M), int(N), int(K), int(N),
+                                  1 if relu else 0, _stream(stream)))
+    return Cf, Cb
 
 
 class Solver:
