@@ -237,6 +237,41 @@ int  nse2d_ensemble_autotune(nse2d_ensemble* e, int trial_steps, int* groups_out
 int  nse2d_gemm_bf16(const void* A, const void* B, const float* bias, float* Cf, void* Cb, int M, int N, int K,
                      int ldc, int relu, cudaStream_t s);
 
+/* Top-hat filter of a fine field [Nyf][Nxf] onto the coarse grid whose nodes are every
+ * Nxf/Nxc-th column and (Nyf-1)/(Nyc-1)-th row (device pointers): the mean over the fine
+ * points within half a coarse cell, half weight on the cell edges, periodic in x, rows beyond
+ * the walls left out. */
+int  nse2d_box_filter(const double* fine, int Nxf, int Nyf, double* coarse, int Nxc, int Nyc, cudaStream_t s);
+
+/* The closure model on an Nx x Ny coarse grid: three 3x3 convolutions 2 -> hidden -> hidden ->
+ * 1 (ReLU after the first two; x periodic, zero beyond the walls) from (omega / w_scale,
+ * psi / psi_scale) to tau / tau_scale, where tau = filter(J(psi, omega)) - J(filter psi,
+ * filter omega) is the subgrid part of the Jacobian. Convolutions are BF16 GEMMs on the tensor
+ * cores with FP32 accumulate; weights are kept in FP32 and trained with AdamW. hidden is a
+ * multiple of 16 in [16, 64]. Weights are passed as [cout][9][cin] (tap = 3 (dy + 1) + dx + 1)
+ * and biases as [cout], on the host. Field pointers are device pointers [Ny][Nx] FP64. */
+typedef struct nse2d_cnn nse2d_cnn;
+int  nse2d_cnn_create(int Nx, int Ny, int hidden, nse2d_cnn** out);
+int  nse2d_cnn_destroy(nse2d_cnn* c);
+int  nse2d_cnn_layer_shape(nse2d_cnn* c, int layer, int* cin, int* cout);
+int  nse2d_cnn_set_params(nse2d_cnn* c, int layer, const float* w, const float* b);
+int  nse2d_cnn_get_params(nse2d_cnn* c, int layer, float* w, float* b);
+/* gradients of the last nse2d_cnn_gradients / nse2d_cnn_train_step */
+int  nse2d_cnn_get_grads(nse2d_cnn* c, int layer, float* w, float* b);
+int  nse2d_cnn_set_scales(nse2d_cnn* c, double w_scale, double psi_scale, double tau_scale);
+/* tau (FP64, zero on the wall rows) from omega and psi; asynchronous, graph-capturable */
+int  nse2d_cnn_forward(nse2d_cnn* c, const double* w, const double* psi, double* tau, cudaStream_t s);
+/* loss = mean over interior pixels of (output - tau_target / tau_scale)^2 and its gradients;
+ * with loss != NULL the call waits and stores the loss */
+int  nse2d_cnn_gradients(nse2d_cnn* c, const double* w, const double* psi, const double* tau_target, float* loss,
+                         cudaStream_t s);
+/* gradients, then one AdamW step (beta1 0.9, beta2 0.999, eps 1e-8, decoupled weight decay) */
+int  nse2d_cnn_train_step(nse2d_cnn* c, const double* w, const double* psi, const double* tau_target, float lr,
+                          float weight_decay, float* loss, cudaStream_t s);
+/* Attach a model of the context's grid (NULL detaches): every stage then evaluates it on its
+ * own psi and omega^(s) and subtracts tau from the rhs of the interior rows. Precision 64. */
+int  nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net);
+
 const char* nse2d_last_error(void);
 
 #ifdef __cplusplus

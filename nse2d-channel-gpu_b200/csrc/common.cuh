@@ -133,6 +133,9 @@ struct Context {
     CUtensorMap tm_hat{}, tm_cp{};
     int num_sms = 0;
     int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
+    // learned closure: the model evaluated before every stage and its output tau [Ny][Nx]
+    struct Cnn* closure_net = nullptr;
+    double* closure_tau = nullptr;
     // FP32-bulk variant (precision 32): base profiles (FP64) and FP32 fluctuations
     bool prec32 = false;
     float *wf = nullptr, *w1f = nullptr, *w2f = nullptr, *psif = nullptr, *rhsf = nullptr;

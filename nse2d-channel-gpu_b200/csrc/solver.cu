@@ -418,6 +418,7 @@ void context_destroy(Context* c) {
                       rt.inv_csup, rt.mms_g, rt.mms_gpp, rt.mms_sin2, rt.mms_sk, rt.mms_s2k, c->w, c->w1, c->w2,
                       c->psi, c->rhs, c->J, c->cp, c->red_blocks, c->red_out})
         if (p) cudaFree(p);
+    if (c->closure_tau) cudaFree(c->closure_tau);
     if (c->hat) cudaFree(c->hat);
     if (c->tconst) cudaFree(c->tconst);
     if (c->tmaps) cudaFree(c->tmaps);
@@ -453,6 +454,11 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
                  double* rhs_out) {
     StageParams p = stage_params(c);
     p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out; p.stage = stage;
+    // the learned closure's tau of this stage's state (the model runs just before the stage)
+    if (c->closure_net) {
+        if (cnn_forward(c->closure_net, w_in, c->psi, c->closure_tau, s)) return -1;
+        p.closure = c->closure_tau;
+    }
     if (c->stage_tma) {
         if (stage > 1 && w_n != c->w) { set_error("launch_stage: omega^n is not the context's omega"); return -1; }
         StageMaps maps;

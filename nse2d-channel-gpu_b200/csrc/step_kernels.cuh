@@ -34,6 +34,7 @@ struct StageParams {
     const double* w_n;       // omega^n (stages 2, 3); may alias w_out in stage 3
     double* w_out;           // omega^(s+1)
     double* rhs_out;         // optional: store rhs (the stage-3 rhs read by the diagnostics)
+    const double* closure;   // optional: learned subgrid term tau [Ny][Nx], rhs -= tau on interior rows
     RowTables rt;
     const Ctl* ctl;
     int Nx, Ny, stage, mms;
@@ -188,6 +189,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageTime
         }
         if (p.mms) rhs += mms_term(p, j, i, st.mA, st.mAp);
         const size_t id = (size_t)j * Nx + i;
+        if (p.closure && j != 0 && j != Ny - 1) rhs -= __ldg(&p.closure[id]);
         if (p.rhs_out) p.rhs_out[id] = rhs;
         double wnew;
         const double dt = st.dt;

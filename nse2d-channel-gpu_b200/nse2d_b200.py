@@ -99,6 +99,18 @@ def load(path=LIB_PATH):
         "nse2d_metrics": (I, [P, I, P]),
         "nse2d_scalar": (I, [P, I, P]),
         "nse2d_gemm_bf16": (I, [P, P, P, P, P, I, I, I, I, I, P]),
+        "nse2d_box_filter": (I, [P, I, I, P, I, I, P]),
+        "nse2d_cnn_create": (I, [I, I, I, ctypes.POINTER(P)]),
+        "nse2d_cnn_destroy": (I, [P]),
+        "nse2d_cnn_layer_shape": (I, [P, I, P, P]),
+        "nse2d_cnn_set_params": (I, [P, I, P, P]),
+        "nse2d_cnn_get_params": (I, [P, I, P, P]),
+        "nse2d_cnn_get_grads": (I, [P, I, P, P]),
+        "nse2d_cnn_set_scales": (I, [P, D, D, D]),
+        "nse2d_cnn_forward": (I, [P, P, P, P, P]),
+        "nse2d_cnn_gradients": (I, [P, P, P, P, P, P]),
+        "nse2d_cnn_train_step": (I, [P, P, P, P, ctypes.c_float, ctypes.c_float, P, P]),
+        "nse2d_set_closure": (I, [P, P]),
         "nse2d_last_error": (ctypes.c_char_p, []),
         "nse2d_set_abort_on_error": (V, [I]),
         "nse2d_testapi_set_free_slip": (V, [I]),
@@ -179,6 +191,87 @@ def gemm_bf16(A, B, bias=None, relu=False, out_f32=True, out_bf16=False, stream=
     return Cf, Cb
 
 
+def box_filter(fine, Nxf, Nyf, coarse, Nxc, Nyc, stream=None):
+    """nse2d_box_filter on device buffers (torch CUDA float64 tensors or raw addresses)."""
+    def dev(a):
+        return ctypes.c_void_p(a) if isinstance(a, int) else _ptr(a)
+    _check(load().nse2d_box_filter(dev(fine), int(Nxf), int(Nyf), dev(coarse), int(Nxc), int(Nyc), _stream(stream)))
+
+
+class Cnn:
+    """The learned closure model (nse2d_cnn_*): BF16 3x3 convolutions on the tensor cores."""
+
+    def __init__(self, Nx, Ny, hidden=32):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        _check(self.lib.nse2d_cnn_create(int(Nx), int(Ny), int(hidden), ctypes.byref(h)))
+        self.h, self.Nx, self.Ny, self.hidden = h, Nx, Ny, hidden
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nse2d_cnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, layer):
+        ci, co = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.nse2d_cnn_layer_shape(self.h, int(layer), ctypes.byref(ci), ctypes.byref(co)))
+        return ci.value, co.value
+
+    def set_params(self, layer, w, b):
+        ci, co = self.shape(layer)
+        w = np.ascontiguousarray(w, dtype=np.float32).reshape(co, 9, ci)
+        b = np.ascontiguousarray(b, dtype=np.float32).reshape(co)
+        _check(self.lib.nse2d_cnn_set_params(self.h, int(layer), _ptr(w), _ptr(b)))
+
+    def _get(self, fn, layer):
+        ci, co = self.shape(layer)
+        w = np.zeros((co, 9, ci), np.float32)
+        b = np.zeros(co, np.float32)
+        _check(fn(self.h, int(layer), _ptr(w), _ptr(b)))
+        return w, b
+
+    def get_params(self, layer):
+        return self._get(self.lib.nse2d_cnn_get_params, layer)
+
+    def get_grads(self, layer):
+        return self._get(self.lib.nse2d_cnn_get_grads, layer)
+
+    def init_params(self, seed=0):
+        """He-uniform weights (bound sqrt(6 / fan_in)), zero biases, from a numpy generator."""
+        rng = np.random.default_rng(seed)
+        for layer in range(3):
+            ci, co = self.shape(layer)
+            bound = np.sqrt(6.0 / (9 * ci))
+            if layer == 2:
+                bound *= 0.1
+            self.set_params(layer, rng.uniform(-bound, bound, (co, 9, ci)).astype(np.float32), np.zeros(co, np.float32))
+
+    def set_scales(self, w_scale, psi_scale, tau_scale):
+        _check(self.lib.nse2d_cnn_set_scales(self.h, float(w_scale), float(psi_scale), float(tau_scale)))
+
+    def forward(self, w, psi, tau, stream=None):
+        _check(self.lib.nse2d_cnn_forward(self.h, _ptr(w), _ptr(psi), _ptr(tau), _stream(stream)))
+
+    def gradients(self, w, psi, tau_target, stream=None):
+        loss = ctypes.c_float()
+        _check(self.lib.nse2d_cnn_gradients(self.h, _ptr(w), _ptr(psi), _ptr(tau_target), ctypes.byref(loss),
+                                            _stream(stream)))
+        return loss.value
+
+    def train_step(self, w, psi, tau_target, lr, weight_decay=0.0, want_loss=True, stream=None):
+        loss = ctypes.c_float()
+        _check(self.lib.nse2d_cnn_train_step(self.h, _ptr(w), _ptr(psi), _ptr(tau_target), float(lr),
+                                             float(weight_decay), ctypes.byref(loss) if want_loss else None,
+                                             _stream(stream)))
+        return loss.value if want_loss else None
+
+
 class Solver:
     """One channel on one GPU: the reference time loop's state and operators."""
 
@@ -208,6 +301,11 @@ class Solver:
         self.close()
 
     # ---- state ----
+    def set_closure(self, cnn):
+        """Attach a closure model (Cnn of this grid) to every stage; None detaches it."""
+        _check(self.lib.nse2d_set_closure(self.h, cnn.h if cnn is not None else None))
+        self._closure = cnn
+
     def set_omega(self, w, stream=None):
         """omega (host numpy [Ny,Nx] or CUDA tensor) -> initial Poisson solve + Thom, t = 0."""
         if hasattr(w, "data_ptr"):

@@ -30,6 +30,11 @@ def _load(name, path):
     return mod
 
 
+def load_oracle_module(name):
+    """A Python module of oracle/ (test infrastructure)."""
+    return _load(name, os.path.join(ORACLE, name + ".py"))
+
+
 def build_all():
     if not os.path.isfile(os.path.join(ORACLE, "_build", "liboracle.so")) or \
             not os.path.isfile(os.path.join(ORACLE, "_build", "nse2d_oracle")):
