@@ -243,31 +243,38 @@ int  nse2d_gemm_bf16(const void* A, const void* B, const float* bias, float* Cf,
  * the walls left out. */
 int  nse2d_box_filter(const double* fine, int Nxf, int Nyf, double* coarse, int Nxc, int Nyc, cudaStream_t s);
 
-/* The closure model on an Nx x Ny coarse grid: three 3x3 convolutions 2 -> hidden -> hidden ->
- * 1 (ReLU after the first two; x periodic, zero beyond the walls) from (omega / w_scale,
- * psi / psi_scale) to tau / tau_scale, where tau = filter(J(psi, omega)) - J(filter psi,
- * filter omega) is the subgrid part of the Jacobian. Convolutions are BF16 GEMMs on the tensor
- * cores with FP32 accumulate; weights are kept in FP32 and trained with AdamW. hidden is a
- * multiple of 16 in [16, 64]. Weights are passed as [cout][9][cin] (tap = 3 (dy + 1) + dx + 1)
- * and biases as [cout], on the host. Field pointers are device pointers [Ny][Nx] FP64. */
+/* The closure model on an Nx x Ny coarse grid: four 3x3 convolutions 5 -> hidden -> hidden ->
+ * hidden -> 1 (GELU, tanh form, after the first three; x periodic, zero beyond the walls) from
+ * (omega / s0, psi / s1, u / s2, v / s3, y) to tau / tau_scale, where tau = filter(J(psi, omega))
+ * - J(filter psi, filter omega) is the subgrid part of the Jacobian. Convolutions are BF16
+ * GEMMs on the tensor cores with FP32 accumulate; weights are kept in FP32 and trained with
+ * AdamW on batches of up to max_batch whole fields. hidden is a multiple of 16 in [16, 64]; y
+ * is the host array of the Ny wall-normal coordinates. Weights are passed as [cout][9][cin]
+ * (tap = 3 (dy + 1) + dx + 1) and biases as [cout], on the host. Field pointers are device
+ * pointers, FP64: one field [Ny][Nx], or S samples [S][Ny][Nx] with the batch's sample
+ * indices idx[nb] (host). */
 typedef struct nse2d_cnn nse2d_cnn;
-int  nse2d_cnn_create(int Nx, int Ny, int hidden, nse2d_cnn** out);
+int  nse2d_cnn_create(int Nx, int Ny, int hidden, int max_batch, const double* y, nse2d_cnn** out);
 int  nse2d_cnn_destroy(nse2d_cnn* c);
 int  nse2d_cnn_layer_shape(nse2d_cnn* c, int layer, int* cin, int* cout);
 int  nse2d_cnn_set_params(nse2d_cnn* c, int layer, const float* w, const float* b);
 int  nse2d_cnn_get_params(nse2d_cnn* c, int layer, float* w, float* b);
 /* gradients of the last nse2d_cnn_gradients / nse2d_cnn_train_step */
 int  nse2d_cnn_get_grads(nse2d_cnn* c, int layer, float* w, float* b);
-int  nse2d_cnn_set_scales(nse2d_cnn* c, double w_scale, double psi_scale, double tau_scale);
-/* tau (FP64, zero on the wall rows) from omega and psi; asynchronous, graph-capturable */
-int  nse2d_cnn_forward(nse2d_cnn* c, const double* w, const double* psi, double* tau, cudaStream_t s);
-/* loss = mean over interior pixels of (output - tau_target / tau_scale)^2 and its gradients;
- * with loss != NULL the call waits and stores the loss */
-int  nse2d_cnn_gradients(nse2d_cnn* c, const double* w, const double* psi, const double* tau_target, float* loss,
-                         cudaStream_t s);
+/* in_scales: the 4 scales of omega, psi, u, v */
+int  nse2d_cnn_set_scales(nse2d_cnn* c, const double* in_scales, double tau_scale);
+/* tau (FP64, zero on the wall rows) from one field's omega, psi, u, v; asynchronous and
+ * graph-capturable */
+int  nse2d_cnn_forward(nse2d_cnn* c, const double* w, const double* psi, const double* u, const double* v, double* tau,
+                       cudaStream_t s);
+/* loss = mean over the interior pixels of the batch of (output - tau / tau_scale)^2 and its
+ * gradients; waits, and stores the loss when loss != NULL */
+int  nse2d_cnn_gradients(nse2d_cnn* c, const double* w, const double* psi, const double* u, const double* v,
+                         const double* tau, const int* idx, int nb, float* loss, cudaStream_t s);
 /* gradients, then one AdamW step (beta1 0.9, beta2 0.999, eps 1e-8, decoupled weight decay) */
-int  nse2d_cnn_train_step(nse2d_cnn* c, const double* w, const double* psi, const double* tau_target, float lr,
-                          float weight_decay, float* loss, cudaStream_t s);
+int  nse2d_cnn_train_step(nse2d_cnn* c, const double* w, const double* psi, const double* u, const double* v,
+                          const double* tau, const int* idx, int nb, float lr, float weight_decay, float* loss,
+                          cudaStream_t s);
 /* Attach a model of the context's grid (NULL detaches): every stage then evaluates it on its
  * own psi and omega^(s) and subtracts tau from the rhs of the interior rows. Precision 64. */
 int  nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net);

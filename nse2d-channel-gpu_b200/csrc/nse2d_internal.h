@@ -16,7 +16,7 @@ int launch_thomas_apply(Context* c, cudaStream_t s, bool homog = false);
 int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog = false);
 // learned closure (closure.cu)
 struct Cnn;
-int cnn_forward(Cnn* n, const double* w, const double* psi, double* tau, cudaStream_t s);
+int cnn_forward(Cnn* n, const double* w, const double* psi, const double* u, const double* v, double* tau, cudaStream_t s);
 bool cnn_matches(const Cnn* n, int Nx, int Ny);
 int thomas_launches(const Context* c);
 const char* thomas_kernel_name(const Context* c, int i);

@@ -15,8 +15,8 @@
 //   - one thread issues four tcgen05.mma (M = 128, N, K = 16) and tcgen05.commit, which arrives
 //     on the buffer's mbarrier when the MMAs have read it.
 // After the last block all threads wait on that barrier; warp w reads TMEM lanes 32w..32w+31
-// (rows of C) with tcgen05.ld 32x32b.x16 and applies the epilogue: + bias[n], optional ReLU,
-// FP32 and/or BF16 stores.
+// (rows of C) with tcgen05.ld 32x32b.x16 and applies the epilogue: + bias[n], an activation,
+// FP32 and/or BF16 stores (the BF16 output after the activation: ReLU or GELU).
 //
 // Every mbarrier wait is bounded. A wait that runs out sets *err and the CTA still waits
 // (bounded) for its MMAs before it frees its TMEM and returns.
@@ -41,8 +41,20 @@ struct TcGemmParams {
     float* Cf;               // [M][ldc] FP32 (pre-activation) or null
     __nv_bfloat16* Cb;       // [M][ldc] BF16 (after the activation) or null
     int* err;                // set to 1 by a wait that ran out
-    int M, N, K, ldc, relu;
+    int M, N, K, ldc;
+    int act;                 // activation of the BF16 output: 0 none, 1 ReLU, 2 GELU (tanh form)
 };
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), and its derivative.
+__device__ __forceinline__ float tg_gelu(float x) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    return 0.5f * x * (1.f + tanhf(u));
+}
+__device__ __forceinline__ float tg_gelu_grad(float x) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    const float t = tanhf(u);
+    return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * 0.7978845608028654f * fmaf(0.134145f, x * x, 1.f);
+}
 
 __device__ __forceinline__ uint32_t tg_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -167,7 +179,10 @@ static __global__ void __launch_bounds__(TG_THREADS) k_tc_gemm(TcGemmParams p) {
                 float z = __uint_as_float(v[i]);
                 if (p.bias) z += p.bias[c0 + i];
                 if (p.Cf) p.Cf[(size_t)row * p.ldc + c0 + i] = z;
-                if (p.Cb) p.Cb[(size_t)row * p.ldc + c0 + i] = __float2bfloat16_rn(p.relu ? fmaxf(z, 0.f) : z);
+                if (p.Cb) {
+                    const float a = p.act == 1 ? fmaxf(z, 0.f) : (p.act == 2 ? tg_gelu(z) : z);
+                    p.Cb[(size_t)row * p.ldc + c0 + i] = __float2bfloat16_rn(a);
+                }
             }
         }
     }

@@ -100,16 +100,16 @@ def load(path=LIB_PATH):
         "nse2d_scalar": (I, [P, I, P]),
         "nse2d_gemm_bf16": (I, [P, P, P, P, P, I, I, I, I, I, P]),
         "nse2d_box_filter": (I, [P, I, I, P, I, I, P]),
-        "nse2d_cnn_create": (I, [I, I, I, ctypes.POINTER(P)]),
+        "nse2d_cnn_create": (I, [I, I, I, I, P, ctypes.POINTER(P)]),
         "nse2d_cnn_destroy": (I, [P]),
         "nse2d_cnn_layer_shape": (I, [P, I, P, P]),
         "nse2d_cnn_set_params": (I, [P, I, P, P]),
         "nse2d_cnn_get_params": (I, [P, I, P, P]),
         "nse2d_cnn_get_grads": (I, [P, I, P, P]),
-        "nse2d_cnn_set_scales": (I, [P, D, D, D]),
-        "nse2d_cnn_forward": (I, [P, P, P, P, P]),
-        "nse2d_cnn_gradients": (I, [P, P, P, P, P, P]),
-        "nse2d_cnn_train_step": (I, [P, P, P, P, ctypes.c_float, ctypes.c_float, P, P]),
+        "nse2d_cnn_set_scales": (I, [P, P, D]),
+        "nse2d_cnn_forward": (I, [P, P, P, P, P, P, P]),
+        "nse2d_cnn_gradients": (I, [P, P, P, P, P, P, P, I, P, P]),
+        "nse2d_cnn_train_step": (I, [P, P, P, P, P, P, P, I, ctypes.c_float, ctypes.c_float, P, P]),
         "nse2d_set_closure": (I, [P, P]),
         "nse2d_last_error": (ctypes.c_char_p, []),
         "nse2d_set_abort_on_error": (V, [I]),
@@ -199,13 +199,17 @@ def box_filter(fine, Nxf, Nyf, coarse, Nxc, Nyc, stream=None):
 
 
 class Cnn:
-    """The learned closure model (nse2d_cnn_*): BF16 3x3 convolutions on the tensor cores."""
+    """The learned closure model (nse2d_cnn_*): BF16 3x3 convolutions on the tensor cores.
+    Inputs (omega, psi, u, v) are torch CUDA float64 tensors, one field [Ny, Nx] or samples
+    [S, Ny, Nx] with batch indices."""
 
-    def __init__(self, Nx, Ny, hidden=32):
+    def __init__(self, Nx, Ny, y, hidden=32, max_batch=1):
         self.lib = load()
+        y = np.ascontiguousarray(y, dtype=np.float64)
         h = ctypes.c_void_p()
-        _check(self.lib.nse2d_cnn_create(int(Nx), int(Ny), int(hidden), ctypes.byref(h)))
-        self.h, self.Nx, self.Ny, self.hidden = h, Nx, Ny, hidden
+        _check(self.lib.nse2d_cnn_create(int(Nx), int(Ny), int(hidden), int(max_batch), _ptr(y), ctypes.byref(h)))
+        self.h, self.Nx, self.Ny, self.hidden, self.max_batch = h, Nx, Ny, hidden, max_batch
+        self.layers = 4
 
     def close(self):
         if getattr(self, "h", None):
@@ -242,32 +246,42 @@ class Cnn:
     def get_grads(self, layer):
         return self._get(self.lib.nse2d_cnn_get_grads, layer)
 
-    def init_params(self, seed=0):
-        """He-uniform weights (bound sqrt(6 / fan_in)), zero biases, from a numpy generator."""
+    def params(self):
+        return [self.get_params(l) for l in range(self.layers)]
+
+    def load_params(self, params):
+        for l, (w, b) in enumerate(params):
+            self.set_params(l, w, b)
+
+    def init_params(self, seed=0, last_gain=0.1):
+        """He-uniform weights (bound sqrt(6 / fan_in)), zero biases, from a numpy generator; the
+        output layer scaled by last_gain."""
         rng = np.random.default_rng(seed)
-        for layer in range(3):
+        for layer in range(self.layers):
             ci, co = self.shape(layer)
-            bound = np.sqrt(6.0 / (9 * ci))
-            if layer == 2:
-                bound *= 0.1
+            bound = np.sqrt(6.0 / (9 * ci)) * (last_gain if layer == self.layers - 1 else 1.0)
             self.set_params(layer, rng.uniform(-bound, bound, (co, 9, ci)).astype(np.float32), np.zeros(co, np.float32))
 
-    def set_scales(self, w_scale, psi_scale, tau_scale):
-        _check(self.lib.nse2d_cnn_set_scales(self.h, float(w_scale), float(psi_scale), float(tau_scale)))
+    def set_scales(self, in_scales, tau_scale):
+        s = np.ascontiguousarray(in_scales, dtype=np.float64)
+        _check(self.lib.nse2d_cnn_set_scales(self.h, _ptr(s), float(tau_scale)))
+        self.scales = (tuple(float(x) for x in s), float(tau_scale))
 
-    def forward(self, w, psi, tau, stream=None):
-        _check(self.lib.nse2d_cnn_forward(self.h, _ptr(w), _ptr(psi), _ptr(tau), _stream(stream)))
+    def forward(self, w, psi, u, v, tau, stream=None):
+        _check(self.lib.nse2d_cnn_forward(self.h, _ptr(w), _ptr(psi), _ptr(u), _ptr(v), _ptr(tau), _stream(stream)))
 
-    def gradients(self, w, psi, tau_target, stream=None):
+    def gradients(self, w, psi, u, v, tau, idx=(0,), stream=None):
         loss = ctypes.c_float()
-        _check(self.lib.nse2d_cnn_gradients(self.h, _ptr(w), _ptr(psi), _ptr(tau_target), ctypes.byref(loss),
-                                            _stream(stream)))
+        ix = np.ascontiguousarray(idx, dtype=np.int32)
+        _check(self.lib.nse2d_cnn_gradients(self.h, _ptr(w), _ptr(psi), _ptr(u), _ptr(v), _ptr(tau), _ptr(ix), len(ix),
+                                            ctypes.byref(loss), _stream(stream)))
         return loss.value
 
-    def train_step(self, w, psi, tau_target, lr, weight_decay=0.0, want_loss=True, stream=None):
+    def train_step(self, w, psi, u, v, tau, lr, idx=(0,), weight_decay=0.0, want_loss=True, stream=None):
         loss = ctypes.c_float()
-        _check(self.lib.nse2d_cnn_train_step(self.h, _ptr(w), _ptr(psi), _ptr(tau_target), float(lr),
-                                             float(weight_decay), ctypes.byref(loss) if want_loss else None,
+        ix = np.ascontiguousarray(idx, dtype=np.int32)
+        _check(self.lib.nse2d_cnn_train_step(self.h, _ptr(w), _ptr(psi), _ptr(u), _ptr(v), _ptr(tau), _ptr(ix), len(ix),
+                                             float(lr), float(weight_decay), ctypes.byref(loss) if want_loss else None,
                                              _stream(stream)))
         return loss.value if want_loss else None
 

@@ -1,14 +1,15 @@
 """CPU oracle of the learned closure model (test infrastructure only).
 
 Restates in numpy the model that nse2d-channel-gpu_b200/csrc/closure.cu runs on the tensor
-cores: three 3x3 convolutions 2 -> H -> H -> 1 with ReLU after the first two, periodic in x and
+cores: inputs (omega/s0, psi/s1, u/s2, v/s3, y) per point, four 3x3 convolutions
+5 -> H -> H -> H -> 1 with GELU (tanh form) after the first three, periodic in x and
 zero-padded beyond the walls, on pixel-major [Ny, Nx, C] activations; the loss is the mean
-over interior pixels of (z - tau / tau_scale)^2. The reference has no closure model, so there
-are no reference vectors for it; the oracle is pinned instead by central finite differences
-of its own loss in float64 (tests/test_closure_oracle.py).
+over the interior pixels of a batch of fields of (z - tau / tau_scale)^2. The reference has no
+closure model, so there are no reference vectors for it; the oracle is pinned instead by
+central finite differences of its own loss in float64 (tests/test_closure_oracle.py).
 
-With bf16=True the forward and backward passes round where the GPU path rounds: the scaled
-inputs, the weights, the hidden activations after ReLU, and dZ before the input-gradient
+With bf=True the forward and backward passes round where the GPU path rounds: the scaled
+inputs, the weights, the hidden activations after GELU, and dZ before the input-gradient
 product (round to nearest even, as __float2bfloat16_rn). Sums are float64 here and float32 on
 the GPU.
 """
@@ -56,43 +57,70 @@ def col2im(g):
     return out
 
 
-def forward(params, w, psi, scales, bf=False):
-    """params: [(W [cout, 9, cin], b [cout])] * 3; w, psi [Ny, Nx]; scales (sw, sp, st).
+C_GELU = np.sqrt(2.0 / np.pi)
+
+
+def gelu(x):
+    return 0.5 * x * (1.0 + np.tanh(C_GELU * (x + 0.044715 * x ** 3)))
+
+
+def gelu_grad(x):
+    t = np.tanh(C_GELU * (x + 0.044715 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * C_GELU * (1.0 + 3 * 0.044715 * x * x)
+
+
+def inputs(w, psi, u, v, y, scales):
+    """[Ny, Nx, 5]: omega, psi, u, v over their scales, and y."""
+    s0, s1, s2, s3 = scales[0]
+    yy = np.broadcast_to(np.asarray(y, np.float64)[:, None], np.shape(w))
+    return np.stack([w / s0, psi / s1, u / s2, v / s3, yy], axis=-1)
+
+
+def forward(params, x, bf=False):
+    """params: [(W [cout, 9, cin], b [cout])] * 4; x: the [Ny, Nx, 5] inputs.
     Returns the per-layer (input h, im2col A, pre-activation z)."""
-    r = bf16 if bf else (lambda x: np.asarray(x, dtype=np.float64))
-    sw, sp, _ = scales
-    h = r(np.stack([w / sw, psi / sp], axis=-1))
+    r = bf16 if bf else (lambda a: np.asarray(a, dtype=np.float64))
+    h = r(x)
     cache = []
     for layer, (W, b) in enumerate(params):
         A = im2col(h)
         z = np.einsum("jitc,otc->jio", A, r(W)) + np.asarray(b, np.float64)
         cache.append((h, A, z))
         if layer < len(params) - 1:
-            h = r(np.maximum(z, 0.0))
+            h = r(gelu(z))
     return cache
 
 
-def loss_and_grads(params, w, psi, tau, scales, bf=False):
-    """Loss and the gradients [(dW, db)] of every layer."""
-    r = bf16 if bf else (lambda x: np.asarray(x, dtype=np.float64))
-    cache = forward(params, w, psi, scales, bf)
-    z = cache[-1][2][:, :, 0]
-    Ny, Nx = z.shape
-    d = np.zeros_like(z)
-    d[1:-1] = z[1:-1] - tau[1:-1] / scales[2]
-    pint = Nx * (Ny - 2)
-    loss = float((d ** 2).sum() / pint)
-    dz = (2.0 * d / pint)[:, :, None]
-    grads = [None] * len(params)
-    for layer in range(len(params) - 1, -1, -1):
-        h, A, zl = cache[layer]
-        W = params[layer][0]
-        grads[layer] = (np.einsum("jio,jitc->otc", dz, A), dz.sum(axis=(0, 1)))
-        if layer == 0:
-            break
-        dA = np.einsum("jio,otc->jitc", r(dz), r(W))
-        dh = col2im(dA)
-        dz = dh * (cache[layer - 1][2] > 0)
+def predict(params, w, psi, u, v, y, scales, bf=False):
+    """tau (zero on the wall rows) of one field."""
+    z = forward(params, inputs(w, psi, u, v, y, scales), bf)[-1][2][:, :, 0] * scales[1]
+    z[0] = z[-1] = 0.0
+    return z
+
+
+def loss_and_grads(params, samples, y, scales, bf=False):
+    """Loss of a batch of samples [(w, psi, u, v, tau)] and the gradients [(dW, db)] of every layer."""
+    r = bf16 if bf else (lambda a: np.asarray(a, dtype=np.float64))
+    Ny, Nx = np.shape(samples[0][0])
+    pint = len(samples) * Nx * (Ny - 2)
+    loss = 0.0
+    grads = [(np.zeros_like(np.asarray(W, np.float64)), np.zeros(len(b))) for W, b in params]
+    for (w, psi, u, v, tau) in samples:
+        cache = forward(params, inputs(w, psi, u, v, y, scales), bf)
+        z = cache[-1][2][:, :, 0]
+        d = np.zeros_like(z)
+        d[1:-1] = z[1:-1] - np.asarray(tau)[1:-1] / scales[1]
+        loss += float((d ** 2).sum() / pint)
+        dz = (2.0 * d / pint)[:, :, None]
+        for layer in range(len(params) - 1, -1, -1):
+            h, A, zl = cache[layer]
+            W = params[layer][0]
+            gw, gb = grads[layer]
+            grads[layer] = (gw + np.einsum("jio,jitc->otc", dz, A), gb + dz.sum(axis=(0, 1)))
+            if layer == 0:
+                break
+            dA = np.einsum("jio,otc->jitc", r(dz), r(W))
+            dz = col2im(dA) * gelu_grad(cache[layer - 1][2])
     return loss, grads
 
 

@@ -1,8 +1,9 @@
 """The closure model's CPU oracle (oracle/closure_oracle.py), pinned by finite differences.
 
 The reference has no closure model, so the oracle's gradients are checked against central
-differences of its own float64 loss (relative error 1e-6 on every layer); im2col and col2im
-are checked to be adjoint (<A x, y> = <x, A^T y> to 1e-12).
+differences of its own float64 loss (relative error 1e-6 on every layer, a batch of two
+fields); im2col and col2im are checked to be adjoint (<A x, y> = <x, A^T y> to 1e-12) and the
+GELU derivative against differences of GELU.
 """
 import numpy as np
 import pytest
@@ -16,7 +17,7 @@ def co():
 
 
 def _params(rng, H):
-    shapes = [(H, 2), (H, H), (1, H)]
+    shapes = [(H, 5), (H, H), (H, H), (1, H)]
     return [(rng.standard_normal((o, 9, i)) * np.sqrt(2.0 / (9 * i)), 0.1 * rng.standard_normal(o)) for o, i in shapes]
 
 
@@ -27,25 +28,32 @@ def test_im2col_col2im_adjoint(co):
     assert abs((co.im2col(x) * y).sum() - (x * co.col2im(y)).sum()) < 1e-12 * np.abs(y).sum()
 
 
+def test_gelu_grad(co):
+    x = np.linspace(-4, 4, 41)
+    fd = (co.gelu(x + 1e-6) - co.gelu(x - 1e-6)) / 2e-6
+    assert np.allclose(co.gelu_grad(x), fd, atol=1e-8)
+
+
 def test_gradients_match_finite_differences(co):
     rng = np.random.default_rng(2)
     Ny, Nx, H = 7, 8, 4
     params = _params(rng, H)
-    w, psi, tau = rng.standard_normal((Ny, Nx)), rng.standard_normal((Ny, Nx)), rng.standard_normal((Ny, Nx))
-    scales = (1.3, 0.7, 2.0)
-    loss, grads = co.loss_and_grads(params, w, psi, tau, scales)
+    samples = [tuple(rng.standard_normal((Ny, Nx)) for _ in range(5)) for _ in range(2)]
+    y = np.linspace(-1, 1, Ny)
+    scales = ((1.3, 0.7, 0.9, 1.1), 2.0)
+    loss, grads = co.loss_and_grads(params, samples, y, scales)
     eps = 1e-6
-    for layer in range(3):
+    for layer in range(4):
         W, b = params[layer]
         for arr, g in ((W, grads[layer][0]), (b, grads[layer][1])):
             flat = arr.reshape(-1)
-            idx = rng.choice(flat.size, size=min(12, flat.size), replace=False)
+            idx = rng.choice(flat.size, size=min(10, flat.size), replace=False)
             for k in idx:
                 old = flat[k]
                 flat[k] = old + eps
-                lp, _ = co.loss_and_grads(params, w, psi, tau, scales)
+                lp, _ = co.loss_and_grads(params, samples, y, scales)
                 flat[k] = old - eps
-                lm, _ = co.loss_and_grads(params, w, psi, tau, scales)
+                lm, _ = co.loss_and_grads(params, samples, y, scales)
                 flat[k] = old
                 fd = (lp - lm) / (2 * eps)
                 assert abs(fd - g.reshape(-1)[k]) <= 1e-6 * max(1.0, abs(fd)), (layer, k, fd, g.reshape(-1)[k])
