@@ -521,6 +521,50 @@ def run_ensemble(args):
             "speedup_vs_sequential": round(seq_ms / ens_ms, 3), "clocks": ck}
 
 
+def run_closure(args):
+    """The learned-closure workflow (closure_pipeline): a 2048x1025 FP64 DNS (Re_b=1e4, tanh
+    beta=2, F0=0.05 at n=8, drag 1e-3, seeded mix) filtered to 256x129 every 0.1 units; the
+    4-layer BF16 CNN trained on it with AdamW; its gain chosen against a validation DNS (seed 5);
+    then, from the filtered state of a fresh seed (7), the DNS, the coarse solve with the model
+    and the plain coarse solve over the same span. Metric: DNS GPU seconds / GPU seconds of the
+    accepted coarse solve (the closure run if within 2% of the DNS on the time-averaged Re_tau
+    and mean-velocity profile, else the plain coarse run if it is, else 1: the DNS itself)."""
+    import torch
+    sys.path.insert(0, PKG)
+    nse = _load("nse2d_b200", os.path.join(PKG, "nse2d_b200.py"))
+    cp = _load("closure_pipeline", os.path.join(PKG, "closure_pipeline.py"))
+    log = lambda m: print(m, file=sys.stderr, flush=True)
+    T = args.closure_span
+    data, y, gen_s = cp.generate(torch, cp.DNS_CFG, seed=1, t_spinup=args.closure_spinup, t_span=T, dt_snap=0.1, log=log)
+    net, hist, train_s = cp.train(torch, data, y, steps=args.closure_train_steps, batch=8, lr=1e-3, hidden=32, seed=0,
+                                  log=log)
+    ref_val = cp.reference(torch, cp.DNS_CFG, seed=5, t_spinup=args.closure_spinup, t_span=args.closure_val_span,
+                           dt_stat=0.5, log=log)
+    gain = cp.select_gain(torch, net, ref_val, log=log)
+    out = cp.a_posteriori(torch, net, cp.DNS_CFG, seed=7, t_spinup=args.closure_spinup, t_span=T, dt_stat=0.5, log=log)
+    dns_s = out["dns"]["gpu_s"]
+    acc = {"none": "closure", "coarse": "coarse", "dns": "dns"}[out["fallback"]]
+    acc_s = dns_s if acc == "dns" else out[acc]["gpu_s"]
+
+    def brief(r):
+        return {"gpu_s": round(r["gpu_s"], 3), "finite": r["finite"], "re_tau": round(float(np.mean(r["re_tau"])), 3),
+                "re_tau_err": round(r.get("re_tau_err", 0.0), 5), "profile_err": round(r.get("profile_err", 0.0), 5)}
+    return {
+        "metric": "closure vs DNS time at 2% Re_tau", "value": round(dns_s / acc_s, 2), "unit": "x (DNS GPU s / accepted coarse GPU s)",
+        "higher_is_better": True, "n_gpus": 1, "steps": args.closure_train_steps, "warmup": 0, "scaling": "none",
+        "vs_baseline": None, "dtype": "bf16 model (FP32 accumulate), FP64 solver", "data": "self-generated DNS",
+        "accepted": acc, "gain": gain, "model_mode": "x-mean of tau on every row",
+        "a_priori": {"val_loss_untrained": round(hist["val0"], 4), "val_loss": round(hist["val"], 4),
+                     "note": "loss normalised by the variance of tau: predicting tau = 0 scores ~1"},
+        "dns": brief(out["dns"]), "closure": brief(out["closure"]), "coarse": brief(out["coarse"]),
+        "gpu_seconds": {"data_generation": round(gen_s, 2), "training": round(train_s, 2),
+                        "validation_dns": round(ref_val["gpu_s"], 2)},
+        "config": {"workload": f"learned closure: DNS 2048x1025 -> 256x129, span {T} units after {args.closure_spinup} "
+                               f"of spin-up, snapshots every 0.1, {args.closure_train_steps} AdamW steps of batch 8",
+                   "Re_b": 1e4, "seeds": {"train": 1, "validation": 5, "test": 7}},
+    }
+
+
 def profile_steps(args):
     """A short, untimed run of the workload for profilers: initial solve, then K plain steps
     (no graph), so that every kernel launch is visible separately."""
@@ -557,14 +601,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", type=int, choices=[64, 32], default=64,
                     help="32: the FP32-bulk variant (its own metric line)")
-    ap.add_argument("--workload", choices=["channel", "ensemble"], default="channel",
-                    help="ensemble: the 64-channel batched ensemble (its own JSON line, 1 GPU)")
+    ap.add_argument("--workload", choices=["channel", "ensemble", "closure"], default="channel",
+                    help="ensemble: the 64-channel batched ensemble; closure: the learned-closure workflow "
+                         "(each its own JSON line, 1 GPU)")
+    ap.add_argument("--closure-span", type=float, default=50.0, help="closure: convective units of data and of the test runs")
+    ap.add_argument("--closure-val-span", type=float, default=20.0)
+    ap.add_argument("--closure-spinup", type=float, default=20.0)
+    ap.add_argument("--closure-train-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.profile_steps > 0:
         profile_steps(args)
         return
     if args.workload == "ensemble":
         print(json.dumps(run_ensemble(args)))
+        return
+    if args.workload == "closure":
+        print(json.dumps(run_closure(args)))
         return
     if args.warmup < 3:
         args.warmup = 3

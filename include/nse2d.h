@@ -263,6 +263,11 @@ int  nse2d_cnn_get_params(nse2d_cnn* c, int layer, float* w, float* b);
 int  nse2d_cnn_get_grads(nse2d_cnn* c, int layer, float* w, float* b);
 /* in_scales: the 4 scales of omega, psi, u, v */
 int  nse2d_cnn_set_scales(nse2d_cnn* c, const double* in_scales, double tau_scale);
+/* Where the model acts: tau = 0 on the wall_rows rows next to each wall (the wall row
+ * included; default 1), in the loss and in the output; the output is multiplied by gain
+ * (default 1); with row_mean != 0 every row of the output is replaced by its x-mean (the
+ * mean-flow part of tau, which is what the mean velocity and Re_tau see). */
+int  nse2d_cnn_set_application(nse2d_cnn* c, int wall_rows, double gain, int row_mean);
 /* tau (FP64, zero on the wall rows) from one field's omega, psi, u, v; asynchronous and
  * graph-capturable */
 int  nse2d_cnn_forward(nse2d_cnn* c, const double* w, const double* psi, const double* u, const double* v, double* tau,
@@ -275,9 +280,11 @@ int  nse2d_cnn_gradients(nse2d_cnn* c, const double* w, const double* psi, const
 int  nse2d_cnn_train_step(nse2d_cnn* c, const double* w, const double* psi, const double* u, const double* v,
                           const double* tau, const int* idx, int nb, float lr, float weight_decay, float* loss,
                           cudaStream_t s);
-/* Attach a model of the context's grid (NULL detaches): every stage then evaluates it on its
- * own psi and omega^(s) and subtracts tau from the rhs of the interior rows. Precision 64. */
-int  nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net);
+/* Attach a model of the context's grid (NULL detaches): tau is subtracted from the rhs of the
+ * interior rows. every_stage != 0: the model runs before every stage on that stage's psi,
+ * omega^(s); 0: it runs once per step on psi^n, omega^n and its tau is held over the three
+ * stages. Precision 64. */
+int  nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net, int every_stage);
 
 const char* nse2d_last_error(void);
 

@@ -78,6 +78,9 @@ struct Cnn {
     int* err = nullptr;
     double in_scale[CN_CIN - 1] = {1.0, 1.0, 1.0, 1.0};
     double out_tau = 1.0;
+    int wall_rows = 1;                    // rows next to each wall (the wall row included) with tau = 0
+    double gain = 1.0;                    // factor on the applied tau
+    bool row_mean = false;                // apply the x-mean of tau on every row (the mean-flow part)
     long long step = 0;
 };
 
@@ -159,17 +162,35 @@ __global__ void k_im2col(const __nv_bfloat16* h, int C, int Nx, int Ny, int P, i
     *reinterpret_cast<uint4*>(A + (size_t)p * K + k0) = *reinterpret_cast<const uint4*>(v);
 }
 
-// tau = tau_scale z[p][0] on interior rows, 0 on the walls (batch slot 0)
-__global__ void k_unpack_output(const float* z, int ldz, double* tau, int Nx, int Ny, double ts) {
+// tau = tau_scale z[p][0] away from the walls, 0 on the wall_rows rows next to each wall
+// (batch slot 0)
+__global__ void k_unpack_output(const float* z, int ldz, double* tau, int Nx, int Ny, double ts, int wall_rows) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= Nx * Ny) return;
     const int j = p / Nx;
-    tau[p] = (j == 0 || j == Ny - 1) ? 0.0 : ts * (double)z[(size_t)p * ldz];
+    tau[p] = (j < wall_rows || j >= Ny - wall_rows) ? 0.0 : ts * (double)z[(size_t)p * ldz];
+}
+
+// the x-mean of tau on every row: one CTA per row
+__global__ void __launch_bounds__(CN_NT) k_unpack_row_mean(const float* z, int ldz, double* tau, int Nx, int Ny, double ts,
+                                                           int wall_rows) {
+    __shared__ double red[CN_NT];
+    const int j = blockIdx.x;
+    double sum = 0.0;
+    for (int i = threadIdx.x; i < Nx; i += CN_NT) sum += (double)z[((size_t)j * Nx + i) * ldz];
+    red[threadIdx.x] = sum;
+    __syncthreads();
+    for (int st = CN_NT / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    const double m = (j < wall_rows || j >= Ny - wall_rows) ? 0.0 : ts * red[0] / (double)Nx;
+    for (int i = threadIdx.x; i < Nx; i += CN_NT) tau[(size_t)j * Nx + i] = m;
 }
 
 // loss partials and dZ of the output layer: d = z - tau / tau_scale on interior pixels
 __global__ void __launch_bounds__(CN_NT) k_loss(const float* z, int ldz, const double* tau, const int* idx, double inv_ts,
-                                                int Nx, int Ny, int P, int Ppad, float inv_pint, float* dz,
+                                                int Nx, int Ny, int P, int Ppad, int wall_rows, float inv_pint, float* dz,
                                                 __nv_bfloat16* dzb, float* lpart) {
     __shared__ float red[CN_NT];
     const int p = blockIdx.x * CN_NT + threadIdx.x;
@@ -179,7 +200,7 @@ __global__ void __launch_bounds__(CN_NT) k_loss(const float* z, int ldz, const d
         float g = 0.f;
         if (p < P) {
             const int b = p / nxy, r = p - b * nxy, j = r / Nx;
-            if (j != 0 && j != Ny - 1) {
+            if (j >= wall_rows && j < Ny - wall_rows) {
                 const float d = z[(size_t)p * ldz] - (float)(tau[(size_t)idx[b] * nxy + r] * inv_ts);
                 l = d * d;
                 g = 2.f * d * inv_pint;
@@ -400,7 +421,12 @@ static PackSrc pack_src(const Cnn* n, const double* w, const double* psi, const 
 int cnn_forward(Cnn* n, const double* w, const double* psi, const double* u, const double* v, double* tau, cudaStream_t s) {
     set_batch(n, 1);
     if (cnn_forward_batch(n, pack_src(n, w, psi, u, v), s)) return -1;
-    k_unpack_output<<<grid_of(n->nxy), CN_NT, 0, s>>>(n->z[CN_LAYERS - 1], n->npad[CN_LAYERS - 1], tau, n->Nx, n->Ny, n->out_tau);
+    if (n->row_mean)
+        k_unpack_row_mean<<<n->Ny, CN_NT, 0, s>>>(n->z[CN_LAYERS - 1], n->npad[CN_LAYERS - 1], tau, n->Nx, n->Ny,
+                                                  n->out_tau * n->gain, n->wall_rows);
+    else
+        k_unpack_output<<<grid_of(n->nxy), CN_NT, 0, s>>>(n->z[CN_LAYERS - 1], n->npad[CN_LAYERS - 1], tau, n->Nx, n->Ny,
+                                                          n->out_tau * n->gain, n->wall_rows);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -408,9 +434,9 @@ int cnn_forward(Cnn* n, const double* w, const double* psi, const double* u, con
 // Loss against tau (samples idx of the batch) and the gradients of every layer (after the forward pass).
 static int cnn_backward(Cnn* n, const double* tau, cudaStream_t s) {
     const int nlb = (n->Ppad + CN_NT - 1) / CN_NT;
-    const int pint = n->nb * n->Nx * (n->Ny - 2);
+    const int pint = n->nb * n->Nx * (n->Ny - 2 * n->wall_rows);
     k_loss<<<nlb, CN_NT, 0, s>>>(n->z[CN_LAYERS - 1], n->npad[CN_LAYERS - 1], tau, n->idx, 1.0 / n->out_tau, n->Nx, n->Ny, n->P,
-                                 n->Ppad, 1.f / (float)pint, n->dz, n->dzb, n->lpart);
+                                 n->Ppad, n->wall_rows, 1.f / (float)pint, n->dz, n->dzb, n->lpart);
     NSE_CUDA_TRY(cudaGetLastError());
     k_fold<<<1, 32, 0, s>>>(n->lpart, nlb, 1, n->loss, 1.f / (float)pint);
     NSE_CUDA_TRY(cudaGetLastError());
@@ -647,7 +673,18 @@ int nse2d_cnn_set_scales(nse2d_cnn* c, const double* in_scales, double tau_scale
     return 0;
 }
 
-int nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net) {
+int nse2d_cnn_set_application(nse2d_cnn* c, int wall_rows, double gain, int row_mean) {
+    if (!c || wall_rows < 1 || 2 * wall_rows >= c->n->Ny - 1 || !(gain >= 0.0)) {
+        set_error("nse2d_cnn_set_application: wall_rows in [1, (Ny - 1) / 2), gain >= 0");
+        return -1;
+    }
+    c->n->wall_rows = wall_rows;
+    c->n->gain = gain;
+    c->n->row_mean = row_mean != 0;
+    return 0;
+}
+
+int nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net, int every_stage) {
     if (!ctx || !ctx->c) { set_error("nse2d_set_closure: null context"); return -1; }
     Context* c = ctx->c;
     if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
@@ -663,6 +700,7 @@ int nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net) {
         NSE_CUDA_TRY(cudaMemset(c->closure_tau, 0, 3 * c->N * sizeof(double)));
     }
     c->closure_net = net->n;
+    c->closure_every_stage = every_stage != 0;
     return 0;
 }
 

@@ -135,7 +135,8 @@ struct Context {
     int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
     // learned closure: the model evaluated before every stage and its output tau [Ny][Nx]
     struct Cnn* closure_net = nullptr;
-    double* closure_tau = nullptr;
+    double* closure_tau = nullptr;       // tau, then the u, v scratch of the model's inputs
+    bool closure_every_stage = true;     // false: tau of the step's first stage for all three
     // FP32-bulk variant (precision 32): base profiles (FP64) and FP32 fluctuations
     bool prec32 = false;
     float *wf = nullptr, *w1f = nullptr, *w2f = nullptr, *psif = nullptr, *rhsf = nullptr;

@@ -456,9 +456,12 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
     p.w_in = w_in; p.w_n = w_n; p.w_out = w_out; p.rhs_out = rhs_out; p.stage = stage;
     // the learned closure's tau of this stage's state (the model runs just before the stage)
     if (c->closure_net) {
-        double* u = c->closure_tau + c->N;
-        double* v = c->closure_tau + 2 * c->N;
-        if (uv_from_psi(c, c->psi, u, v, s) || cnn_forward(c->closure_net, w_in, c->psi, u, v, c->closure_tau, s)) return -1;
+        if (stage == 1 || c->closure_every_stage) {
+            double* u = c->closure_tau + c->N;
+            double* v = c->closure_tau + 2 * c->N;
+            if (uv_from_psi(c, c->psi, u, v, s) || cnn_forward(c->closure_net, w_in, c->psi, u, v, c->closure_tau, s))
+                return -1;
+        }
         p.closure = c->closure_tau;
     }
     if (c->stage_tma) {

@@ -107,10 +107,11 @@ def load(path=LIB_PATH):
         "nse2d_cnn_get_params": (I, [P, I, P, P]),
         "nse2d_cnn_get_grads": (I, [P, I, P, P]),
         "nse2d_cnn_set_scales": (I, [P, P, D]),
+        "nse2d_cnn_set_application": (I, [P, I, D, I]),
         "nse2d_cnn_forward": (I, [P, P, P, P, P, P, P]),
         "nse2d_cnn_gradients": (I, [P, P, P, P, P, P, P, I, P, P]),
         "nse2d_cnn_train_step": (I, [P, P, P, P, P, P, P, I, ctypes.c_float, ctypes.c_float, P, P]),
-        "nse2d_set_closure": (I, [P, P]),
+        "nse2d_set_closure": (I, [P, P, I]),
         "nse2d_last_error": (ctypes.c_char_p, []),
         "nse2d_set_abort_on_error": (V, [I]),
         "nse2d_testapi_set_free_slip": (V, [I]),
@@ -267,6 +268,11 @@ class Cnn:
         _check(self.lib.nse2d_cnn_set_scales(self.h, _ptr(s), float(tau_scale)))
         self.scales = (tuple(float(x) for x in s), float(tau_scale))
 
+    def set_application(self, wall_rows=1, gain=1.0, row_mean=False):
+        """tau = 0 on the wall_rows rows next to each wall (loss and output); output times gain;
+        row_mean: every output row replaced by its x-mean."""
+        _check(self.lib.nse2d_cnn_set_application(self.h, int(wall_rows), float(gain), 1 if row_mean else 0))
+
     def forward(self, w, psi, u, v, tau, stream=None):
         _check(self.lib.nse2d_cnn_forward(self.h, _ptr(w), _ptr(psi), _ptr(u), _ptr(v), _ptr(tau), _stream(stream)))
 
@@ -315,9 +321,10 @@ class Solver:
         self.close()
 
     # ---- state ----
-    def set_closure(self, cnn):
-        """Attach a closure model (Cnn of this grid) to every stage; None detaches it."""
-        _check(self.lib.nse2d_set_closure(self.h, cnn.h if cnn is not None else None))
+    def set_closure(self, cnn, every_stage=True):
+        """Attach a closure model (Cnn of this grid): evaluated before every stage, or once per
+        step and held over its stages; None detaches it."""
+        _check(self.lib.nse2d_set_closure(self.h, cnn.h if cnn is not None else None, 1 if every_stage else 0))
         self._closure = cnn
 
     def set_omega(self, w, stream=None):
