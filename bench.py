@@ -123,10 +123,11 @@ def kernel_bytes(name, stage, Nx, Ny):
     return 0
 
 
-def read_traffic(Nx, Ny):
+def read_traffic(Nx, Ny, precision=64):
     """DRAM bytes (read + write) per launch of each kernel from the committed ncu summary of
-    this grid (lines `kernel bytes`), or {} when there is none."""
-    path = os.path.join(ROOT, "profiles", f"traffic_step_{Nx}x{Ny}.txt")
+    this grid and precision (lines `kernel bytes`), or {} when there is none."""
+    tag = "step" if precision == 64 else "step32"
+    path = os.path.join(ROOT, "profiles", f"traffic_{tag}_{Nx}x{Ny}.txt")
     out = {}
     if os.path.isfile(path):
         for ln in open(path):
@@ -328,7 +329,7 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": int(a["bytes"] / a["launches"])}
     dom = max(agg, key=lambda k: agg[k]["ms"])
     dk = kernels[dom]
-    traffic = read_traffic(Nx, Ny).get(dom)
+    traffic = read_traffic(Nx, Ny, P).get(dom)
     step_gbs = B_step / (step_ms * 1e-3) / 1e9
     h2d = N * 8 / args.steps + 8 * 3
     d2h = 2 * N * 8 / args.steps + 128
@@ -574,7 +575,7 @@ def profile_steps(args):
     if args.nx:
         W["Nx"], W["Ny"] = args.nx, args.ny
     y = tanh_y(W["Ny"], W["beta"], W["h"])
-    s = nse.Solver(**W)
+    s = nse.Solver(precision=args.precision, **W)
     s.set_omega(initial_vorticity(W["Nx"], W["Ny"], W["Lx"], y, seed=1))
     s.step(args.profile_steps, use_graph=False)
     torch.cuda.synchronize()
