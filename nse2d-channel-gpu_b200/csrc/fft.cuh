@@ -61,10 +61,54 @@ template <typename T, bool INV> NSE_HD void dft8(cpx<T>* v) {
     v[3] = cadd(e[3], o3);   v[7] = csub(e[3], o3);
 }
 
+// 16-point DFT as 4 x 4: four 4-point DFTs over x[4 n1 + n2] (n1), the twiddles W16^(n2 k1),
+// four 4-point DFTs over n2; X[k1 + 4 k2]. W16^j = e^{-/+ 2 pi i j / 16}: cos(pi/8), sin(pi/8)
+// and 1/sqrt(2) are the only constants.
+template <typename T> NSE_HD cpx<T> mul_w16(cpx<T> a, int j, bool inv) {
+    const T c = (T)0.92387953251128675612818318939678828682;   // cos(pi/8)
+    const T s = (T)0.38268343236508977172845998403039886676;   // sin(pi/8)
+    const T r = (T)0.70710678118654752440084436210484903928;   // 1/sqrt(2)
+    // forward W16^j = (cos(2 pi j/16), -sin(2 pi j/16)); inverse conjugated
+    T wr, wi;
+    switch (j) {
+        case 1: wr = c; wi = -s; break;
+        case 2: wr = r; wi = -r; break;
+        case 3: wr = s; wi = -c; break;
+        case 6: wr = -r; wi = -r; break;
+        case 9: wr = -c; wi = s; break;
+        default: wr = 1; wi = 0; break;                          // j = 0 (j = 4 is handled by the caller)
+    }
+    if (inv) wi = -wi;
+    return {a.x * wr - a.y * wi, a.x * wi + a.y * wr};
+}
+template <typename T, bool INV> NSE_HD void dft16(cpx<T>* v) {
+    cpx<T> y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        cpx<T> q[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+        dft4<T, INV>(q);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            const int j = n2 * k1;
+            if (j == 0) y[n2][k1] = q[k1];
+            else if (j == 4) y[n2][k1] = INV ? mul_pi(q[k1]) : mul_mi(q[k1]);
+            else y[n2][k1] = mul_w16(q[k1], j, INV);
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        cpx<T> q[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+        dft4<T, INV>(q);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = q[k2];
+    }
+}
+
 template <typename T, int R, bool INV> NSE_HD void dftR(cpx<T>* v) {
     if constexpr (R == 2) dft2<T, INV>(v);
     else if constexpr (R == 4) dft4<T, INV>(v);
-    else dft8<T, INV>(v);
+    else if constexpr (R == 8) dft8<T, INV>(v);
+    else dft16<T, INV>(v);
 }
 
 }  // namespace nse2d

@@ -141,4 +141,111 @@ __device__ __forceinline__ void ip_passes(cpx<T>* buf, const cpx<T>* tw) {
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Radix-16 plan of the FP64 row transforms: passes of radix 16, the last one of the remaining
+// 1..4 bits. Pass 0 reads its 16 points straight from global memory into registers: with the
+// digit-reversed layout, the butterfly that starts at position dit16_pos(t) (t < M/16) holds
+// the points t + (M/16) r, r < 16, so thread t loads a coalesced column of the row and writes
+// its 16 outputs to positions dit16_pos(t) + s. Later passes exchange through shared memory as
+// above (same padding). Twiddles of pass q >= 1 come from a table of (W^m, W^2m, W^4m, W^8m),
+// L = R LP, m < LP; W^(r m) is applied as W^(a m) W^(4 b m) with r = a + 4 b, so that at most
+// six twiddles are live at a time.
+// ---------------------------------------------------------------------------------------
+template <int M> struct p16_plan {
+    static constexpr int m = ilog2<M>::v;
+    static constexpr int P = (m + 3) / 4;
+    static constexpr int bits(int q) { return (q < P - 1) ? 4 : m - 4 * (P - 1); }
+    static constexpr int R(int q) { return 1 << bits(q); }
+    static constexpr int LP(int q) { return 1 << (4 * q); }
+    static constexpr int off(int q) {           // first table entry of pass q >= 1
+        int o = 0;
+        for (int i = 1; i < q; ++i) o += 4 * LP(i);
+        return o;
+    }
+};
+
+template <int M> __host__ __device__ __forceinline__ int dit16_pos(int n) {
+    constexpr int P = p16_plan<M>::P;
+    int p = 0, sn = 0;
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q) {
+        const int b = p16_plan<M>::bits(q);
+        p |= ((n >> sn) & ((1 << b) - 1)) << (4 * q);
+        sn += b;
+    }
+    return p;
+}
+
+template <typename C>
+inline void p16_twiddle_table(int M, const C* tw, std::vector<C>& out) {
+    out.clear();
+    int m = 0;
+    while ((1 << m) < M) ++m;
+    const int P = (m + 3) / 4;
+    for (int q = 1; q < P; ++q) {
+        const int LP = 1 << (4 * q), R = 1 << ((q < P - 1) ? 4 : m - 4 * (P - 1)), L = R * LP, step = M / L;
+        for (int k = 0; k < LP; ++k)
+            for (int e = 1; e <= 8; e *= 2) out.push_back(tw[((long long)e * step * k) % M]);
+    }
+    if (out.empty()) out.push_back(tw[0]);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ cpx<T> p16_tw(cpx<T> a, cpx<T> w) {
+    return INV ? cmulc(a, w) : cmul(a, w);
+}
+
+template <typename T, int M, int Q, bool INV, int NT>
+__device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw) {
+    constexpr int R = p16_plan<M>::R(Q), LP = p16_plan<M>::LP(Q), NB = M / R, OFF = p16_plan<M>::off(Q);
+#pragma unroll 1
+    for (int b0 = 0; b0 < NB; b0 += NT) {
+        const int b = b0 + (int)threadIdx.x;
+        if (NB % NT != 0 && b >= NB) break;
+        const int mm = b & (LP - 1);
+        const int base = (b - mm) * R + mm;
+        cpx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = buf[ip_idx(base + r * LP)];
+        if (mm > 0) {
+            const int t = OFF + 4 * mm;
+            const cpx<T> w1 = ldtw(tw, t);
+            if constexpr (R == 2) {
+                v[1] = p16_tw<T, INV>(v[1], w1);
+            } else {
+                const cpx<T> w2 = ldtw(tw, t + 1), w3 = cmul(w1, w2);
+#pragma unroll
+                for (int r = 1; r < R; ++r) {                  // low digit a = r mod 4
+                    const int a = r & 3;
+                    if (a) v[r] = p16_tw<T, INV>(v[r], a == 1 ? w1 : (a == 2 ? w2 : w3));
+                }
+                if constexpr (R >= 8) {                        // high digit b = r / 4
+                    const cpx<T> w4 = ldtw(tw, t + 2);
+                    cpx<T> w8 = w4, w12 = w4;
+                    if constexpr (R == 16) {
+                        w8 = ldtw(tw, t + 3);
+                        w12 = cmul(w4, w8);
+                    }
+#pragma unroll
+                    for (int r = 4; r < R; ++r) {
+                        const int hb = r >> 2;
+                        v[r] = p16_tw<T, INV>(v[r], hb == 1 ? w4 : (hb == 2 ? w8 : w12));
+                    }
+                }
+            }
+        }
+        dftR<T, R, INV>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[ip_idx(base + r * LP)] = v[r];
+    }
+}
+
+template <typename T, int M, int Q, bool INV, int NT>
+__device__ __forceinline__ void p16_passes_from(cpx<T>* buf, const cpx<T>* tw) {
+    if constexpr (Q < p16_plan<M>::P) {
+        p16_pass<T, M, Q, INV, NT>(buf, tw);
+        __syncthreads();
+        p16_passes_from<T, M, Q + 1, INV, NT>(buf, tw);
+    }
+}
+
 }  // namespace nse2d

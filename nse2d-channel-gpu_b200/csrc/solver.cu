@@ -309,7 +309,7 @@ int context_create(const Config& cfg, Context** out) {
     }
     std::vector<cpx<double>> tw_full, tw, wN;
     twiddles(c->M, tw_full, wN);
-    pass_twiddle_table(c->M, tw_full.data(), tw);
+    p16_twiddle_table(c->M, tw_full.data(), tw);
     if (dalloc(&c->tw, tw.size())) return fail();
     if (cudaMemcpy(c->tw, tw.data(), tw.size() * sizeof(tw[0]), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->wN, wN.data(), wN.size() * sizeof(wN[0]), cudaMemcpyHostToDevice)) {

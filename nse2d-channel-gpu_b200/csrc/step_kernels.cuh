@@ -430,23 +430,45 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const int jb = p.row0 + blockIdx.x * p.rows_per_cta;
     const int je = min(p.row0 + p.nrows, jb + p.rows_per_cta);
+    constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     for (int j = jb; j < je; ++j) {
-        const cpx<double>* row = reinterpret_cast<const cpx<double>*>(p.src + (size_t)j * p.Nx);
-        for (int n = threadIdx.x; n < M; n += IP_NT) cp_async16(&buf[ip_idx(dit_pos<M>(n))], &row[n]);
-        cp_async_wait_all();
+        const double2* row = reinterpret_cast<const double2*>(p.src + (size_t)j * p.Nx);
+        // pass 0 from global: thread t transforms the points t + NB0 r (a coalesced column)
+#pragma unroll 1
+        for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+            const int t = b0 + (int)threadIdx.x;
+            if (NB0 % IP_NT != 0 && t >= NB0) break;
+            cpx<double> v[R0];
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const double2 z = __ldg(row + t + NB0 * r);
+                v[r] = {z.x, z.y};
+            }
+            dftR<double, R0, false>(v);
+            const int p0 = dit16_pos<M>(t);
+#pragma unroll
+            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+        }
         __syncthreads();
-        ip_passes<double, M, 1, false, IP_NT>(buf, p.tw);
+        p16_passes_from<double, M, 1, false, IP_NT>(buf, p.tw);
+        // X_k and X_{M-k} from one pair: with s = Z_k + conj Z_{M-k}, d = Z_k - conj Z_{M-k},
+        //   X_k = s/2 + W^k (-i d)/2,   X_{M-k} = conj(s)/2 + W^{M-k} (i conj d)/2
+        // (k = 0 pairs Z_0 with itself and gives X_0 and X_M; k = M/2 is its own pair).
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-#pragma unroll 4
-        for (int k = threadIdx.x; k <= M; k += IP_NT) {
-            const int ka = (k == M ? 0 : k), kb = (k == 0 ? 0 : M - k);
-            const cpx<double> a = buf[ip_idx(ka)];
-            const cpx<double> b0 = buf[ip_idx(kb)];
-            const cpx<double> b = {b0.x, -b0.y};
-            const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
-            const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
-            const cpx<double> X = cadd(E, cmul(ldtw(p.wN, k), mul_mi(D)));
+#pragma unroll 2
+        for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+            const int kb = (k == 0 ? 0 : M - k);
+            const cpx<double> a = buf[ip_idx(k)];
+            const cpx<double> b = buf[ip_idx(kb)];
+            const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
+            const cpx<double> df = {0.5 * (a.x - b.x), 0.5 * (a.y + b.y)};     // d/2
+            const cpx<double> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
             dst[k] = make_double2(X.x, X.y);
+            if (k < M / 2) {
+                const int m = M - k;                                           // m = M when k = 0
+                const cpx<double> Y = cadd(cpx<double>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<double>{df.y, df.x}));
+                dst[m] = make_double2(Y.x, Y.y);
+            }
         }
         __syncthreads();
     }
@@ -507,6 +529,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr double scale = 1.0 / (double)M;
+    constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     for (int j = j0; j < j1; ++j) {
         double* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {
@@ -514,17 +537,30 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             for (int i = threadIdx.x; i < Nx; i += IP_NT) dst[i] = v;
             continue;
         }
+        // pass 0 from global with the merge: thread t forms Z_n, n = t + NB0 r, from X_n and
+        // X_{M-n} (s = X_n + conj X_{M-n}, d = X_n - conj X_{M-n}, Z_n = s/2 + i d conj(W^n)/2)
+        // and transforms them in registers
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
-#pragma unroll 4
-        for (int k = threadIdx.x; k < M; k += IP_NT) {
-            const double2 av = __ldcs(X + k), bv = __ldcs(X + (M - k));
-            const cpx<double> a = {av.x, av.y}, b = {bv.x, -bv.y};
-            const cpx<double> E = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y)};
-            const cpx<double> D = {0.5 * (a.x - b.x), 0.5 * (a.y - b.y)};
-            buf[ip_idx(dit_pos<M>(k))] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, k))));
+#pragma unroll 1
+        for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+            const int t = b0 + (int)threadIdx.x;
+            if (NB0 % IP_NT != 0 && t >= NB0) break;
+            cpx<double> v[R0];
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + NB0 * r;
+                const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
+                const cpx<double> sm = {0.5 * (av.x + bv.x), 0.5 * (av.y - bv.y)};
+                const cpx<double> df = {0.5 * (av.x - bv.x), 0.5 * (av.y + bv.y)};
+                v[r] = cadd(sm, mul_pi(cmulc(df, ldtw(p.wN, n))));
+            }
+            dftR<double, R0, true>(v);
+            const int p0 = dit16_pos<M>(t);
+#pragma unroll
+            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
         }
         __syncthreads();
-        ip_passes<double, M, 1, true, IP_NT>(buf, p.tw);
+        p16_passes_from<double, M, 1, true, IP_NT>(buf, p.tw);
         for (int n = threadIdx.x; n < M; n += IP_NT) {
             const cpx<double> z = buf[ip_idx(n)];
             reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
