@@ -493,22 +493,36 @@ static FftParams fft_params(Context* c) {
 }
 
 // Forward transforms: one row per CTA (many small CTAs per SM hide each other's load latency).
+// Row transforms: one wave of CTAs (occupancy x SMs, at most the number of rows), each taking
+// the rows blockIdx.x, blockIdx.x + grid, ...; a partial second wave of one-row CTAs would
+// leave most SMs idle at its end.
+template <typename K> static int fft_wave(K kern, size_t smem, int nrows, int num_sms, int* grid) {
+    int per_sm = 0;
+    NSE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, IP_NT, smem));
+    if (per_sm < 1) { set_error("a row transform kernel cannot be resident (%zu bytes of shared memory)", smem); return -1; }
+    *grid = std::max(1, std::min(nrows, per_sm * num_sms));
+    return 0;
+}
+
 template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) {
     const size_t sm = fft_smem(M);
-    NSE_CUDA_TRY(cudaFuncSetAttribute(k_fft_fwd<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    p.rows_per_cta = 1;
-    k_fft_fwd<M><<<p.nrows, IP_NT, sm, s>>>(p);
+    int grid = 0;
+    if (fft_wave(k_fft_fwd<M>, sm, p.nrows, c->num_sms, &grid)) return -1;
+    k_fft_fwd<M><<<grid, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-// Inverse transforms: bands of at least 3 rows (the Thom closure needs rows 1-2 and Ny-3..Ny-2
-// in one CTA each).
+// Inverse transforms: contiguous bands of L = ceil(Ny / wave) rows, one wave of CTAs (adjacent
+// rows of the spectral buffer are adjacent in memory; strided rows measured slower). The Thom
+// closure is applied by the CTA that writes the second row of each wall.
 template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
     const size_t sm = fft_smem(M);
-    NSE_CUDA_TRY(cudaFuncSetAttribute(k_ifft_thom<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    p.rows_per_cta = 3;
-    const int grid = std::max(1, c->Ny / p.rows_per_cta);   // the last band takes the remainder
+    int wave = 0;
+    if (fft_wave(k_ifft_thom<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
+    p.rows_per_cta = (c->Ny + wave - 1) / wave;
+    const int grid = std::max(1, c->Ny / p.rows_per_cta);          // the last band takes the remainder
     k_ifft_thom<M><<<grid, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;

@@ -391,7 +391,8 @@ struct FftParams {
     double* psi;             // inverse output [Ny][Nx]
     const cpx<double>* tw;   // per-pass twiddle pairs of the M-point transform (pass_twiddle_table)
     const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
-    int Nx, Ny, Hp, rows_per_cta;
+    int Nx, Ny, Hp;
+    int rows_per_cta;        // inverse: rows of a band
     int row0, nrows;         // forward: transform rows row0 .. row0 + nrows - 1
     // inverse only: Thom closure (src/ops.cu:102-158) and the closure_diag wall bookkeeping
     double* w;               // omega^(s+1): wall rows rewritten
@@ -428,10 +429,9 @@ template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
-    const int jb = p.row0 + blockIdx.x * p.rows_per_cta;
-    const int je = min(p.row0 + p.nrows, jb + p.rows_per_cta);
+    const int je = p.row0 + p.nrows;
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
-    for (int j = jb; j < je; ++j) {
+    for (int j = p.row0 + blockIdx.x; j < je; j += gridDim.x) {      // rows strided over one wave of CTAs
         const double2* row = reinterpret_cast<const double2*>(p.src + (size_t)j * p.Nx);
         // pass 0 from global: thread t transforms the points t + NB0 r (a coalesced column)
 #pragma unroll 1
@@ -518,19 +518,21 @@ __host__ __device__ __forceinline__ void band_of(int b, int nb, int L, int Ny, i
 
 // Inverse real FFT of every row (the reference's cuFFT inverse + scale, src/poisson.cuh:110-114):
 // the merge step forms Z_k = E_k + i O_k, E_k = (X_k + conj X_{M-k}) / 2,
-// O_k = (X_k - conj X_{M-k}) W_{2M}^{-k} / 2, straight from HBM into the digit-reversed layout;
-// the passes give z_n = x_2n + i x_2n+1 (times M). Then the Thom closure of omega^(s+1) by the
-// first and the last CTA, and, in the stage-3 launch, the time advance by the last CTA.
+// O_k = (X_k - conj X_{M-k}) W_{2M}^{-k} / 2, straight from HBM into the registers of the first
+// (radix-16) pass; the passes give z_n = x_2n + i x_2n+1 (times M). The Thom closure of
+// omega^(s+1) is applied by the CTA that writes the second of rows 1-2 (bottom) or
+// Ny-3..Ny-2 (top), and, in the stage-3 launch, the last CTA advances the time.
 template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
+    __shared__ bool thom_now;
     const int Nx = p.Nx, Ny = p.Ny;
-    int j0, j1;
-    band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr double scale = 1.0 / (double)M;
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
-    for (int j = j0; j < j1; ++j) {
+    int j0, j1;
+    band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
+    for (int j = j0; j < j1; ++j) {                                   // a contiguous band of rows
         double* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {
             const double v = (j == 0) ? p.psi_bot : p.psi_top;
@@ -566,10 +568,27 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
         }
         __syncthreads();
-    }
-    if (p.do_thom) {
-        if (j0 <= 1 && j1 >= 3) thom_row<IP_NT>(p, false);
-        if (j0 <= Ny - 3 && j1 >= Ny - 1) thom_row<IP_NT>(p, true);
+        if (p.do_thom) {
+            // rows 1, 2 close the bottom wall and rows Ny-3, Ny-2 the top one: the CTA that
+            // writes the second row of a wall applies its Thom closure (an arrival count per
+            // wall, reset by that CTA)
+            const bool bot = (j == 1 || j == 2), top = (j == Ny - 3 || j == Ny - 2);
+            if (bot || top) {
+                __threadfence();                             // this row before the arrival count
+                __syncthreads();
+                for (int wall = 0; wall < 2; ++wall) {
+                    if (!(wall == 0 ? bot : top)) continue;
+                    if (threadIdx.x == 0) thom_now = (atomicAdd(&p.ctl->thom_done[wall], 1u) == 1u);
+                    __syncthreads();
+                    if (thom_now) {
+                        __threadfence();
+                        thom_row<IP_NT>(p, wall == 1);
+                        if (threadIdx.x == 0) p.ctl->thom_done[wall] = 0;
+                    }
+                    __syncthreads();
+                }
+            }
+        }
     }
     if (p.advance) {
         // the last CTA to finish advances the time: t += dt and the output snap
