@@ -231,7 +231,7 @@ struct Fft32Params {
     cpx<double>* hat;          // [Ny][Hp], FP64
     float* psi;                // inverse output psi'
     float* w;                  // inverse: w'^(s+1), whose wall rows the Thom closure sets
-    const cpx<float>* tw;      // per-pass twiddle pairs (pass_twiddle_table), FP32
+    const cpx<float>* tw;      // per-pass twiddles of the radix-16 plan (p16_twiddle_table), FP32
     const cpx<float>* wN;      // M + 1 split/merge twiddles, FP32
     const double* dy_edge;
     Ctl* ctl;
@@ -247,21 +247,41 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
     cpx<float>* buf = reinterpret_cast<cpx<float>*>(smem_raw);
     const int j = 1 + blockIdx.x;                       // interior rows
     if (j > p.Ny - 2) return;
-    const cpx<float>* row = reinterpret_cast<const cpx<float>*>(p.src + (size_t)j * p.Nx);
-    for (int n = threadIdx.x; n < M; n += IP_NT) cp_async8(&buf[ip_idx(dit_pos<M>(n))], &row[n]);
-    cp_async_wait_all();
+    const float2* row = reinterpret_cast<const float2*>(p.src + (size_t)j * p.Nx);
+    constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
+    // pass 0 from global (radix-16 plan of fft_rows.cuh): thread t transforms t + NB0 r
+#pragma unroll 1
+    for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+        const int t = b0 + (int)threadIdx.x;
+        if (NB0 % IP_NT != 0 && t >= NB0) break;
+        cpx<float> v[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const float2 z = __ldg(row + t + NB0 * r);
+            v[r] = {z.x, z.y};
+        }
+        dftR<float, R0, false>(v);
+        const int p0 = dit16_pos<M>(t);
+#pragma unroll
+        for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+    }
     __syncthreads();
-    ip_passes<float, M, 1, false, IP_NT>(buf, p.tw);
+    p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
+    // the split step for the pair (k, M - k) (see k_fft_fwd)
     double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-    for (int k = threadIdx.x; k <= M; k += IP_NT) {
-        const int ka = (k == M ? 0 : k), kb = (k == 0 ? 0 : M - k);
-        const cpx<float> a = buf[ip_idx(ka)];
-        const cpx<float> b0 = buf[ip_idx(kb)];
-        const cpx<float> b = {b0.x, -b0.y};
-        const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
-        const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
-        const cpx<float> X = cadd(E, cmul(ldtw(p.wN, k), mul_mi(D)));
+    for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+        const int kb = (k == 0 ? 0 : M - k);
+        const cpx<float> a = buf[ip_idx(k)];
+        const cpx<float> b = buf[ip_idx(kb)];
+        const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
+        const cpx<float> df = {0.5f * (a.x - b.x), 0.5f * (a.y + b.y)};
+        const cpx<float> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
         dst[k] = make_double2((double)X.x, (double)X.y);
+        if (k < M / 2) {
+            const int m = M - k;
+            const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<float>{df.y, df.x}));
+            dst[m] = make_double2((double)Y.x, (double)Y.y);
+        }
     }
 }
 
@@ -273,22 +293,36 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr float scale = 1.0f / (float)M;
+    constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     for (int j = j0; j < j1; ++j) {
         float* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {                    // psi' = 0 on the walls
             for (int i = threadIdx.x; i < Nx; i += IP_NT) dst[i] = 0.f;
             continue;
         }
+        // pass 0 from global with the merge (see k_ifft_thom)
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
-        for (int k = threadIdx.x; k < M; k += IP_NT) {
-            const double2 av = __ldcs(X + k), bv = __ldcs(X + (M - k));
-            const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
-            const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
-            const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
-            buf[ip_idx(dit_pos<M>(k))] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, k))));
+#pragma unroll 1
+        for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+            const int t = b0 + (int)threadIdx.x;
+            if (NB0 % IP_NT != 0 && t >= NB0) break;
+            cpx<float> v[R0];
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int n = t + NB0 * r;
+                const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
+                const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
+                const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
+                const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
+                v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
+            }
+            dftR<float, R0, true>(v);
+            const int p0 = dit16_pos<M>(t);
+#pragma unroll
+            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
         }
         __syncthreads();
-        ip_passes<float, M, 1, true, IP_NT>(buf, p.tw);
+        p16_passes_from<float, M, 1, true, IP_NT>(buf, p.tw);
         for (int n = threadIdx.x; n < M; n += IP_NT) {
             const cpx<float> z = buf[ip_idx(n)];
             reinterpret_cast<float2*>(dst)[n] = make_float2(z.x * scale, z.y * scale);

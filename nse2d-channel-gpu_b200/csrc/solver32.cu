@@ -39,7 +39,7 @@ int setup32(Context* c) {
     wN[0] = {1.f, 0.f};
     wN[M] = {-1.f, 0.f};
     if (M % 2 == 0) wN[M / 2] = {0.f, -1.f};
-    pass_twiddle_table(M, full.data(), tw);
+    p16_twiddle_table(M, full.data(), tw);
     if (alloc(&c->twf, tw.size()) || alloc(&c->wNf, wN.size())) return -1;
     NSE_CUDA_TRY(cudaMemcpy(c->twf, tw.data(), tw.size() * sizeof(tw[0]), cudaMemcpyHostToDevice));
     NSE_CUDA_TRY(cudaMemcpy(c->wNf, wN.data(), wN.size() * sizeof(wN[0]), cudaMemcpyHostToDevice));

@@ -389,7 +389,7 @@ struct FftParams {
     const double* src;       // forward: real rows [Ny][Nx]
     cpx<double>* hat;        // [Ny][Hp]
     double* psi;             // inverse output [Ny][Nx]
-    const cpx<double>* tw;   // per-pass twiddle pairs of the M-point transform (pass_twiddle_table)
+    const cpx<double>* tw;   // per-pass twiddles of the radix-16 plan (p16_twiddle_table)
     const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
     int Nx, Ny, Hp;
     int rows_per_cta;        // inverse: rows of a band
