@@ -184,7 +184,9 @@ int  nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s);
  * cudaMalloc/cudaFree pair in its loop. The reduction's scratch is a fixed array inside the
  * library, room for NSE2D_MAXUV_NOALLOC_MAX_BLOCKS per-CTA partials (24 KiB) plus a small
  * control block; the launch uses at most that many CTAs, which stride over the rows, so
- * every Ny fits. Nx must be in [2, 2^30] and Ny >= 3; other sizes are rejected with an error.
+ * every Ny fits. Nx must be in [2, 2^30] and Ny >= 3, and both pointers 8-byte aligned (any
+ * Nx and offset work; 16-byte loads are used where Nx is even and psi 16-byte aligned); other
+ * arguments are rejected with an error.
  * The first call on a device (with that device current) looks up the scratch address and
  * should come before any stream capture on that device. Every call clears the control block
  * on stream s first. One scratch serves all callers on a device: calls that overlap in time

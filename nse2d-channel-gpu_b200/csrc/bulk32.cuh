@@ -362,61 +362,73 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
     }
 }
 
-// ---- max |u|, |v|, |v| a of psibar + psi' (one row per CTA at a time, the grid one wave) ----
+// ---- max |u|, |v|, |v| a of psibar + psi' ----
+// The item layout of k_maxuv_dt: (column strip, row band) items, a window of rows j-1, j, j+1
+// in registers down the band, MX_U rows loaded at a time; here a thread holds 4 columns (one
+// 16-byte load per row; Nx is a power of two >= 4), so a strip is MX32_COLS columns, and the x
+// neighbours c-1 and c+4 come from the adjacent lanes.
 struct Max32Params {
-    MaxParams base;          // a_node, partials, control block, dt constants (base.psi unused)
+    MaxParams base;          // a_node, partials, control block, dt constants, items (base.psi unused)
     const float* psi;        // psi'
     const float* dpsibar;    // [Ny]: psibar_{j+1} - psibar_{j-1} (the RC_DPB row constant)
 };
+constexpr int MX32_COLS = 1024;
 
 static __global__ void __launch_bounds__(256, 3) k_maxuv32(Max32Params q) {
     const MaxParams& p = q.base;
     const int Nx = p.Nx, Ny = p.Ny;
+    const int lane = threadIdx.x & 31;
     double um = 0.0, vm = 0.0, vmm = 0.0;
     float probe = 0.f;
     const double cy = 0.5 * p.inv_deta, cx = 0.5 * p.inv_dx;
-    for (int j = 1 + blockIdx.x; j < Ny - 1; j += gridDim.x) {
-        const float* rm = q.psi + (size_t)(j - 1) * Nx;
-        const float* r0 = q.psi + (size_t)j * Nx;
-        const float* rp = q.psi + (size_t)(j + 1) * Nx;
-        const float db = __ldg(&q.dpsibar[j]);
-        float dym = 0.f, dxm = 0.f;
-        // 4 adjacent columns per thread and load (16 bytes of each row), 2 quads in flight
-        constexpr int U = 2;
-        for (int q0 = threadIdx.x; 4 * q0 < Nx; q0 += U * blockDim.x) {
-            float4 a[U], u[U], d[U];
-            float xl[U], xr[U];
+    const int nitems = p.nstrips * p.nbands;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int strip = item % p.nstrips, band = item / p.nstrips;
+        const int c0 = strip * MX32_COLS + 4 * (int)threadIdx.x;
+        const bool act = c0 < Nx;
+        const int cs = act ? c0 : 0;
+        const int cl = cs > 0 ? cs - 1 : Nx - 1, cr = cs + 4 < Nx ? cs + 4 : 0;
+        const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
+        const bool ldl = act && lane == 0, ldr = act && (lane == 31 || c0 + 4 >= Nx);
+        auto ld4 = [&](int row) { return __ldg(reinterpret_cast<const float4*>(q.psi + (size_t)row * Nx + cs)); };
+        float4 w0 = ld4(j0 - 1), w1 = ld4(j0);
+        for (int j = j0; j < j1; j += MX_U) {
+            float4 nx[MX_U];
+            float el[MX_U], er[MX_U], db[MX_U];
+            double an[MX_U];
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                const int c = 4 * (q0 + k * (int)blockDim.x);
-                if (c < Nx) {
-                    a[k] = __ldg(reinterpret_cast<const float4*>(r0 + c));
-                    u[k] = __ldg(reinterpret_cast<const float4*>(rp + c));
-                    d[k] = __ldg(reinterpret_cast<const float4*>(rm + c));
-                    xl[k] = __ldg(r0 + (c > 0 ? c - 1 : Nx - 1));
-                    xr[k] = __ldg(r0 + (c + 4 < Nx ? c + 4 : 0));
-                } else {
-                    a[k] = u[k] = d[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    xl[k] = xr[k] = 0.f;
-                }
+            for (int u = 0; u < MX_U; ++u) {
+                const int jc = min(j + u, j1 - 1);
+                nx[u] = ld4(jc + 1);
+                const float* rc = q.psi + (size_t)jc * Nx;
+                el[u] = ldl ? __ldg(rc + cl) : 0.f;
+                er[u] = ldr ? __ldg(rc + cr) : 0.f;
+                db[u] = __ldg(&q.dpsibar[jc]);
+                an[u] = __ldg(&p.a_node[jc]);
             }
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                const int c = 4 * (q0 + k * (int)blockDim.x);
-                if (c >= Nx) continue;
-                const float e0 = (u[k].x - d[k].x) + db, e1 = (u[k].y - d[k].y) + db;
-                const float e2 = (u[k].z - d[k].z) + db, e3 = (u[k].w - d[k].w) + db;
-                const float f0 = a[k].y - xl[k], f1 = a[k].z - a[k].x, f2 = a[k].w - a[k].y, f3 = xr[k] - a[k].z;
-                dym = fmaxf(dym, fmaxf(fmaxf(fabsf(e0), fabsf(e1)), fmaxf(fabsf(e2), fabsf(e3))));
-                dxm = fmaxf(dxm, fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))));
+            for (int u = 0; u < MX_U; ++u) {
+                const float4 wc = (u == 0) ? w1 : nx[u - 1];
+                const float4 wm = (u == 0) ? w0 : (u == 1 ? w1 : nx[u - 2]);
+                const float sl = __shfl_up_sync(0xffffffffu, wc.w, 1);
+                const float sr = __shfl_down_sync(0xffffffffu, wc.x, 1);
+                const float xl = ldl ? el[u] : sl, xr = ldr ? er[u] : sr;
+                if (j + u >= j1 || !act) continue;
+                const float d = db[u];
+                const float e0 = (nx[u].x - wm.x) + d, e1 = (nx[u].y - wm.y) + d;
+                const float e2 = (nx[u].z - wm.z) + d, e3 = (nx[u].w - wm.w) + d;
+                const float f0 = wc.y - xl, f1 = wc.z - wc.x, f2 = wc.w - wc.y, f3 = xr - wc.z;
+                const float dym = fmaxf(fmaxf(fabsf(e0), fabsf(e1)), fmaxf(fabsf(e2), fabsf(e3)));
+                const float dxm = fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3)));
                 probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
+                const double a = an[u];
+                const double av = (double)dxm * cx;
+                um = fmax(um, a * ((double)dym * cy));
+                vm = fmax(vm, av);
+                vmm = fmax(vmm, av * a);
             }
+            w0 = nx[MX_U - 2]; w1 = nx[MX_U - 1];
         }
-        const double a = __ldg(&p.a_node[j]);
-        const double av = (double)dxm * cx;
-        um = fmax(um, a * ((double)dym * cy));
-        vm = fmax(vm, av);
-        vmm = fmax(vmm, av * a);
     }
     const int nonfinite = !(probe - probe == 0.f) || !(um <= 1e300) || !(vm <= 1e300);
     maxuv_finish(p, um, vm, vmm, nonfinite);

@@ -133,7 +133,7 @@ struct Context {
     size_t tc_smem = 0;
     CUtensorMap tm_hat{}, tm_cp{};
     int num_sms = 0;
-    int maxuv_grid = 0;            // one wave of k_maxuv_dt (occupancy x SMs, at most Ny - 2)
+    int maxuv_ctas = 0;            // resident CTAs of k_maxuv_dt (occupancy x SMs)
     // learned closure: the model evaluated before every stage and its output tau [Ny][Nx]
     struct Cnn* closure_net = nullptr;
     double* closure_tau = nullptr;       // tau, then the u, v scratch of the model's inputs
@@ -145,7 +145,7 @@ struct Context {
     float* rc32 = nullptr;                 // [RC32_N][Ny] row constants of the FP32 stage
     cpx<float> *twf = nullptr, *wNf = nullptr;
     double wall_bot32 = 0.0, wall_top32 = 0.0;
-    int maxuv32_grid = 0;
+    int maxuv32_ctas = 0;          // resident CTAs of k_maxuv32 (occupancy x SMs)
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false;
     int stage_tma_grid = 0;

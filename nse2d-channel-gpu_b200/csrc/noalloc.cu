@@ -16,6 +16,7 @@
 // Every call clears the control block (the last-CTA counter and the non-finite flag must
 // start at zero) with cudaMemsetAsync. One scratch array serves every caller on a device,
 // so calls that overlap in time on one device, from two streams or two host threads, race.
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -67,7 +68,7 @@ static int device_slot(DeviceSlot& out) {
         int sms = 0;
         NSE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         int per_sm = 0;
-        NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt, 256, 0));
+        NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt<false>, 256, 0));
         slot.num_sms = sms > 0 ? sms : 1;
         slot.per_sm = per_sm > 0 ? per_sm : 1;
         slot.scratch = static_cast<MaxUvScratch*>(ptr);
@@ -89,22 +90,31 @@ extern "C" int nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node,
         set_error("nse2d_max_uv_noalloc: grid %d x %d too small (need Nx >= 2, Ny >= 3)", Nx, Ny);
         return -1;
     }
+    if (reinterpret_cast<uintptr_t>(d_psi) % 8 != 0 || reinterpret_cast<uintptr_t>(d_a_node) % 8 != 0) {
+        set_error("nse2d_max_uv_noalloc: psi and a_node must be 8-byte aligned device pointers");
+        return -1;
+    }
     if (Nx > (1 << 30)) {
         set_error("nse2d_max_uv_noalloc: Nx = %d exceeds the maximum %d (32-bit column index)", Nx, 1 << 30);
         return -1;
     }
     DeviceSlot slot;
     if (device_slot(slot)) return -1;
-    // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, one partial slot each; the CTAs stride over
-    // the interior rows, so every Ny is covered by that fixed number of slots.
-    const int grid = std::max(1, std::min(std::min(slot.per_sm * slot.num_sms, Ny - 2), kMaxUvNoAllocBlocks));
     MaxUvScratch* sc = slot.scratch;
     NSE_CUDA_TRY(cudaMemsetAsync(&sc->ctl, 0, sizeof(Ctl), s));
     MaxParams p{};
     p.psi = d_psi; p.a_node = d_a_node; p.blocks = sc->blocks; p.ctl = &sc->ctl;
     p.Nx = Nx; p.Ny = Ny; p.adapt = 0; p.set_dt = 0;
     p.inv_dx = inv_dx; p.inv_deta = inv_deta;
-    k_maxuv_dt<<<grid, 256, 0, s>>>(p);
+    // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, one partial slot each; the CTAs stride over
+    // the (column strip, row band) items, so every grid is covered by that fixed number of slots.
+    int grid = 1;
+    maxuv_plan(p, slot.per_sm * slot.num_sms, kMaxUvNoAllocBlocks, grid);
+    // 16-byte loads only where every row and column pair is 16-byte aligned; a caller's psi may
+    // be any 8-byte-aligned pointer and Nx any size from 2
+    const bool vec = (Nx % 2 == 0) && (reinterpret_cast<uintptr_t>(d_psi) % 16 == 0);
+    if (vec) k_maxuv_dt<true><<<grid, 256, 0, s>>>(p);
+    else k_maxuv_dt<false><<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     NSE_CUDA_TRY(cudaMemcpyAsync(out3, &sc->ctl.umax, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     NSE_CUDA_TRY(cudaStreamSynchronize(s));

@@ -377,11 +377,11 @@ int context_create(const Config& cfg, Context** out) {
     }
     {
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt, 256, 0) != cudaSuccess || per_sm < 1) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv_dt<true>, 256, 0) != cudaSuccess || per_sm < 1) {
             set_error("k_maxuv_dt cannot be resident: %s", cudaGetErrorString(cudaGetLastError()));
             return fail();
         }
-        c->maxuv_grid = std::max(1, std::min(per_sm * c->num_sms, Ny - 2));
+        c->maxuv_ctas = per_sm * c->num_sms;
     }
     // stage kernel: persistent TMA variant when every tile row holds two or more tiles
     c->stage_tma = (c->Nx >= 2 * ST_TX);
@@ -636,7 +636,9 @@ int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
     p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
     p.dt_max = c->cfg.dt_max;
-    k_maxuv_dt<<<c->maxuv_grid, 256, 0, s>>>(p);        // partials fit red_blocks (>= 32 Ny)
+    int grid = 1;
+    maxuv_plan(p, c->maxuv_ctas, (int)(c->red_capacity / 3), grid);   // one partial triple per CTA
+    k_maxuv_dt<true><<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }

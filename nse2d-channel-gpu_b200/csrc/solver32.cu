@@ -45,7 +45,7 @@ int setup32(Context* c) {
     NSE_CUDA_TRY(cudaMemcpy(c->wNf, wN.data(), wN.size() * sizeof(wN[0]), cudaMemcpyHostToDevice));
     int per_sm = 0;
     NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv32, 256, 0));
-    c->maxuv32_grid = std::max(1, std::min(std::max(per_sm, 1) * c->num_sms, c->Ny - 2));
+    c->maxuv32_ctas = std::max(per_sm, 1) * c->num_sms;
     return 0;
 }
 
@@ -160,7 +160,9 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
         p.dt_max = c->cfg.dt_max;
         q.psi = c->psif;
         q.dpsibar = c->rc32 + (size_t)RC_DPB * c->Ny;
-        k_maxuv32<<<c->maxuv32_grid, 256, 0, s>>>(q);
+        int grid = 1;
+        maxuv_plan(p, c->maxuv32_ctas, (int)(c->red_capacity / 3), grid, MX32_COLS);
+        k_maxuv32<<<grid, 256, 0, s>>>(q);
         NSE_CUDA_TRY(cudaGetLastError());
         if (mark()) return -1;
     }

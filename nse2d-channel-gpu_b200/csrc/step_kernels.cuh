@@ -136,6 +136,29 @@ __device__ __forceinline__ StageTime stage_time(const StageParams& p) {
 // nu lap = nu/dx^2 (om_{i+1} + om_{i-1} - 2 om) + A+_j (om_{j+1} - om) - A-_j (om - om_{j-1}),
 // A+-_j = nu a_j a_{j+-1/2} / deta^2 from the row tables. The regrouping moves the result by a few
 // ulps of its terms; the stage parity bounds hold with margin.
+__device__ __forceinline__ double stage_rhs_interior(double rhs, double wc, double p_xm, double p_xp, double p_ym,
+                                                    double p_yp, double dyp_m, double dyp_c, double dyp_p,
+                                                    const double (&dxp)[3], double o_xm, double o_xp, double o_ym,
+                                                    double o_yp, double dyo_m, double dyo_c, double dyo_p,
+                                                    const double (&dxo)[3], double nu_dx2, double ap, double am,
+                                                    double cj) {
+    double s1 = dxp[1] * dyo_c;
+    s1 = fma(-dyp_c, dxo[1], s1);
+    s1 = fma(p_xp, dyo_p, s1);
+    s1 = fma(-p_xm, dyo_m, s1);
+    s1 = fma(-p_yp, dxo[2], s1);
+    s1 = fma(p_ym, dxo[0], s1);
+    double s2 = -o_xp * dyp_p;
+    s2 = fma(o_xm, dyp_m, s2);
+    s2 = fma(o_yp, dxp[2], s2);
+    s2 = fma(-o_ym, dxp[0], s2);
+    const double lapx = fma(-2.0, wc, o_xp + o_xm);
+    rhs = fma(nu_dx2, lapx, rhs);
+    rhs = fma(ap, o_yp - wc, rhs);
+    rhs = fma(-am, wc - o_ym, rhs);
+    return fma(cj, s1 + s2, rhs);                                                         // -J = c_j S
+}
+
 __device__ __forceinline__ void stage_tile(const StageParams& p, const StageTime& st, const double* sp,
                                            const double* so, int ld, int coff, int x0, int y0,
                                            const double* swn = nullptr) {
@@ -170,22 +193,10 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageTime
         if (j != 0 && j != Ny - 1) {
             const double dyo_m = om[2][0] - om[0][0], dyo_c = om[2][1] - om[0][1], dyo_p = om[2][2] - om[0][2];
             const double dyp_m = ps[2][0] - ps[0][0], dyp_c = ps[2][1] - ps[0][1], dyp_p = ps[2][2] - ps[0][2];
-            double s1 = dxp[1] * dyo_c;
-            s1 = fma(-dyp_c, dxo[1], s1);
-            s1 = fma(ps[1][2], dyo_p, s1);
-            s1 = fma(-ps[1][0], dyo_m, s1);
-            s1 = fma(-ps[2][1], dxo[2], s1);
-            s1 = fma(ps[0][1], dxo[0], s1);
-            double s2 = -om[1][2] * dyp_p;
-            s2 = fma(om[1][0], dyp_m, s2);
-            s2 = fma(om[2][1], dxp[2], s2);
-            s2 = fma(-om[0][1], dxp[0], s2);
-            const double lapx = fma(-2.0, wc, om[1][2] + om[1][0]);
             const double ap = __ldg(&p.rt.st_ap[j]), am = __ldg(&p.rt.st_am[j]), cj = __ldg(&p.rt.st_cj[j]);
-            rhs = fma(nu_dx2, lapx, rhs);
-            rhs = fma(ap, om[2][1] - wc, rhs);
-            rhs = fma(-am, wc - om[0][1], rhs);
-            rhs = fma(cj, s1 + s2, rhs);                                                  // -J = c_j S
+            rhs = stage_rhs_interior(rhs, wc, ps[1][0], ps[1][2], ps[0][1], ps[2][1], dyp_m, dyp_c, dyp_p, dxp,
+                                     om[1][0], om[1][2], om[0][1], om[2][1], dyo_m, dyo_c, dyo_p, dxo,
+                                     nu_dx2, ap, am, cj);
         }
         if (p.mms) rhs += mms_term(p, j, i, st.mA, st.mAp);
         const size_t id = (size_t)j * Nx + i;
@@ -292,6 +303,94 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
 }
 
+// The points of one tile from the TMA box (row stride SB_W; box column b holds x = x0 - 2 + b),
+// two adjacent columns per thread: warp g takes tile rows 4g .. 4g + 3, lane l the columns
+// x0 + 2l and x0 + 2l + 1. A row of the window (columns x - 1 .. x + 2) is three 16-byte shared
+// loads, the two points share their y differences, and the results leave as 16-byte stores.
+// The arithmetic of every point is stage_tile's (stage_rhs_interior), so both give the same bits.
+constexpr int ST2_RPT = 4;
+static_assert(8 * ST2_RPT == ST_TY && 64 == ST_TX, "pair layout: 8 warps x 4 rows, 32 lanes x 2 columns");
+
+__device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTime& st, const double* sp,
+                                            const double* so, const double* swn, int x0, int y0) {
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int lp = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int i0 = x0 + 2 * lp;
+    const int ly0 = g * ST2_RPT;                        // tile row ly <-> box row ly + 1
+    const double nu_dx2 = p.nu * p.inv_dx2;
+    double P[3][4], O[3][4];                            // rows j-1, j, j+1 x columns i0-1 .. i0+2
+    double dxpA[3], dxpB[3], dxoA[3], dxoB[3];          // x differences of the two points' rows
+    auto ld_row = [&](const double* f, int r, double (&v)[4]) {
+        const double2* q = reinterpret_cast<const double2*>(f + r * SB_W + 2 * lp);
+        const double2 a = q[0], b = q[1], c = q[2];
+        v[0] = a.y; v[1] = b.x; v[2] = b.y; v[3] = c.x;
+    };
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        ld_row(sp, ly0 + r, P[r + 1]);
+        ld_row(so, ly0 + r, O[r + 1]);
+        dxpA[r + 1] = P[r + 1][2] - P[r + 1][0]; dxpB[r + 1] = P[r + 1][3] - P[r + 1][1];
+        dxoA[r + 1] = O[r + 1][2] - O[r + 1][0]; dxoB[r + 1] = O[r + 1][3] - O[r + 1][1];
+    }
+#pragma unroll
+    for (int q = 0; q < ST2_RPT; ++q) {
+        const int ly = ly0 + q, j = y0 + ly;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            P[0][c] = P[1][c]; P[1][c] = P[2][c];
+            O[0][c] = O[1][c]; O[1][c] = O[2][c];
+        }
+        ld_row(sp, ly + 2, P[2]);
+        ld_row(so, ly + 2, O[2]);
+        dxpA[0] = dxpA[1]; dxpA[1] = dxpA[2]; dxpA[2] = P[2][2] - P[2][0];
+        dxpB[0] = dxpB[1]; dxpB[1] = dxpB[2]; dxpB[2] = P[2][3] - P[2][1];
+        dxoA[0] = dxoA[1]; dxoA[1] = dxoA[2]; dxoA[2] = O[2][2] - O[2][0];
+        dxoB[0] = dxoB[1]; dxoB[1] = dxoB[2]; dxoB[2] = O[2][3] - O[2][1];
+        if (j >= Ny) break;
+        const double wa = O[1][1], wb = O[1][2];
+        const double fj = __ldg(&p.rt.frow[j]);
+        double ra = fma(-p.lin_drag, wa, fj), rb = fma(-p.lin_drag, wb, fj);              // f - r omega
+        const bool interior = (j != 0 && j != Ny - 1);
+        if (interior) {
+            double dyo[4], dyp[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) { dyo[c] = O[2][c] - O[0][c]; dyp[c] = P[2][c] - P[0][c]; }
+            const double ap = __ldg(&p.rt.st_ap[j]), am = __ldg(&p.rt.st_am[j]), cj = __ldg(&p.rt.st_cj[j]);
+            ra = stage_rhs_interior(ra, wa, P[1][0], P[1][2], P[0][1], P[2][1], dyp[0], dyp[1], dyp[2], dxpA,
+                                    O[1][0], O[1][2], O[0][1], O[2][1], dyo[0], dyo[1], dyo[2], dxoA, nu_dx2, ap, am, cj);
+            rb = stage_rhs_interior(rb, wb, P[1][1], P[1][3], P[0][2], P[2][2], dyp[1], dyp[2], dyp[3], dxpB,
+                                    O[1][1], O[1][3], O[0][2], O[2][2], dyo[1], dyo[2], dyo[3], dxoB, nu_dx2, ap, am, cj);
+        }
+        if (p.mms) {
+            ra += mms_term(p, j, i0, st.mA, st.mAp);
+            rb += mms_term(p, j, i0 + 1, st.mA, st.mAp);
+        }
+        const size_t id = (size_t)j * Nx + i0;
+        if (p.closure && interior) {
+            const double2 tau = __ldg(reinterpret_cast<const double2*>(p.closure + id));
+            ra -= tau.x;
+            rb -= tau.y;
+        }
+        if (p.rhs_out) *reinterpret_cast<double2*>(p.rhs_out + id) = make_double2(ra, rb);
+        double na, nb;
+        const double dt = st.dt;
+        if (p.stage == 1) {
+            na = wa + dt * ra;                                                              // ops.cu:646
+            nb = wb + dt * rb;
+        } else {
+            const double2 wn = *reinterpret_cast<const double2*>(swn + ly * ST_TX + 2 * lp);
+            if (p.stage == 2) {
+                na = 0.75 * wn.x + 0.25 * (wa + dt * ra);                                   // ops.cu:650
+                nb = 0.75 * wn.y + 0.25 * (wb + dt * rb);
+            } else {
+                na = (1.0 / 3.0) * wn.x + (2.0 / 3.0) * (wa + dt * ra);                    // ops.cu:654
+                nb = (1.0 / 3.0) * wn.y + (2.0 / 3.0) * (wb + dt * rb);
+            }
+        }
+        *reinterpret_cast<double2*>(p.w_out + id) = make_double2(na, nb);
+    }
+}
+
 static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_constant__ StageMaps maps, StageParams p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -349,8 +448,7 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
             }
         }
         __syncthreads();
-        stage_tile(p, st, sp, so, SB_W, 1, x0, y0,
-                   reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD));
+        stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
         __syncthreads();
     }
@@ -1291,14 +1389,15 @@ static __global__ void __launch_bounds__(256) k_thom(ThomParams p) {
     }
 }
 
-// max |u|, |v|, |v| a over the interior (src/diag.cu:702-816), one row at a time per CTA,
-// and, in the last block, the adaptive time step with output trimming (src/main.cu:439-480).
+// max |u|, |v|, |v| a over the interior (src/diag.cu:702-816) and, in the last block, the
+// adaptive time step with output trimming (src/main.cu:439-480).
 struct MaxParams {
     const double* psi;
     const double* a_node;
     double* blocks;          // [gridDim.x][3]
     Ctl* ctl;
     int Nx, Ny, adapt, set_dt;
+    int nstrips, nbands, band_rows;   // work items of k_maxuv_dt (maxuv_plan)
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
@@ -1360,61 +1459,113 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
     ctl->dt = dt;
 }
 
-// max |u|, |v|, |v| a over the interior (src/diag.cu:702-866). One row per CTA at a time; a
-// thread takes 4 adjacent columns (16-byte loads of rows j-1, j, j+1). The maxima of
-// |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| over a row are scaled once per row: for
-// positive factors, rounding is monotone, so max_i |a (d_i c)| = a (max_i |d_i| c) exactly and the
-// result is the reference's per-point maximum to the bit. A running sum of the differences
-// turns NaN or Inf anywhere into a non-finite flag.
+// max |u|, |v|, |v| a over the interior (src/diag.cu:702-866).
+//
+// Work items are (column strip, row band) pairs: a strip is MX_COLS columns, 2 per thread, and a
+// band is p.band_rows consecutive interior rows; CTAs stride over the items. A thread walks down
+// its band with a window of rows j-1, j, j+1 in registers, so that every row of the band is
+// read from HBM once (plus one halo row at each end of the band), and MX_U rows are loaded at a
+// time to keep loads in flight. The x neighbours c-1 and c+2 come from the adjacent lanes by
+// warp shuffle; the lanes at the ends of a warp load them.
+//
+// The maxima of |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| of a thread's points in
+// row j are scaled once per row: for positive factors, rounding is monotone, so
+// max_i |a (d_i c)| = a (max_i |d_i| c) exactly and the result is the reference's per-point
+// maximum to the bit. A running sum of the differences turns NaN or Inf anywhere into a
+// non-finite flag.
+//
+// VEC: 16-byte loads of a thread's two columns (Nx even and psi 16-byte aligned); otherwise
+// every value is an 8-byte load and any Nx >= 2 works.
+constexpr int MX_COLS = 512, MX_U = 4;
+
+__host__ __device__ inline int mx_wrap(int i, int Nx) { return i < 0 ? i + Nx : (i >= Nx ? i - Nx : i); }
+
+template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
+    const int lane = threadIdx.x & 31;
     double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;
     const double cy = 0.5 * p.inv_deta, cx = 0.5 * p.inv_dx;
-    for (int j = 1 + blockIdx.x; j < Ny - 1; j += gridDim.x) {
-        const double* rm = p.psi + (size_t)(j - 1) * Nx;
-        const double* r0 = p.psi + (size_t)j * Nx;
-        const double* rp = p.psi + (size_t)(j + 1) * Nx;
-        double dym = 0.0, dxm = 0.0;
-        constexpr int U = 2;                           // column quads per thread and iteration
-        for (int q0 = threadIdx.x; 4 * q0 < Nx; q0 += U * blockDim.x) {
-            double2 a0[U], a1[U], u0[U], u1[U], d0[U], d1[U];
-            double xl[U], xr[U];
+    const int nitems = p.nstrips * p.nbands;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int strip = item % p.nstrips, band = item / p.nstrips;
+        const int c0 = strip * MX_COLS + 2 * (int)threadIdx.x;
+        const bool act = c0 < Nx, two = c0 + 1 < Nx;
+        const int cs = act ? c0 : 0;                     // an in-bounds column for idle lanes
+        const int cl = mx_wrap(cs - 1, Nx), cr1 = mx_wrap(cs + 1, Nx), cr2 = mx_wrap(cs + 2, Nx);
+        const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
+        // lanes that take a neighbour from memory: the first lane of a warp (column c-1), and
+        // the last active lane (column c+2, whose owner is in another warp or wraps around)
+        const bool ldl = act && lane == 0, ldr = act && (lane == 31 || c0 + 2 >= Nx);
+        auto ld2 = [&](int row) -> double2 {
+            const double* r = p.psi + (size_t)row * Nx;
+            if constexpr (VEC) return __ldg(reinterpret_cast<const double2*>(r + cs));
+            else return make_double2(__ldg(r + cs), __ldg(r + cr1));
+        };
+        double2 w0 = ld2(j0 - 1), w1 = ld2(j0);         // rows j-1 and j
+        for (int j = j0; j < j1; j += MX_U) {
+            double2 nx[MX_U];
+            double el[MX_U], er[MX_U];
+            double an[MX_U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = 4 * (q0 + u * (int)blockDim.x);
-                if (c < Nx) {
-                    a0[u] = __ldg(reinterpret_cast<const double2*>(r0 + c));
-                    a1[u] = __ldg(reinterpret_cast<const double2*>(r0 + c + 2));
-                    u0[u] = __ldg(reinterpret_cast<const double2*>(rp + c));
-                    u1[u] = __ldg(reinterpret_cast<const double2*>(rp + c + 2));
-                    d0[u] = __ldg(reinterpret_cast<const double2*>(rm + c));
-                    d1[u] = __ldg(reinterpret_cast<const double2*>(rm + c + 2));
-                    xl[u] = __ldg(r0 + (c > 0 ? c - 1 : Nx - 1));
-                    xr[u] = __ldg(r0 + (c + 4 < Nx ? c + 4 : 0));
-                } else {
-                    a0[u] = a1[u] = u0[u] = u1[u] = d0[u] = d1[u] = make_double2(0.0, 0.0);
-                    xl[u] = xr[u] = 0.0;
+            for (int u = 0; u < MX_U; ++u) {
+                const int jc = min(j + u, j1 - 1);       // centre row (clamped: rows past the band are not used)
+                nx[u] = ld2(jc + 1);
+                const double* rc = p.psi + (size_t)jc * Nx;
+                el[u] = 0.0; er[u] = 0.0;
+                if (!VEC || ldl) el[u] = __ldg(rc + cl);
+                if (!VEC || ldr) er[u] = __ldg(rc + cr2);
+                an[u] = __ldg(&p.a_node[jc]);
+            }
+#pragma unroll
+            for (int u = 0; u < MX_U; ++u) {
+                const double2 wc = (u == 0) ? w1 : nx[u - 1];
+                const double2 wm = (u == 0) ? w0 : (u == 1 ? w1 : nx[u - 2]);
+                double xl = el[u], xr = er[u];
+                if constexpr (VEC) {
+                    const double sl = __shfl_up_sync(0xffffffffu, wc.y, 1);
+                    const double sr = __shfl_down_sync(0xffffffffu, wc.x, 1);
+                    if (!ldl) xl = sl;
+                    if (!ldr) xr = sr;
                 }
+                if (j + u >= j1 || !act) continue;
+                // column c0: psi_{c0+1} - psi_{c0-1}; column c0+1: psi_{c0+2} - psi_{c0}
+                const double e0 = nx[u].x - wm.x, f0 = wc.y - xl;
+                double dym = fabs(e0), dxm = fabs(f0), sum = e0 + f0;
+                if (two) {
+                    const double e1 = nx[u].y - wm.y, f1 = xr - wc.x;
+                    dym = fmax(dym, fabs(e1));
+                    dxm = fmax(dxm, fabs(f1));
+                    sum += e1 + f1;
+                }
+                probe += sum;
+                const double a = an[u];
+                const double av = dxm * cx;
+                um = fmax(um, a * (dym * cy));
+                vm = fmax(vm, av);
+                vmm = fmax(vmm, av * a);
             }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const double e0 = u0[u].x - d0[u].x, e1 = u0[u].y - d0[u].y;
-                const double e2 = u1[u].x - d1[u].x, e3 = u1[u].y - d1[u].y;
-                const double f0 = a0[u].y - xl[u], f1 = a1[u].x - a0[u].x;
-                const double f2 = a1[u].y - a0[u].y, f3 = xr[u] - a1[u].x;
-                dym = fmax(dym, fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))));
-                dxm = fmax(dxm, fmax(fmax(fabs(f0), fabs(f1)), fmax(fabs(f2), fabs(f3))));
-                probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
-            }
+            if constexpr (MX_U == 1) { w0 = w1; w1 = nx[0]; }
+            else { w0 = nx[MX_U - 2]; w1 = nx[MX_U - 1]; }
         }
-        const double a = __ldg(&p.a_node[j]);
-        const double av = dxm * cx;
-        um = fmax(um, a * (dym * cy));
-        vm = fmax(vm, av);
-        vmm = fmax(vmm, av * a);
     }
     const int nonfinite = !(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300);
     maxuv_finish(p, um, vm, vmm, nonfinite);
+}
+
+// Strips of `cols` columns, bands and grid of the max reduction for a target of `ctas`
+// resident CTAs, at most `max_grid` CTAs (the partial slots); the CTAs stride over the items.
+inline void maxuv_plan(MaxParams& p, int ctas, int max_grid, int& grid, int cols = MX_COLS) {
+    const int Ni = p.Ny - 2;
+    p.nstrips = (p.Nx + cols - 1) / cols;
+    int nb = ctas / p.nstrips;                       // at most one item per resident CTA
+    nb = nb < 1 ? 1 : (nb > Ni ? Ni : nb);
+    p.band_rows = (Ni + nb - 1) / nb;
+    p.nbands = (Ni + p.band_rows - 1) / p.band_rows;
+    const long long items = (long long)p.nstrips * p.nbands;
+    long long g = items < ctas ? items : ctas;
+    if (g > max_grid) g = max_grid;
+    grid = g < 1 ? 1 : (int)g;
 }
 
 }  // namespace nse2d
