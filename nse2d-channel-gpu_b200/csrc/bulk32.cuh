@@ -122,6 +122,53 @@ struct Stage32Params {
     float nu_dx2, lin_drag;
 };
 
+// The row constants of an interior row j that the stage reads.
+struct Rc32Row {
+    float dpb, dpp, dpm, dwb, dwp, dwm, ap, am, cj;
+};
+__device__ __forceinline__ Rc32Row rc32_row(const float* rc, int Ny, int j) {
+    Rc32Row k;
+    k.dpb = __ldg(&rc[(size_t)RC_DPB * Ny + j]); k.dpp = __ldg(&rc[(size_t)RC_DPP * Ny + j]);
+    k.dpm = __ldg(&rc[(size_t)RC_DPM * Ny + j]); k.dwb = __ldg(&rc[(size_t)RC_DWB * Ny + j]);
+    k.dwp = __ldg(&rc[(size_t)RC_DWP * Ny + j]); k.dwm = __ldg(&rc[(size_t)RC_DWM * Ny + j]);
+    k.ap = __ldg(&rc[(size_t)RC_AP * Ny + j]); k.am = __ldg(&rc[(size_t)RC_AM * Ny + j]);
+    k.cj = __ldg(&rc[(size_t)RC_CJ * Ny + j]);
+    return k;
+}
+
+// rhs of one interior point from its 3 x 3 neighbourhood: S'(psi', w') + the base profiles'
+// share of S, the mapped Laplacian and the forcing row constant (already in rhs). p_xm, p_xp,
+// p_ym, p_yp are psi' at x-1, x+1, y-1, y+1 (likewise o_ for w'); dxp/dxo[r] the x differences
+// of rows j-1, j, j+1. Both FP32 stage kernels call it, so they give the same bits.
+__device__ __forceinline__ float stage32_rhs_interior(float rhs, float wc, float p_xm, float p_xp, float p_ym,
+                                                      float p_yp, float dyp_m, float dyp_c, float dyp_p,
+                                                      const float (&dxp)[3], float o_xm, float o_xp, float o_ym,
+                                                      float o_yp, float dyo_m, float dyo_c, float dyo_p,
+                                                      const float (&dxo)[3], float nu_dx2, const Rc32Row& k) {
+    float s1 = dxp[1] * dyo_c;
+    s1 = fmaf(-dyp_c, dxo[1], s1);
+    s1 = fmaf(p_xp, dyo_p, s1);
+    s1 = fmaf(-p_xm, dyo_m, s1);
+    s1 = fmaf(-p_yp, dxo[2], s1);
+    s1 = fmaf(p_ym, dxo[0], s1);
+    float s2 = -o_xp * dyp_p;
+    s2 = fmaf(o_xm, dyp_m, s2);
+    s2 = fmaf(o_yp, dxp[2], s2);
+    s2 = fmaf(-o_ym, dxp[0], s2);
+    // the base profiles' share of S
+    float s3 = -2.f * k.dpb * dxo[1];
+    s3 = fmaf(-k.dpp, dxo[2], s3);
+    s3 = fmaf(-k.dpm, dxo[0], s3);
+    s3 = fmaf(2.f * k.dwb, dxp[1], s3);
+    s3 = fmaf(k.dwp, dxp[2], s3);
+    s3 = fmaf(k.dwm, dxp[0], s3);
+    const float lapx = fmaf(-2.f, wc, o_xp + o_xm);
+    rhs = fmaf(nu_dx2, lapx, rhs);
+    rhs = fmaf(k.ap, o_yp - wc, rhs);
+    rhs = fmaf(-k.am, wc - o_ym, rhs);
+    return fmaf(k.cj, (s1 + s2) + s3, rhs);
+}
+
 static __global__ void __launch_bounds__(256) k_stage32(Stage32Params p) {
     __shared__ float sp[ST_H][ST_W + 1];
     __shared__ float so[ST_H][ST_W + 1];
@@ -187,33 +234,9 @@ static __global__ void __launch_bounds__(256) k_stage32(Stage32Params p) {
         if (j != 0 && j != Ny - 1) {
             const float dyo_m = om[2][0] - om[0][0], dyo_c = om[2][1] - om[0][1], dyo_p = om[2][2] - om[0][2];
             const float dyp_m = ps[2][0] - ps[0][0], dyp_c = ps[2][1] - ps[0][1], dyp_p = ps[2][2] - ps[0][2];
-            float s1 = dxp[1] * dyo_c;
-            s1 = fmaf(-dyp_c, dxo[1], s1);
-            s1 = fmaf(ps[1][2], dyo_p, s1);
-            s1 = fmaf(-ps[1][0], dyo_m, s1);
-            s1 = fmaf(-ps[2][1], dxo[2], s1);
-            s1 = fmaf(ps[0][1], dxo[0], s1);
-            float s2 = -om[1][2] * dyp_p;
-            s2 = fmaf(om[1][0], dyp_m, s2);
-            s2 = fmaf(om[2][1], dxp[2], s2);
-            s2 = fmaf(-om[0][1], dxp[0], s2);
-            // the base profiles' share of S
-            const float dpb = __ldg(&rc[(size_t)RC_DPB * Ny + j]), dpp = __ldg(&rc[(size_t)RC_DPP * Ny + j]);
-            const float dpm = __ldg(&rc[(size_t)RC_DPM * Ny + j]), dwb = __ldg(&rc[(size_t)RC_DWB * Ny + j]);
-            const float dwp = __ldg(&rc[(size_t)RC_DWP * Ny + j]), dwm = __ldg(&rc[(size_t)RC_DWM * Ny + j]);
-            float s3 = -2.f * dpb * dxo[1];
-            s3 = fmaf(-dpp, dxo[2], s3);
-            s3 = fmaf(-dpm, dxo[0], s3);
-            s3 = fmaf(2.f * dwb, dxp[1], s3);
-            s3 = fmaf(dwp, dxp[2], s3);
-            s3 = fmaf(dwm, dxp[0], s3);
-            const float lapx = fmaf(-2.f, wc, om[1][2] + om[1][0]);
-            const float ap = __ldg(&rc[(size_t)RC_AP * Ny + j]), am = __ldg(&rc[(size_t)RC_AM * Ny + j]);
-            const float cj = __ldg(&rc[(size_t)RC_CJ * Ny + j]);
-            rhs = fmaf(p.nu_dx2, lapx, rhs);
-            rhs = fmaf(ap, om[2][1] - wc, rhs);
-            rhs = fmaf(-am, wc - om[0][1], rhs);
-            rhs = fmaf(cj, (s1 + s2) + s3, rhs);
+            const Rc32Row k = rc32_row(rc, Ny, j);
+            rhs = stage32_rhs_interior(rhs, wc, ps[1][0], ps[1][2], ps[0][1], ps[2][1], dyp_m, dyp_c, dyp_p, dxp,
+                                       om[1][0], om[1][2], om[0][1], om[2][1], dyo_m, dyo_c, dyo_p, dxo, p.nu_dx2, k);
         }
         const size_t id = (size_t)j * Nx + i;
         if (p.rhs_out) p.rhs_out[id] = rhs;
@@ -222,6 +245,161 @@ static __global__ void __launch_bounds__(256) k_stage32(Stage32Params p) {
         else if (p.stage == 2) wnew = 0.75f * p.w_n[id] + 0.25f * fmaf(dt, rhs, wc);
         else wnew = (1.0f / 3.0f) * p.w_n[id] + (2.0f / 3.0f) * fmaf(dt, rhs, wc);
         p.w_out[id] = wnew;
+    }
+}
+
+// ---- k_stage32_tma: persistent CTAs, halos moved by the tensor memory accelerator ----
+// The scheme of the FP64 k_stage_tma with FP32 boxes: tiles of S32_TX x S32_TY points, the halo
+// boxes of psi' and w'^(s) (S32_W x S32_H, starting at column x0 - 4 so that x is a multiple of
+// 16 bytes) and the w'^n tile box of the next tile in flight while the current one is
+// computed; the periodic columns -1 and Nx of the first and last tile column are patched with
+// plain loads. Warp g takes tile rows 4g .. 4g + 3, lane l the columns x0 + 4l .. x0 + 4l + 3: a
+// row of the window (columns x - 1 .. x + 4) is three 16-byte shared loads, the four points
+// share their y differences, and the results leave as 16-byte stores. A wait that does not
+// complete within kTmaWaitLimit polls sets bit 1 of the error flags and ends the CTA.
+constexpr int S32_TX = 128, S32_TY = 32, S32_W = S32_TX + 8, S32_H = S32_TY + 2, S32_RPT = 4;
+constexpr int S32_FIELD = ((S32_H * S32_W * 4 + 127) / 128) * 128;
+constexpr int S32_WN = S32_TX * S32_TY * 4;
+constexpr int S32_BUF = 2 * S32_FIELD + S32_WN;
+constexpr unsigned S32_TX_BYTES = 2u * S32_H * S32_W * 4;
+static_assert(8 * S32_RPT == S32_TY && 32 * 4 == S32_TX, "4 columns x 32 lanes, 4 rows x 8 warps");
+__host__ __device__ constexpr size_t stage32_tma_smem_bytes() { return 2 * (size_t)S32_BUF + 128; }
+
+struct Stage32Maps {
+    CUtensorMap psi, w;      // halo boxes (S32_W x S32_H)
+    CUtensorMap wn;          // w'^n tile box (S32_TX x S32_TY), stages 2 and 3
+};
+
+__device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, const float* sp, const float* so,
+                                              const float* swn, int x0, int y0) {
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int l = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int ly0 = g * S32_RPT;                        // tile row ly <-> box row ly + 1
+    float P[3][6], O[3][6];                             // rows j-1, j, j+1 x columns x0+4l-1 .. x0+4l+4
+    float dxp[4][3], dxo[4][3];                         // per point, rows j-1, j, j+1
+    auto ld_row = [&](const float* f, int r, float (&v)[6]) {
+        const float4* q = reinterpret_cast<const float4*>(f + r * S32_W + 4 * l);
+        const float4 a = q[0], b = q[1], c = q[2];
+        v[0] = a.w; v[1] = b.x; v[2] = b.y; v[3] = b.z; v[4] = b.w; v[5] = c.x;
+    };
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        ld_row(sp, ly0 + r, P[r + 1]);
+        ld_row(so, ly0 + r, O[r + 1]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            dxp[k][r + 1] = P[r + 1][k + 2] - P[r + 1][k];
+            dxo[k][r + 1] = O[r + 1][k + 2] - O[r + 1][k];
+        }
+    }
+    const float* rc = p.rc;
+#pragma unroll
+    for (int q = 0; q < S32_RPT; ++q) {
+        const int ly = ly0 + q, j = y0 + ly;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            P[0][c] = P[1][c]; P[1][c] = P[2][c];
+            O[0][c] = O[1][c]; O[1][c] = O[2][c];
+        }
+        ld_row(sp, ly + 2, P[2]);
+        ld_row(so, ly + 2, O[2]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            dxp[k][0] = dxp[k][1]; dxp[k][1] = dxp[k][2]; dxp[k][2] = P[2][k + 2] - P[2][k];
+            dxo[k][0] = dxo[k][1]; dxo[k][1] = dxo[k][2]; dxo[k][2] = O[2][k + 2] - O[2][k];
+        }
+        if (j >= Ny) break;
+        const float fr = __ldg(&rc[(size_t)RC_R * Ny + j]);
+        float rhs[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rhs[k] = fmaf(-p.lin_drag, O[1][k + 1], fr);
+        if (j != 0 && j != Ny - 1) {
+            float dyo[6], dyp[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) { dyo[c] = O[2][c] - O[0][c]; dyp[c] = P[2][c] - P[0][c]; }
+            const Rc32Row kr = rc32_row(rc, Ny, j);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                rhs[k] = stage32_rhs_interior(rhs[k], O[1][k + 1], P[1][k], P[1][k + 2], P[0][k + 1], P[2][k + 1],
+                                              dyp[k], dyp[k + 1], dyp[k + 2], dxp[k], O[1][k], O[1][k + 2],
+                                              O[0][k + 1], O[2][k + 1], dyo[k], dyo[k + 1], dyo[k + 2], dxo[k],
+                                              p.nu_dx2, kr);
+        }
+        const size_t id = (size_t)j * Nx + x0 + 4 * l;
+        if (p.rhs_out) *reinterpret_cast<float4*>(p.rhs_out + id) = make_float4(rhs[0], rhs[1], rhs[2], rhs[3]);
+        float wn[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) wn[k] = fmaf(dt, rhs[k], O[1][k + 1]);
+        if (p.stage > 1) {
+            const float4 n4 = *reinterpret_cast<const float4*>(swn + ly * S32_TX + 4 * l);
+            const float nn[4] = {n4.x, n4.y, n4.z, n4.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                wn[k] = (p.stage == 2) ? 0.75f * nn[k] + 0.25f * wn[k] : (1.0f / 3.0f) * nn[k] + (2.0f / 3.0f) * wn[k];
+        }
+        *reinterpret_cast<float4*>(p.w_out + id) = make_float4(wn[0], wn[1], wn[2], wn[3]);
+    }
+}
+
+static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_constant__ Stage32Maps maps, Stage32Params p) {
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    __shared__ __align__(8) uint64_t bars[2];
+    unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int tiles_x = Nx / S32_TX, ntiles = tiles_x * ((Ny + S32_TY - 1) / S32_TY);
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    auto issue = [&](int tile, int b) {
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        unsigned char* dst = smem_raw + b * S32_BUF;
+        mbar_expect_tx(&bars[b], S32_TX_BYTES + (p.stage > 1 ? (unsigned)S32_WN : 0u));
+        tma_load_2d(dst, &maps.psi, tx * S32_TX - 4, ty * S32_TY - 1, &bars[b]);
+        tma_load_2d(dst + S32_FIELD, &maps.w, tx * S32_TX - 4, ty * S32_TY - 1, &bars[b]);
+        if (p.stage > 1) tma_load_2d(dst + 2 * S32_FIELD, &maps.wn, tx * S32_TX, ty * S32_TY, &bars[b]);
+    };
+    const float dt = (float)p.ctl->dt;
+    int k = 0;
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+        const int b = k & 1;
+        const int next = tile + gridDim.x;
+        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
+        const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
+        if (!ok) {
+            if (threadIdx.x == 0) {
+                atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
+                if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+            }
+            return;
+        }
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        const int x0 = tx * S32_TX, y0 = ty * S32_TY;
+        float* sp = reinterpret_cast<float*>(smem_raw + b * S32_BUF);
+        float* so = reinterpret_cast<float*>(smem_raw + b * S32_BUF + S32_FIELD);
+        if (tx == 0 || tx == tiles_x - 1) {
+            // periodic halo columns: box column 3 is x = -1, box column S32_TX + 4 is x = Nx
+            for (int r = threadIdx.x; r < S32_H; r += blockDim.x) {
+                const int gy = y0 - 1 + r;
+                if (gy < 0 || gy >= Ny) continue;
+                if (tx == 0) {
+                    sp[r * S32_W + 3] = __ldg(&p.psi[(size_t)gy * Nx + Nx - 1]);
+                    so[r * S32_W + 3] = __ldg(&p.w_in[(size_t)gy * Nx + Nx - 1]);
+                }
+                if (tx == tiles_x - 1) {
+                    sp[r * S32_W + S32_TX + 4] = __ldg(&p.psi[(size_t)gy * Nx]);
+                    so[r * S32_W + S32_TX + 4] = __ldg(&p.w_in[(size_t)gy * Nx]);
+                }
+            }
+        }
+        __syncthreads();
+        stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0);
+        fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
+        __syncthreads();
     }
 }
 
@@ -263,7 +441,7 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
         dftR<float, R0, false>(v);
         const int p0 = dit16_pos<M>(t);
 #pragma unroll
-        for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+        for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
     }
     __syncthreads();
     p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
@@ -271,8 +449,8 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
     double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
     for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
         const int kb = (k == 0 ? 0 : M - k);
-        const cpx<float> a = buf[ip_idx(k)];
-        const cpx<float> b = buf[ip_idx(kb)];
+        const cpx<float> a = buf[ip_idx<M>(k)];
+        const cpx<float> b = buf[ip_idx<M>(kb)];
         const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
         const cpx<float> df = {0.5f * (a.x - b.x), 0.5f * (a.y + b.y)};
         const cpx<float> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
@@ -319,12 +497,12 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
             dftR<float, R0, true>(v);
             const int p0 = dit16_pos<M>(t);
 #pragma unroll
-            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+            for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
         __syncthreads();
         p16_passes_from<float, M, 1, true, IP_NT>(buf, p.tw);
         for (int n = threadIdx.x; n < M; n += IP_NT) {
-            const cpx<float> z = buf[ip_idx(n)];
+            const cpx<float> z = buf[ip_idx<M>(n)];
             reinterpret_cast<float2*>(dst)[n] = make_float2(z.x * scale, z.y * scale);
         }
         __syncthreads();
@@ -363,71 +541,64 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
 }
 
 // ---- max |u|, |v|, |v| a of psibar + psi' ----
-// The item layout of k_maxuv_dt: (column strip, row band) items, a window of rows j-1, j, j+1
-// in registers down the band, MX_U rows loaded at a time; here a thread holds 4 columns (one
-// 16-byte load per row; Nx is a power of two >= 4), so a strip is MX32_COLS columns, and the x
-// neighbours c-1 and c+4 come from the adjacent lanes.
+// The item layout of k_maxuv_dt with 4 columns per lane (one 16-byte load per row; Nx is a
+// power of two >= 4): lanes 1..30 own a warp's 120 columns, lanes 0 and 31 hold their outer
+// neighbours, and the next MX_U rows are in flight while the current ones are reduced.
 struct Max32Params {
     MaxParams base;          // a_node, partials, control block, dt constants, items (base.psi unused)
     const float* psi;        // psi'
     const float* dpsibar;    // [Ny]: psibar_{j+1} - psibar_{j-1} (the RC_DPB row constant)
 };
-constexpr int MX32_COLS = 1024;
+constexpr int MX32_WCOLS = 120, MX32_COLS = 8 * MX32_WCOLS;
 
 static __global__ void __launch_bounds__(256, 3) k_maxuv32(Max32Params q) {
     const MaxParams& p = q.base;
     const int Nx = p.Nx, Ny = p.Ny;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double um = 0.0, vm = 0.0, vmm = 0.0;
     float probe = 0.f;
     const double cy = 0.5 * p.inv_deta, cx = 0.5 * p.inv_dx;
     const int nitems = p.nstrips * p.nbands;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int strip = item % p.nstrips, band = item / p.nstrips;
-        const int c0 = strip * MX32_COLS + 4 * (int)threadIdx.x;
-        const bool act = c0 < Nx;
-        const int cs = act ? c0 : 0;
-        const int cl = cs > 0 ? cs - 1 : Nx - 1, cr = cs + 4 < Nx ? cs + 4 : 0;
+        const int c = strip * MX32_COLS + warp * MX32_WCOLS + 4 * (lane - 1);
+        const bool own = lane >= 1 && lane <= 30 && c < Nx;
+        const int ca = ((c % Nx) + Nx) % Nx;
         const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
-        const bool ldl = act && lane == 0, ldr = act && (lane == 31 || c0 + 4 >= Nx);
-        auto ld4 = [&](int row) { return __ldg(reinterpret_cast<const float4*>(q.psi + (size_t)row * Nx + cs)); };
+        auto ld4 = [&](int row) { return __ldg(reinterpret_cast<const float4*>(q.psi + (size_t)row * Nx + ca)); };
         float4 w0 = ld4(j0 - 1), w1 = ld4(j0);
+        float4 nx[MX_U];
+        auto load_batch = [&](int jb) {
+#pragma unroll
+            for (int u = 0; u < MX_U; ++u) nx[u] = ld4(min(jb + u, j1 - 1) + 1);
+        };
+        load_batch(j0);
         for (int j = j0; j < j1; j += MX_U) {
-            float4 nx[MX_U];
-            float el[MX_U], er[MX_U], db[MX_U];
-            double an[MX_U];
+            float4 cur[MX_U];
+#pragma unroll
+            for (int u = 0; u < MX_U; ++u) cur[u] = nx[u];
+            if (j + MX_U < j1) load_batch(j + MX_U);
 #pragma unroll
             for (int u = 0; u < MX_U; ++u) {
-                const int jc = min(j + u, j1 - 1);
-                nx[u] = ld4(jc + 1);
-                const float* rc = q.psi + (size_t)jc * Nx;
-                el[u] = ldl ? __ldg(rc + cl) : 0.f;
-                er[u] = ldr ? __ldg(rc + cr) : 0.f;
-                db[u] = __ldg(&q.dpsibar[jc]);
-                an[u] = __ldg(&p.a_node[jc]);
-            }
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) {
-                const float4 wc = (u == 0) ? w1 : nx[u - 1];
-                const float4 wm = (u == 0) ? w0 : (u == 1 ? w1 : nx[u - 2]);
-                const float sl = __shfl_up_sync(0xffffffffu, wc.w, 1);
-                const float sr = __shfl_down_sync(0xffffffffu, wc.x, 1);
-                const float xl = ldl ? el[u] : sl, xr = ldr ? er[u] : sr;
-                if (j + u >= j1 || !act) continue;
-                const float d = db[u];
-                const float e0 = (nx[u].x - wm.x) + d, e1 = (nx[u].y - wm.y) + d;
-                const float e2 = (nx[u].z - wm.z) + d, e3 = (nx[u].w - wm.w) + d;
+                const float4 wc = (u == 0) ? w1 : cur[u - 1];
+                const float4 wm = (u == 0) ? w0 : (u == 1 ? w1 : cur[u - 2]);
+                const float xl = __shfl_up_sync(0xffffffffu, wc.w, 1);
+                const float xr = __shfl_down_sync(0xffffffffu, wc.x, 1);
+                if (j + u >= j1 || !own) continue;
+                const float d = __ldg(&q.dpsibar[j + u]);
+                const float e0 = (cur[u].x - wm.x) + d, e1 = (cur[u].y - wm.y) + d;
+                const float e2 = (cur[u].z - wm.z) + d, e3 = (cur[u].w - wm.w) + d;
                 const float f0 = wc.y - xl, f1 = wc.z - wc.x, f2 = wc.w - wc.y, f3 = xr - wc.z;
                 const float dym = fmaxf(fmaxf(fabsf(e0), fabsf(e1)), fmaxf(fabsf(e2), fabsf(e3)));
                 const float dxm = fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3)));
                 probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
-                const double a = an[u];
+                const double a = __ldg(&p.a_node[j + u]);
                 const double av = (double)dxm * cx;
                 um = fmax(um, a * ((double)dym * cy));
                 vm = fmax(vm, av);
                 vmm = fmax(vmm, av * a);
             }
-            w0 = nx[MX_U - 2]; w1 = nx[MX_U - 1];
+            w0 = cur[MX_U - 2]; w1 = cur[MX_U - 1];
         }
     }
     const int nonfinite = !(probe - probe == 0.f) || !(um <= 1e300) || !(vm <= 1e300);

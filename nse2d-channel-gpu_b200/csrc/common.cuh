@@ -146,6 +146,10 @@ struct Context {
     cpx<float> *twf = nullptr, *wNf = nullptr;
     double wall_bot32 = 0.0, wall_top32 = 0.0;
     int maxuv32_ctas = 0;          // resident CTAs of k_maxuv32 (occupancy x SMs)
+    // FP32 stage kernel: TMA tensor maps of psi' and of the three w' buffers (Nx >= 256)
+    bool stage32_tma = false;
+    int stage32_tma_grid = 0;
+    CUtensorMap tm32_psi{}, tm32_w[3]{}, tm32_wn{};
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false;
     int stage_tma_grid = 0;

@@ -21,10 +21,21 @@ __device__ __forceinline__ cpx<float> ldtw(const cpx<float>* tw, int i) {
     return {v.x, v.y};
 }
 
-// Shared-memory layout of a row: ip_idx(i) = i + i/8 + i/512 (in elements) spreads the strided
-// accesses of the passes and the digit-reversed writes of the first pass over the banks.
-__host__ __device__ __forceinline__ int ip_idx(int i) { return i + (i >> 3) + (i >> 9); }
-__host__ __device__ constexpr int ip_size(int M) { return M + (M >> 3) + (M >> 9) + 1; }
+// Shared-memory layout of a row of M points: ip_idx<M>(i) = i + (i >> A) + (i >> B) (in elements)
+// spreads the digit-reversed writes of the first pass, the strided accesses of the later passes
+// and the split step's descending reads over the banks. A and B are chosen per M by counting
+// the shared-memory wavefronts of all of these accesses, for 16-byte (FP64) and 8-byte (FP32)
+// elements; at M = 2048 every access is conflict-free (one pad element per 256).
+__host__ __device__ constexpr int ip_shift_a(int M) { return M >= 8192 ? 7 : (M >= 2048 ? 8 : 4); }
+__host__ __device__ constexpr int ip_shift_b(int M) {
+    return M == 64 ? 6 : M == 128 ? 7 : M == 256 ? 8 : M == 512 ? 6 : M == 1024 ? 7 : M == 2048 ? 11 : M >= 4096 ? 12 : 30;
+}
+template <int M> __host__ __device__ __forceinline__ int ip_idx(int i) {
+    return i + (i >> ip_shift_a(M)) + (i >> ip_shift_b(M));
+}
+__host__ __device__ constexpr int ip_size(int M) {
+    return M + ((M - 1) >> ip_shift_a(M)) + ((M - 1) >> ip_shift_b(M));
+}
 
 // ---------------------------------------------------------------------------------------
 // Radix-16 plan of the row transforms (FP64 and FP32): in-place decimation-in-time passes of
@@ -95,7 +106,7 @@ __device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>*
         const int base = (b - mm) * R + mm;
         cpx<T> v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = buf[ip_idx(base + r * LP)];
+        for (int r = 0; r < R; ++r) v[r] = buf[ip_idx<M>(base + r * LP)];
         if (mm > 0) {
             const int t = OFF + 4 * mm;
             const cpx<T> w1 = ldtw(tw, t);
@@ -125,7 +136,7 @@ __device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>*
         }
         dftR<T, R, INV>(v);
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[ip_idx(base + r * LP)] = v[r];
+        for (int r = 0; r < R; ++r) buf[ip_idx<M>(base + r * LP)] = v[r];
     }
 }
 

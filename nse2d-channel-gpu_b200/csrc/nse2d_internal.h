@@ -23,6 +23,8 @@ const char* thomas_kernel_name(const Context* c, int i);
 int launch_thomas_part(Context* c, int i, cudaStream_t s, bool homog = false);
 // FP32-bulk variant (csrc/solver32.cu)
 int setup32(Context* c);
+// 2-D tensor map of a [Ny][Nx] FP64 (or FP32) field with a bw x bh box (solver.cu).
+int encode_map_2d(CUtensorMap* map, const void* base, bool f32, int Nx, int Ny, int bw, int bh);
 void destroy32(Context* c);
 int split32(Context* c, cudaStream_t s);
 int export32(Context* c, bool with_rhs, cudaStream_t s);

@@ -181,8 +181,8 @@ static void twiddles(int M, std::vector<cpx<double>>& tw, std::vector<cpx<double
     if (M % 2 == 0) wN[M / 2] = {0.0, -1.0};
 }
 
-// 2-D tensor map of one [Ny][Nx] FP64 field with a box of bw x bh elements.
-static int encode_field_map(CUtensorMap* map, const double* base, int Nx, int Ny, int bw = SB_W, int bh = SB_H) {
+// 2-D tensor map of one [Ny][Nx] field (FP64, or FP32 with f32) with a box of bw x bh elements.
+int encode_map_2d(CUtensorMap* map, const void* base, bool f32, int Nx, int Ny, int bw, int bh) {
     static PFN_cuTensorMapEncodeTiled encode = nullptr;
     if (!encode) {
         void* fn = nullptr;
@@ -195,10 +195,11 @@ static int encode_field_map(CUtensorMap* map, const double* base, int Nx, int Ny
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
     }
     const cuuint64_t dims[2] = {(cuuint64_t)Nx, (cuuint64_t)Ny};
-    const cuuint64_t strides[1] = {(cuuint64_t)Nx * sizeof(double)};
+    const cuuint64_t strides[1] = {(cuuint64_t)Nx * (f32 ? sizeof(float) : sizeof(double))};
     const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
     const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+    const CUresult r = encode(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                              const_cast<void*>(base), dims, strides, box,
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -206,6 +207,10 @@ static int encode_field_map(CUtensorMap* map, const double* base, int Nx, int Ny
         return -1;
     }
     return 0;
+}
+
+static int encode_field_map(CUtensorMap* map, const double* base, int Nx, int Ny, int bw = SB_W, int bh = SB_H) {
+    return encode_map_2d(map, base, false, Nx, Ny, bw, bh);
 }
 
 template <typename T> static int dalloc(T** p, size_t n) {

@@ -46,6 +46,27 @@ int setup32(Context* c) {
     int per_sm = 0;
     NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv32, 256, 0));
     c->maxuv32_ctas = std::max(per_sm, 1) * c->num_sms;
+    // stage kernel: the persistent TMA form when every tile row holds two or more tiles
+    c->stage32_tma = (c->Nx >= 2 * S32_TX);
+    if (c->stage32_tma) {
+        const int Nx = c->Nx, Ny = c->Ny;
+        if (encode_map_2d(&c->tm32_psi, c->psif, true, Nx, Ny, S32_W, S32_H) ||
+            encode_map_2d(&c->tm32_w[0], c->wf, true, Nx, Ny, S32_W, S32_H) ||
+            encode_map_2d(&c->tm32_w[1], c->w1f, true, Nx, Ny, S32_W, S32_H) ||
+            encode_map_2d(&c->tm32_w[2], c->w2f, true, Nx, Ny, S32_W, S32_H) ||
+            encode_map_2d(&c->tm32_wn, c->wf, true, Nx, Ny, S32_TX, S32_TY))
+            return -1;
+        int per = 0;
+        NSE_CUDA_TRY(cudaFuncSetAttribute(k_stage32_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)stage32_tma_smem_bytes()));
+        NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage32_tma, 256, stage32_tma_smem_bytes()));
+        if (per < 1) {
+            set_error("k_stage32_tma cannot be resident");
+            return -1;
+        }
+        const int ntiles = (Nx / S32_TX) * ((Ny + S32_TY - 1) / S32_TY);
+        c->stage32_tma_grid = std::min(ntiles, per * c->num_sms);
+    }
     return 0;
 }
 
@@ -175,7 +196,15 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
         sp.rhs_out = (store_rhs && st == 3) ? c->rhsf : nullptr;
         sp.rc = c->rc32; sp.ctl = c->ctl; sp.Nx = c->Nx; sp.Ny = c->Ny; sp.stage = st;
         sp.nu_dx2 = (float)(c->nu * c->inv_dx2); sp.lin_drag = (float)c->cfg.lin_drag;
-        k_stage32<<<grid, 256, 0, s>>>(sp);
+        if (c->stage32_tma) {
+            Stage32Maps maps;
+            maps.psi = c->tm32_psi;
+            maps.w = c->tm32_w[st - 1];          // w'^(s): wf, w1f, w2f in stages 1, 2, 3
+            maps.wn = c->tm32_wn;
+            k_stage32_tma<<<c->stage32_tma_grid, 256, stage32_tma_smem_bytes(), s>>>(maps, sp);
+        } else {
+            k_stage32<<<grid, 256, 0, s>>>(sp);
+        }
         NSE_CUDA_TRY(cudaGetLastError());
         if (mark()) return -1;
         if (fft32_fwd(c, wst[st - 1], s) || mark()) return -1;
@@ -194,7 +223,7 @@ const char* step32_kernel_name(const Context* c, int k) {
     const int per = 3 + thomas_launches(c);
     if (k < 0 || k >= 3 * per) return "";
     const int i = k % per;
-    if (i == 0) return "k_stage32";
+    if (i == 0) return c->stage32_tma ? "k_stage32_tma" : "k_stage32";
     if (i == 1) return "k_fft_fwd32";
     if (i == per - 1) return "k_ifft_thom32";
     return thomas_kernel_name(c, i - 2);

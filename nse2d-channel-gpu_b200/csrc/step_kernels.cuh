@@ -545,7 +545,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
             dftR<double, R0, false>(v);
             const int p0 = dit16_pos<M>(t);
 #pragma unroll
-            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+            for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
         __syncthreads();
         p16_passes_from<double, M, 1, false, IP_NT>(buf, p.tw);
@@ -556,8 +556,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
 #pragma unroll 2
         for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
             const int kb = (k == 0 ? 0 : M - k);
-            const cpx<double> a = buf[ip_idx(k)];
-            const cpx<double> b = buf[ip_idx(kb)];
+            const cpx<double> a = buf[ip_idx<M>(k)];
+            const cpx<double> b = buf[ip_idx<M>(kb)];
             const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
             const cpx<double> df = {0.5 * (a.x - b.x), 0.5 * (a.y + b.y)};     // d/2
             const cpx<double> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
@@ -657,12 +657,12 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             dftR<double, R0, true>(v);
             const int p0 = dit16_pos<M>(t);
 #pragma unroll
-            for (int q = 0; q < R0; ++q) buf[ip_idx(p0 + q)] = v[q];
+            for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
         __syncthreads();
         p16_passes_from<double, M, 1, true, IP_NT>(buf, p.tw);
         for (int n = threadIdx.x; n < M; n += IP_NT) {
-            const cpx<double> z = buf[ip_idx(n)];
+            const cpx<double> z = buf[ip_idx<M>(n)];
             reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
         }
         __syncthreads();
@@ -1461,12 +1461,15 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 
 // max |u|, |v|, |v| a over the interior (src/diag.cu:702-866).
 //
-// Work items are (column strip, row band) pairs: a strip is MX_COLS columns, 2 per thread, and a
-// band is p.band_rows consecutive interior rows; CTAs stride over the items. A thread walks down
-// its band with a window of rows j-1, j, j+1 in registers, so that every row of the band is
-// read from HBM once (plus one halo row at each end of the band), and MX_U rows are loaded at a
-// time to keep loads in flight. The x neighbours c-1 and c+2 come from the adjacent lanes by
-// warp shuffle; the lanes at the ends of a warp load them.
+// Work items are (column strip, row band) pairs: a band is p.band_rows consecutive interior rows
+// and a strip MX_COLS columns, 60 per warp; CTAs stride over the items (one item per CTA at the
+// full grid). Lane l of a warp holds
+// the columns base + 2 (l - 1) and base + 2 (l - 1) + 1 (taken modulo Nx), so that lanes 1..30
+// own the warp's 60 columns and lanes 0 and 31 hold their outer neighbours: the x neighbours
+// of every owned column come from the adjacent lanes by warp shuffle. A thread walks down its
+// band with a window of rows j-1, j, j+1 in registers, so that every row of the band is read
+// from HBM once (plus one halo row at each end of the band); MX_U rows are loaded at a time,
+// the next MX_U while the current ones are reduced, to keep loads in flight.
 //
 // The maxima of |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| of a thread's points in
 // row j are scaled once per row: for positive factors, rounding is monotone, so
@@ -1474,87 +1477,73 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 // maximum to the bit. A running sum of the differences turns NaN or Inf anywhere into a
 // non-finite flag.
 //
-// VEC: 16-byte loads of a thread's two columns (Nx even and psi 16-byte aligned); otherwise
-// every value is an 8-byte load and any Nx >= 2 works.
-constexpr int MX_COLS = 512, MX_U = 4;
-
-__host__ __device__ inline int mx_wrap(int i, int Nx) { return i < 0 ? i + Nx : (i >= Nx ? i - Nx : i); }
+// VEC: one 16-byte load per row (Nx even and psi 16-byte aligned); otherwise two 8-byte loads,
+// and any Nx >= 2 works.
+constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS, MX_U = 4;
 
 template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;
     const double cy = 0.5 * p.inv_deta, cx = 0.5 * p.inv_dx;
     const int nitems = p.nstrips * p.nbands;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int strip = item % p.nstrips, band = item / p.nstrips;
-        const int c0 = strip * MX_COLS + 2 * (int)threadIdx.x;
-        const bool act = c0 < Nx, two = c0 + 1 < Nx;
-        const int cs = act ? c0 : 0;                     // an in-bounds column for idle lanes
-        const int cl = mx_wrap(cs - 1, Nx), cr1 = mx_wrap(cs + 1, Nx), cr2 = mx_wrap(cs + 2, Nx);
+        const int c = strip * MX_COLS + warp * MX_WCOLS + 2 * (lane - 1);
+        const bool own = lane >= 1 && lane <= 30 && c < Nx, two = c + 1 < Nx;
+        const int ca = ((c % Nx) + Nx) % Nx, cb = ((c + 1) % Nx + Nx) % Nx;     // the columns, modulo Nx
         const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
-        // lanes that take a neighbour from memory: the first lane of a warp (column c-1), and
-        // the last active lane (column c+2, whose owner is in another warp or wraps around)
-        const bool ldl = act && lane == 0, ldr = act && (lane == 31 || c0 + 2 >= Nx);
         auto ld2 = [&](int row) -> double2 {
             const double* r = p.psi + (size_t)row * Nx;
-            if constexpr (VEC) return __ldg(reinterpret_cast<const double2*>(r + cs));
-            else return make_double2(__ldg(r + cs), __ldg(r + cr1));
+            if constexpr (VEC) return __ldg(reinterpret_cast<const double2*>(r + ca));
+            else return make_double2(__ldg(r + ca), __ldg(r + cb));
         };
         double2 w0 = ld2(j0 - 1), w1 = ld2(j0);         // rows j-1 and j
+        double2 nx[MX_U];
+        auto load_batch = [&](int jb) {
+#pragma unroll
+            for (int u = 0; u < MX_U; ++u) nx[u] = ld2(min(jb + u, j1 - 1) + 1);   // rows past the band are not used
+        };
+        load_batch(j0);
         for (int j = j0; j < j1; j += MX_U) {
-            double2 nx[MX_U];
-            double el[MX_U], er[MX_U];
-            double an[MX_U];
+            double2 cur[MX_U];
+#pragma unroll
+            for (int u = 0; u < MX_U; ++u) cur[u] = nx[u];
+            if (j + MX_U < j1) load_batch(j + MX_U);
 #pragma unroll
             for (int u = 0; u < MX_U; ++u) {
-                const int jc = min(j + u, j1 - 1);       // centre row (clamped: rows past the band are not used)
-                nx[u] = ld2(jc + 1);
-                const double* rc = p.psi + (size_t)jc * Nx;
-                el[u] = 0.0; er[u] = 0.0;
-                if (!VEC || ldl) el[u] = __ldg(rc + cl);
-                if (!VEC || ldr) er[u] = __ldg(rc + cr2);
-                an[u] = __ldg(&p.a_node[jc]);
-            }
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) {
-                const double2 wc = (u == 0) ? w1 : nx[u - 1];
-                const double2 wm = (u == 0) ? w0 : (u == 1 ? w1 : nx[u - 2]);
-                double xl = el[u], xr = er[u];
-                if constexpr (VEC) {
-                    const double sl = __shfl_up_sync(0xffffffffu, wc.y, 1);
-                    const double sr = __shfl_down_sync(0xffffffffu, wc.x, 1);
-                    if (!ldl) xl = sl;
-                    if (!ldr) xr = sr;
-                }
-                if (j + u >= j1 || !act) continue;
-                // column c0: psi_{c0+1} - psi_{c0-1}; column c0+1: psi_{c0+2} - psi_{c0}
-                const double e0 = nx[u].x - wm.x, f0 = wc.y - xl;
+                const double2 wc = (u == 0) ? w1 : cur[u - 1];
+                const double2 wm = (u == 0) ? w0 : (u == 1 ? w1 : cur[u - 2]);
+                const double xl = __shfl_up_sync(0xffffffffu, wc.y, 1);      // column c - 1
+                const double xr = __shfl_down_sync(0xffffffffu, wc.x, 1);    // column c + 2
+                if (j + u >= j1 || !own) continue;
+                // column c: psi_{c+1} - psi_{c-1}; column c+1: psi_{c+2} - psi_{c}
+                const double e0 = cur[u].x - wm.x, f0 = wc.y - xl;
                 double dym = fabs(e0), dxm = fabs(f0), sum = e0 + f0;
                 if (two) {
-                    const double e1 = nx[u].y - wm.y, f1 = xr - wc.x;
+                    const double e1 = cur[u].y - wm.y, f1 = xr - wc.x;
                     dym = fmax(dym, fabs(e1));
                     dxm = fmax(dxm, fabs(f1));
                     sum += e1 + f1;
                 }
                 probe += sum;
-                const double a = an[u];
+                const double a = __ldg(&p.a_node[j + u]);
                 const double av = dxm * cx;
                 um = fmax(um, a * (dym * cy));
                 vm = fmax(vm, av);
                 vmm = fmax(vmm, av * a);
             }
-            if constexpr (MX_U == 1) { w0 = w1; w1 = nx[0]; }
-            else { w0 = nx[MX_U - 2]; w1 = nx[MX_U - 1]; }
+            if constexpr (MX_U == 1) { w0 = w1; w1 = cur[0]; }
+            else { w0 = cur[MX_U - 2]; w1 = cur[MX_U - 1]; }
         }
     }
     const int nonfinite = !(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300);
     maxuv_finish(p, um, vm, vmm, nonfinite);
 }
 
-// Strips of `cols` columns, bands and grid of the max reduction for a target of `ctas`
-// resident CTAs, at most `max_grid` CTAs (the partial slots); the CTAs stride over the items.
+// Strips of `cols` columns, bands and grid of the max reduction for a target of `ctas` resident
+// CTAs, at most `max_grid` CTAs (the partial slots); the CTAs stride over the items.
 inline void maxuv_plan(MaxParams& p, int ctas, int max_grid, int& grid, int cols = MX_COLS) {
     const int Ni = p.Ny - 2;
     p.nstrips = (p.Nx + cols - 1) / cols;
