@@ -423,43 +423,45 @@ template <int M>
 static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<float>* buf = reinterpret_cast<cpx<float>*>(smem_raw);
-    const int j = 1 + blockIdx.x;                       // interior rows
-    if (j > p.Ny - 2) return;
-    const float2* row = reinterpret_cast<const float2*>(p.src + (size_t)j * p.Nx);
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
-    // pass 0 from global (radix-16 plan of fft_rows.cuh): thread t transforms t + NB0 r
+    const int je = p.Ny - 1;                            // interior rows 1 .. Ny-2, strided over one wave of CTAs
+    for (int j = 1 + blockIdx.x; j < je; j += gridDim.x) {
+        const float2* row = reinterpret_cast<const float2*>(p.src + (size_t)j * p.Nx);
+        // pass 0 from global (radix-16 plan of fft_rows.cuh): thread t transforms t + NB0 r
 #pragma unroll 1
-    for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
-        const int t = b0 + (int)threadIdx.x;
-        if (NB0 % IP_NT != 0 && t >= NB0) break;
-        cpx<float> v[R0];
+        for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+            const int t = b0 + (int)threadIdx.x;
+            if (NB0 % IP_NT != 0 && t >= NB0) break;
+            cpx<float> v[R0];
 #pragma unroll
-        for (int r = 0; r < R0; ++r) {
-            const float2 z = __ldg(row + t + NB0 * r);
-            v[r] = {z.x, z.y};
-        }
-        dftR<float, R0, false>(v);
-        const int p0 = dit16_pos<M>(t);
+            for (int r = 0; r < R0; ++r) {
+                const float2 z = __ldg(row + t + NB0 * r);
+                v[r] = {z.x, z.y};
+            }
+            dftR<float, R0, false>(v);
+            const int p0 = dit16_pos<M>(t);
 #pragma unroll
-        for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
-    }
-    __syncthreads();
-    p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
-    // the split step for the pair (k, M - k) (see k_fft_fwd)
-    double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-    for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
-        const int kb = (k == 0 ? 0 : M - k);
-        const cpx<float> a = buf[ip_idx<M>(k)];
-        const cpx<float> b = buf[ip_idx<M>(kb)];
-        const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
-        const cpx<float> df = {0.5f * (a.x - b.x), 0.5f * (a.y + b.y)};
-        const cpx<float> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
-        dst[k] = make_double2((double)X.x, (double)X.y);
-        if (k < M / 2) {
-            const int m = M - k;
-            const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<float>{df.y, df.x}));
-            dst[m] = make_double2((double)Y.x, (double)Y.y);
+            for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
+        __syncthreads();
+        p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
+        // the split step for the pair (k, M - k) (see k_fft_fwd)
+        double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+        for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+            const int kb = (k == 0 ? 0 : M - k);
+            const cpx<float> a = buf[ip_idx<M>(k)];
+            const cpx<float> b = buf[ip_idx<M>(kb)];
+            const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
+            const cpx<float> df = {0.5f * (a.x - b.x), 0.5f * (a.y + b.y)};
+            const cpx<float> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
+            dst[k] = make_double2((double)X.x, (double)X.y);
+            if (k < M / 2) {
+                const int m = M - k;
+                const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<float>{df.y, df.x}));
+                dst[m] = make_double2((double)Y.x, (double)Y.y);
+            }
+        }
+        __syncthreads();                                // the split reads before the next row's pass 0
     }
 }
 
@@ -543,7 +545,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
 // ---- max |u|, |v|, |v| a of psibar + psi' ----
 // The item layout of k_maxuv_dt with 4 columns per lane (one 16-byte load per row; Nx is a
 // power of two >= 4): lanes 1..30 own a warp's 120 columns, lanes 0 and 31 hold their outer
-// neighbours, and the next MX_U rows are in flight while the current ones are reduced.
+// neighbours, and the next four rows are in flight while the current ones are reduced.
 struct Max32Params {
     MaxParams base;          // a_node, partials, control block, dt constants, items (base.psi unused)
     const float* psi;        // psi'
@@ -565,40 +567,55 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv32(Max32Params q) {
         const bool own = lane >= 1 && lane <= 30 && c < Nx;
         const int ca = ((c % Nx) + Nx) % Nx;
         const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
-        auto ld4 = [&](int row) { return __ldg(reinterpret_cast<const float4*>(q.psi + (size_t)row * Nx + ca)); };
-        float4 w0 = ld4(j0 - 1), w1 = ld4(j0);
-        float4 nx[MX_U];
-        auto load_batch = [&](int jb) {
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) nx[u] = ld4(min(jb + u, j1 - 1) + 1);
-        };
-        load_batch(j0);
-        for (int j = j0; j < j1; j += MX_U) {
-            float4 cur[MX_U];
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) cur[u] = nx[u];
-            if (j + MX_U < j1) load_batch(j + MX_U);
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) {
-                const float4 wc = (u == 0) ? w1 : cur[u - 1];
-                const float4 wm = (u == 0) ? w0 : (u == 1 ? w1 : cur[u - 2]);
-                const float xl = __shfl_up_sync(0xffffffffu, wc.w, 1);
-                const float xr = __shfl_down_sync(0xffffffffu, wc.x, 1);
-                if (j + u >= j1 || !own) continue;
-                const float d = __ldg(&q.dpsibar[j + u]);
-                const float e0 = (cur[u].x - wm.x) + d, e1 = (cur[u].y - wm.y) + d;
-                const float e2 = (cur[u].z - wm.z) + d, e3 = (cur[u].w - wm.w) + d;
+        auto row = [&](const float4& wm, const float4& wc, const float4& wp, double a, float d) {
+            const float xl = __shfl_up_sync(0xffffffffu, wc.w, 1);
+            const float xr = __shfl_down_sync(0xffffffffu, wc.x, 1);
+            if (own) {
+                const float e0 = (wp.x - wm.x) + d, e1 = (wp.y - wm.y) + d;
+                const float e2 = (wp.z - wm.z) + d, e3 = (wp.w - wm.w) + d;
                 const float f0 = wc.y - xl, f1 = wc.z - wc.x, f2 = wc.w - wc.y, f3 = xr - wc.z;
                 const float dym = fmaxf(fmaxf(fabsf(e0), fabsf(e1)), fmaxf(fabsf(e2), fabsf(e3)));
                 const float dxm = fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3)));
                 probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
-                const double a = __ldg(&p.a_node[j + u]);
                 const double av = (double)dxm * cx;
                 um = fmax(um, a * ((double)dym * cy));
                 vm = fmax(vm, av);
                 vmm = fmax(vmm, av * a);
             }
-            w0 = cur[MX_U - 2]; w1 = cur[MX_U - 1];
+        };
+        const size_t nx1 = (size_t)Nx;
+        const float* rp = q.psi + (size_t)(j0 - 1) * Nx + ca;
+        float4 wm = __ldg(reinterpret_cast<const float4*>(rp));
+        float4 wc = __ldg(reinterpret_cast<const float4*>(rp + nx1));
+        rp += 2 * nx1;
+        int j = j0;
+        float4 n0, n1, n2, n3;
+        auto load4 = [&](const float* r) {
+            n0 = __ldg(reinterpret_cast<const float4*>(r));
+            n1 = __ldg(reinterpret_cast<const float4*>(r + nx1));
+            n2 = __ldg(reinterpret_cast<const float4*>(r + 2 * nx1));
+            n3 = __ldg(reinterpret_cast<const float4*>(r + 3 * nx1));
+        };
+        if (j + 4 <= j1) load4(rp);
+        for (; j + 4 <= j1; j += 4) {
+            const float4 c0 = n0, c1 = n1, c2 = n2, c3 = n3;
+            const double a0 = __ldg(&p.a_node[j]), a1 = __ldg(&p.a_node[j + 1]);
+            const double a2 = __ldg(&p.a_node[j + 2]), a3 = __ldg(&p.a_node[j + 3]);
+            const float d0 = __ldg(&q.dpsibar[j]), d1 = __ldg(&q.dpsibar[j + 1]);
+            const float d2 = __ldg(&q.dpsibar[j + 2]), d3 = __ldg(&q.dpsibar[j + 3]);
+            rp += 4 * nx1;
+            if (j + 8 <= j1) load4(rp);
+            row(wm, wc, c0, a0, d0);
+            row(wc, c0, c1, a1, d1);
+            row(c0, c1, c2, a2, d2);
+            row(c1, c2, c3, a3, d3);
+            wm = c2; wc = c3;
+        }
+        for (; j < j1; ++j) {
+            const float4 c0 = __ldg(reinterpret_cast<const float4*>(rp));
+            rp += nx1;
+            row(wm, wc, c0, __ldg(&p.a_node[j]), __ldg(&q.dpsibar[j]));
+            wm = wc; wc = c0;
         }
     }
     const int nonfinite = !(probe - probe == 0.f) || !(um <= 1e300) || !(vm <= 1e300);

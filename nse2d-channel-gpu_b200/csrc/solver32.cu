@@ -124,7 +124,10 @@ static Fft32Params fft32_params(Context* c) {
 template <int M> static int fft32_fwd_t(Context* c, Fft32Params& p, cudaStream_t s) {
     const size_t sm = fft32_smem_bytes(M);
     NSE_CUDA_TRY(cudaFuncSetAttribute(k_fft_fwd32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_fft_fwd32<M><<<c->Ni, IP_NT, sm, s>>>(p);
+    int per_sm = 0;                                      // one wave of CTAs over the interior rows
+    NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_fwd32<M>, IP_NT, sm));
+    const int grid = std::max(1, std::min(c->Ni, std::max(per_sm, 1) * c->num_sms));
+    k_fft_fwd32<M><<<grid, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -1468,8 +1468,8 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 // own the warp's 60 columns and lanes 0 and 31 hold their outer neighbours: the x neighbours
 // of every owned column come from the adjacent lanes by warp shuffle. A thread walks down its
 // band with a window of rows j-1, j, j+1 in registers, so that every row of the band is read
-// from HBM once (plus one halo row at each end of the band); MX_U rows are loaded at a time,
-// the next MX_U while the current ones are reduced, to keep loads in flight.
+// from HBM once (plus one halo row at each end of the band); four rows are loaded at a time,
+// the next four while the current ones are reduced, to keep loads in flight.
 //
 // The maxima of |psi_{j+1} - psi_{j-1}| and |psi_{i+1} - psi_{i-1}| of a thread's points in
 // row j are scaled once per row: for positive factors, rounding is monotone, so
@@ -1478,8 +1478,8 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 // non-finite flag.
 //
 // VEC: one 16-byte load per row (Nx even and psi 16-byte aligned); otherwise two 8-byte loads,
-// and any Nx >= 2 works.
-constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS, MX_U = 4;
+// one row at a time, and any Nx >= 2 works.
+constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS, MX_U = 4;   // MX_U: rows per load batch (FP32 kernel)
 
 template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
@@ -1494,48 +1494,84 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
         const bool own = lane >= 1 && lane <= 30 && c < Nx, two = c + 1 < Nx;
         const int ca = ((c % Nx) + Nx) % Nx, cb = ((c + 1) % Nx + Nx) % Nx;     // the columns, modulo Nx
         const int j0 = 1 + band * p.band_rows, j1 = min(Ny - 1, j0 + p.band_rows);
-        auto ld2 = [&](int row) -> double2 {
-            const double* r = p.psi + (size_t)row * Nx;
-            if constexpr (VEC) return __ldg(reinterpret_cast<const double2*>(r + ca));
-            else return make_double2(__ldg(r + ca), __ldg(r + cb));
-        };
-        double2 w0 = ld2(j0 - 1), w1 = ld2(j0);         // rows j-1 and j
-        double2 nx[MX_U];
-        auto load_batch = [&](int jb) {
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) nx[u] = ld2(min(jb + u, j1 - 1) + 1);   // rows past the band are not used
-        };
-        load_batch(j0);
-        for (int j = j0; j < j1; j += MX_U) {
-            double2 cur[MX_U];
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) cur[u] = nx[u];
-            if (j + MX_U < j1) load_batch(j + MX_U);
-#pragma unroll
-            for (int u = 0; u < MX_U; ++u) {
-                const double2 wc = (u == 0) ? w1 : cur[u - 1];
-                const double2 wm = (u == 0) ? w0 : (u == 1 ? w1 : cur[u - 2]);
+        if constexpr (VEC) {
+            // one row of the window: rows wm (j-1), wc (j), wp (j+1) of the columns c, c+1
+            auto row = [&](const double2& wm, const double2& wc, const double2& wp, double a) {
                 const double xl = __shfl_up_sync(0xffffffffu, wc.y, 1);      // column c - 1
                 const double xr = __shfl_down_sync(0xffffffffu, wc.x, 1);    // column c + 2
-                if (j + u >= j1 || !own) continue;
-                // column c: psi_{c+1} - psi_{c-1}; column c+1: psi_{c+2} - psi_{c}
-                const double e0 = cur[u].x - wm.x, f0 = wc.y - xl;
-                double dym = fabs(e0), dxm = fabs(f0), sum = e0 + f0;
-                if (two) {
-                    const double e1 = cur[u].y - wm.y, f1 = xr - wc.x;
-                    dym = fmax(dym, fabs(e1));
-                    dxm = fmax(dxm, fabs(f1));
-                    sum += e1 + f1;
+                if (own) {
+                    const double e0 = wp.x - wm.x, e1 = wp.y - wm.y;
+                    const double f0 = wc.y - xl, f1 = xr - wc.x;
+                    probe += (e0 + f0) + (e1 + f1);
+                    const double dym = fmax(fabs(e0), fabs(e1)), dxm = fmax(fabs(f0), fabs(f1));
+                    const double av = dxm * cx;
+                    um = fmax(um, a * (dym * cy));
+                    vm = fmax(vm, av);
+                    vmm = fmax(vmm, av * a);
                 }
-                probe += sum;
-                const double a = __ldg(&p.a_node[j + u]);
-                const double av = dxm * cx;
-                um = fmax(um, a * (dym * cy));
-                vm = fmax(vm, av);
-                vmm = fmax(vmm, av * a);
+            };
+            const double* rp = p.psi + (size_t)(j0 - 1) * Nx + ca;     // row j0 - 1 of this lane's columns
+            const size_t nx1 = (size_t)Nx;
+            double2 wm = __ldg(reinterpret_cast<const double2*>(rp));
+            double2 wc = __ldg(reinterpret_cast<const double2*>(rp + nx1));
+            rp += 2 * nx1;                                            // row j0 + 1
+            int j = j0;
+            // four rows per step, the next four in flight while these are reduced
+            double2 n0, n1, n2, n3;
+            auto load4 = [&](const double* q) {
+                n0 = __ldg(reinterpret_cast<const double2*>(q));
+                n1 = __ldg(reinterpret_cast<const double2*>(q + nx1));
+                n2 = __ldg(reinterpret_cast<const double2*>(q + 2 * nx1));
+                n3 = __ldg(reinterpret_cast<const double2*>(q + 3 * nx1));
+            };
+            if (j + 4 <= j1) load4(rp);
+            for (; j + 4 <= j1; j += 4) {
+                const double2 c0 = n0, c1 = n1, c2 = n2, c3 = n3;
+                const double a0 = __ldg(&p.a_node[j]), a1 = __ldg(&p.a_node[j + 1]);
+                const double a2 = __ldg(&p.a_node[j + 2]), a3 = __ldg(&p.a_node[j + 3]);
+                rp += 4 * nx1;
+                if (j + 8 <= j1) load4(rp);
+                row(wm, wc, c0, a0);
+                row(wc, c0, c1, a1);
+                row(c0, c1, c2, a2);
+                row(c1, c2, c3, a3);
+                wm = c2; wc = c3;
             }
-            if constexpr (MX_U == 1) { w0 = w1; w1 = cur[0]; }
-            else { w0 = cur[MX_U - 2]; w1 = cur[MX_U - 1]; }
+            for (; j < j1; ++j) {                                     // the last rows of the band
+                const double2 c0 = __ldg(reinterpret_cast<const double2*>(rp));
+                rp += nx1;
+                row(wm, wc, c0, __ldg(&p.a_node[j]));
+                wm = wc; wc = c0;
+            }
+        } else {
+            auto ld2 = [&](int row) -> double2 {
+                const double* r = p.psi + (size_t)row * Nx;
+                return make_double2(__ldg(r + ca), __ldg(r + cb));
+            };
+            double2 w0 = ld2(j0 - 1), w1 = ld2(j0);                   // rows j-1 and j
+            for (int j = j0; j < j1; ++j) {
+                const double2 wp = ld2(j + 1);
+                const double xl = __shfl_up_sync(0xffffffffu, w1.y, 1);     // column c - 1
+                const double xr = __shfl_down_sync(0xffffffffu, w1.x, 1);   // column c + 2
+                if (own) {
+                    // column c: psi_{c+1} - psi_{c-1}; column c+1 (when it exists): psi_{c+2} - psi_{c}
+                    const double e0 = wp.x - w0.x, f0 = w1.y - xl;
+                    double dym = fabs(e0), dxm = fabs(f0), sum = e0 + f0;
+                    if (two) {
+                        const double e1 = wp.y - w0.y, f1 = xr - w1.x;
+                        dym = fmax(dym, fabs(e1));
+                        dxm = fmax(dxm, fabs(f1));
+                        sum += e1 + f1;
+                    }
+                    probe += sum;
+                    const double a = __ldg(&p.a_node[j]);
+                    const double av = dxm * cx;
+                    um = fmax(um, a * (dym * cy));
+                    vm = fmax(vm, av);
+                    vmm = fmax(vmm, av * a);
+                }
+                w0 = w1; w1 = wp;
+            }
         }
     }
     const int nonfinite = !(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300);
