@@ -578,9 +578,9 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv32(Max32Params q) {
                 const float dxm = fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3)));
                 probe += ((e0 + e1) + (e2 + e3)) + ((f0 + f1) + (f2 + f3));
                 const double av = (double)dxm * cx;
-                um = fmax(um, a * ((double)dym * cy));
-                vm = fmax(vm, av);
-                vmm = fmax(vmm, av * a);
+                um = nn_max(um, a * ((double)dym * cy));
+                vm = nn_max(vm, av);
+                vmm = nn_max(vmm, av * a);
             }
         };
         const size_t nx1 = (size_t)Nx;

@@ -1401,50 +1401,56 @@ struct MaxParams {
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
-// The block maxima of one reduction CTA, the last-CTA fold of all CTAs' partials, and dt from
-// the reference's formula with the output trimming (src/main.cu:439-480). All threads call it.
+// The larger of a and b for a >= 0 that is not NaN: a compare and a select. A NaN b is skipped
+// (as fmax skips it), and an accumulator that starts at 0 never becomes NaN.
+__device__ __forceinline__ double nn_max(double a, double b) { return b > a ? b : a; }
+__device__ __forceinline__ double warp_max_nn(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nn_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// The block maxima of one reduction CTA (warp shuffles, then the warp maxima in shared memory),
+// the last-CTA fold of all CTAs' partials by one warp, and dt from the reference's formula
+// with the output trimming (src/main.cu:439-480). All threads call it.
 __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, double vm, double vmm, int nonfinite) {
-    __shared__ double s[3][256];
-    __shared__ int snf;
+    __shared__ double s[3][32];
     __shared__ bool last;
-    if (threadIdx.x == 0) snf = 0;
-    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
-    __syncthreads();
-    if (nonfinite) atomicOr(&snf, 1);
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st)
-            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
-        __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
+    if (lane == 0) { s[0][warp] = um; s[1][warp] = vm; s[2][warp] = vmm; }
+    const int anynf = __syncthreads_or(nonfinite);
+    if (warp == 0) {
+        um = lane < nw ? s[0][lane] : 0.0;
+        vm = lane < nw ? s[1][lane] : 0.0;
+        vmm = lane < nw ? s[2][lane] : 0.0;
+        um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
+        if (lane == 0) {
+            p.blocks[blockIdx.x * 3 + 0] = um;
+            p.blocks[blockIdx.x * 3 + 1] = vm;
+            p.blocks[blockIdx.x * 3 + 2] = vmm;
+            if (anynf) atomicOr(&p.ctl->nonfinite, 1);
+            __threadfence();
+            const unsigned int done = atomicAdd(&p.ctl->blocks_done, 1u);
+            last = (done == gridDim.x - 1);
+        }
     }
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < 3; ++c) p.blocks[blockIdx.x * 3 + c] = s[c][0];
-        if (snf) atomicOr(&p.ctl->nonfinite, 1);
-        __threadfence();
-        const unsigned int done = atomicAdd(&p.ctl->blocks_done, 1u);
-        last = (done == gridDim.x - 1);
-    }
     __syncthreads();
-    if (!last) return;
+    if (!last || warp != 0) return;
     __threadfence();
     um = 0.0; vm = 0.0; vmm = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        um = fmax(um, __ldcg(&p.blocks[b * 3 + 0]));
-        vm = fmax(vm, __ldcg(&p.blocks[b * 3 + 1]));
-        vmm = fmax(vmm, __ldcg(&p.blocks[b * 3 + 2]));
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+        um = nn_max(um, __ldcg(&p.blocks[b * 3 + 0]));
+        vm = nn_max(vm, __ldcg(&p.blocks[b * 3 + 1]));
+        vmm = nn_max(vmm, __ldcg(&p.blocks[b * 3 + 2]));
     }
-    s[0][threadIdx.x] = um; s[1][threadIdx.x] = vm; s[2][threadIdx.x] = vmm;
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if ((int)threadIdx.x < st)
-            for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
+    um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
+    if (lane != 0) return;
     Ctl* ctl = p.ctl;
     ctl->blocks_done = 0;
-    ctl->umax = s[0][0]; ctl->vmax = s[1][0]; ctl->vmaxm = s[2][0];
+    ctl->umax = um; ctl->vmax = vm; ctl->vmaxm = vmm;
     if (!p.set_dt || !p.adapt) return;
-    const double umax = s[0][0], vmaxm = s[2][0];
+    const double umax = um, vmaxm = vmm;
     const double dt_x = (umax > 0 ? p.cfl * (p.dx / umax) : 1e30);
     const double dt_y = (vmaxm > 0 ? p.cfl * (p.deta / vmaxm) : 1e30);
     const double dt_adv = fmin(dt_x, dt_y);
@@ -1503,11 +1509,11 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
                     const double e0 = wp.x - wm.x, e1 = wp.y - wm.y;
                     const double f0 = wc.y - xl, f1 = xr - wc.x;
                     probe += (e0 + f0) + (e1 + f1);
-                    const double dym = fmax(fabs(e0), fabs(e1)), dxm = fmax(fabs(f0), fabs(f1));
+                    const double dym = nn_max(fabs(e0), fabs(e1)), dxm = nn_max(fabs(f0), fabs(f1));
                     const double av = dxm * cx;
-                    um = fmax(um, a * (dym * cy));
-                    vm = fmax(vm, av);
-                    vmm = fmax(vmm, av * a);
+                    um = nn_max(um, a * (dym * cy));
+                    vm = nn_max(vm, av);
+                    vmm = nn_max(vmm, av * a);
                 }
             };
             const double* rp = p.psi + (size_t)(j0 - 1) * Nx + ca;     // row j0 - 1 of this lane's columns
@@ -1559,16 +1565,16 @@ static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
                     double dym = fabs(e0), dxm = fabs(f0), sum = e0 + f0;
                     if (two) {
                         const double e1 = wp.y - w0.y, f1 = xr - w1.x;
-                        dym = fmax(dym, fabs(e1));
-                        dxm = fmax(dxm, fabs(f1));
+                        dym = nn_max(dym, fabs(e1));
+                        dxm = nn_max(dxm, fabs(f1));
                         sum += e1 + f1;
                     }
                     probe += sum;
                     const double a = __ldg(&p.a_node[j]);
                     const double av = dxm * cx;
-                    um = fmax(um, a * (dym * cy));
-                    vm = fmax(vm, av);
-                    vmm = fmax(vmm, av * a);
+                    um = nn_max(um, a * (dym * cy));
+                    vm = nn_max(vm, av);
+                    vmm = nn_max(vmm, av * a);
                 }
                 w0 = w1; w1 = wp;
             }
