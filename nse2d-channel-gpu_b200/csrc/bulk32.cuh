@@ -474,6 +474,9 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr float scale = 1.0f / (float)M;
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
+    // staged rows (M = 16 IP_NT): one pass-0 butterfly per thread, and the row fits in the buffer
+    constexpr bool kStageRow = (NB0 == IP_NT) && (ip_size(M) >= M + 1);
+    constexpr int kRowLoads = (M + 1 + IP_NT - 1) / IP_NT;
     for (int j = j0; j < j1; ++j) {
         float* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {                    // psi' = 0 on the walls
@@ -482,24 +485,62 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
         }
         // pass 0 from global with the merge (see k_ifft_thom)
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
-#pragma unroll 1
-        for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
-            const int t = b0 + (int)threadIdx.x;
-            if (NB0 % IP_NT != 0 && t >= NB0) break;
-            cpx<float> v[R0];
+        if constexpr (kStageRow) {
+            // the row X_0 .. X_M, rounded to FP32, first into shared memory (contiguous, every
+            // load of a thread in flight at once), so that the merge reads X_n and X_{M-n} there
+            float2* sx = reinterpret_cast<float2*>(buf);
+            double2 tmp[kRowLoads];
 #pragma unroll
-            for (int r = 0; r < R0; ++r) {
-                const int n = t + NB0 * r;
-                const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
-                const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
-                const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
-                const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
-                v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
+            for (int u = 0; u < kRowLoads; ++u) {
+                const int k = (int)threadIdx.x + IP_NT * u;
+                if (k <= M) tmp[u] = __ldcs(X + k);
             }
-            dftR<float, R0, true>(v);
-            const int p0 = dit16_pos<M>(t);
 #pragma unroll
-            for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+            for (int u = 0; u < kRowLoads; ++u) {
+                const int k = (int)threadIdx.x + IP_NT * u;
+                if (k <= M) sx[k] = make_float2((float)tmp[u].x, (float)tmp[u].y);
+            }
+            __syncthreads();
+            const int t = (int)threadIdx.x;
+            cpx<float> v[R0];
+            if (t < NB0) {
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int n = t + NB0 * r;
+                    const float2 av = sx[n], bv = sx[M - n];
+                    const cpx<float> a = {av.x, av.y}, b = {bv.x, -bv.y};
+                    const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
+                    const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
+                    v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
+                }
+            }
+            __syncthreads();                         // the whole row read before the butterflies overwrite it
+            if (t < NB0) {
+                dftR<float, R0, true>(v);
+                const int p0 = dit16_pos<M>(t);
+#pragma unroll
+                for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+            }
+        } else {
+#pragma unroll 1
+            for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
+                const int t = b0 + (int)threadIdx.x;
+                if (NB0 % IP_NT != 0 && t >= NB0) break;
+                cpx<float> v[R0];
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int n = t + NB0 * r;
+                    const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
+                    const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
+                    const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
+                    const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
+                    v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
+                }
+                dftR<float, R0, true>(v);
+                const int p0 = dit16_pos<M>(t);
+#pragma unroll
+                for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+            }
         }
         __syncthreads();
         p16_passes_from<float, M, 1, true, IP_NT>(buf, p.tw);
