@@ -435,7 +435,7 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
             cpx<float> v[R0];
 #pragma unroll
             for (int r = 0; r < R0; ++r) {
-                const float2 z = __ldg(row + t + NB0 * r);
+                const float2 z = ld_na(row + t + NB0 * r);
                 v[r] = {z.x, z.y};
             }
             dftR<float, R0, false>(v);

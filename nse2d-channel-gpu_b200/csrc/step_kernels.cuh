@@ -515,6 +515,19 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Row FFT kernels: one CTA of IP_NT threads transforms one row at a time in ONE shared buffer
 // (in-place decimation-in-time passes, fft_rows.cuh), so that 5 CTAs fit on an SM and the
 // load latency of one row is hidden behind the passes of the others.
+// 16-byte read-only load that does not allocate in L1 (rows read once, so that they do not
+// evict the twiddle tables the passes read from L1)
+__device__ __forceinline__ double2 ld_na(const double2* p) {
+    double2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float2 ld_na(const float2* p) {
+    float2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+
 constexpr int IP_NT = 128;
 __host__ __device__ constexpr size_t fft_smem_bytes(int M) { return (size_t)ip_size(M) * 16; }
 
@@ -539,7 +552,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
             cpx<double> v[R0];
 #pragma unroll
             for (int r = 0; r < R0; ++r) {
-                const double2 z = __ldg(row + t + NB0 * r);
+                const double2 z = ld_na(row + t + NB0 * r);
                 v[r] = {z.x, z.y};
             }
             dftR<double, R0, false>(v);
