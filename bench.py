@@ -97,7 +97,7 @@ def kernel_bytes(name, stage, Nx, Ny):
     """Algorithmic bytes of one launch of each kernel of this implementation (inputs read
     once, outputs written once); FP32-bulk kernels end in 32 (4-byte fields, FP64 spectra)."""
     N, H, Ni = Nx * Ny, Nx // 2 + 1, Ny - 2
-    if name == "k_stage32":
+    if name.startswith("k_stage32"):                              # k_stage32, k_stage32_tma
         return 4 * N * (2 if stage == 1 else 3) + 4 * N
     if name.startswith("k_fft_fwd32"):
         return 4 * Nx * Ni + 16 * H * Ni
