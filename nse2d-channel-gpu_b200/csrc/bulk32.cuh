@@ -270,8 +270,9 @@ struct Stage32Maps {
     CUtensorMap wn;          // w'^n tile box (S32_TX x S32_TY), stages 2 and 3
 };
 
+// srow[q][r]: the row constant q (RC_*) of tile row r, staged by the kernel for the tile.
 __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, const float* sp, const float* so,
-                                              const float* swn, int x0, int y0) {
+                                              const float* swn, int x0, int y0, const float (*srow)[S32_TY]) {
     const int Nx = p.Nx, Ny = p.Ny;
     const int l = threadIdx.x & 31, g = threadIdx.x >> 5;
     const int ly0 = g * S32_RPT;                        // tile row ly <-> box row ly + 1
@@ -292,7 +293,6 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
             dxo[k][r + 1] = O[r + 1][k + 2] - O[r + 1][k];
         }
     }
-    const float* rc = p.rc;
 #pragma unroll
     for (int q = 0; q < S32_RPT; ++q) {
         const int ly = ly0 + q, j = y0 + ly;
@@ -309,7 +309,7 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
             dxo[k][0] = dxo[k][1]; dxo[k][1] = dxo[k][2]; dxo[k][2] = O[2][k + 2] - O[2][k];
         }
         if (j >= Ny) break;
-        const float fr = __ldg(&rc[(size_t)RC_R * Ny + j]);
+        const float fr = srow[RC_R][ly];
         float rhs[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) rhs[k] = fmaf(-p.lin_drag, O[1][k + 1], fr);
@@ -317,7 +317,10 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
             float dyo[6], dyp[6];
 #pragma unroll
             for (int c = 0; c < 6; ++c) { dyo[c] = O[2][c] - O[0][c]; dyp[c] = P[2][c] - P[0][c]; }
-            const Rc32Row kr = rc32_row(rc, Ny, j);
+            Rc32Row kr;
+            kr.dpb = srow[RC_DPB][ly]; kr.dpp = srow[RC_DPP][ly]; kr.dpm = srow[RC_DPM][ly];
+            kr.dwb = srow[RC_DWB][ly]; kr.dwp = srow[RC_DWP][ly]; kr.dwm = srow[RC_DWM][ly];
+            kr.ap = srow[RC_AP][ly]; kr.am = srow[RC_AM][ly]; kr.cj = srow[RC_CJ][ly];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
                 rhs[k] = stage32_rhs_interior(rhs[k], O[1][k + 1], P[1][k], P[1][k + 2], P[0][k + 1], P[2][k + 1],
@@ -344,6 +347,7 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
 static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_constant__ Stage32Maps maps, Stage32Params p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t bars[2];
+    __shared__ float srow[RC32_N][S32_TY];
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     const int Nx = p.Nx, Ny = p.Ny;
     const int tiles_x = Nx / S32_TX, ntiles = tiles_x * ((Ny + S32_TY - 1) / S32_TY);
@@ -381,6 +385,10 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
         const int x0 = tx * S32_TX, y0 = ty * S32_TY;
         float* sp = reinterpret_cast<float*>(smem_raw + b * S32_BUF);
         float* so = reinterpret_cast<float*>(smem_raw + b * S32_BUF + S32_FIELD);
+        for (int e = threadIdx.x; e < RC32_N * S32_TY; e += blockDim.x) {   // the tile rows' constants
+            const int q = e / S32_TY, r = e % S32_TY;
+            srow[q][r] = __ldg(&p.rc[(size_t)q * Ny + min(y0 + r, Ny - 1)]);
+        }
         if (tx == 0 || tx == tiles_x - 1) {
             // periodic halo columns: box column 3 is x = -1, box column S32_TX + 4 is x = Nx
             for (int r = threadIdx.x; r < S32_H; r += blockDim.x) {
@@ -397,7 +405,7 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
             }
         }
         __syncthreads();
-        stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0);
+        stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0, srow);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
         __syncthreads();
     }

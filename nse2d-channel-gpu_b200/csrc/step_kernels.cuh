@@ -307,12 +307,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 // two adjacent columns per thread: warp g takes tile rows 4g .. 4g + 3, lane l the columns
 // x0 + 2l and x0 + 2l + 1. A row of the window (columns x - 1 .. x + 2) is three 16-byte shared
 // loads, the two points share their y differences, and the results leave as 16-byte stores.
+// srow[q][r] holds the row tables frow, st_ap, st_am, st_cj (q = 0..3) of tile row r.
 // The arithmetic of every point is stage_tile's (stage_rhs_interior), so both give the same bits.
 constexpr int ST2_RPT = 4;
 static_assert(8 * ST2_RPT == ST_TY && 64 == ST_TX, "pair layout: 8 warps x 4 rows, 32 lanes x 2 columns");
 
 __device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTime& st, const double* sp,
-                                            const double* so, const double* swn, int x0, int y0) {
+                                            const double* so, const double* swn, int x0, int y0,
+                                            const double (*srow)[ST_TY]) {
     const int Nx = p.Nx, Ny = p.Ny;
     const int lp = threadIdx.x & 31, g = threadIdx.x >> 5;
     const int i0 = x0 + 2 * lp;
@@ -348,14 +350,14 @@ __device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTim
         dxoB[0] = dxoB[1]; dxoB[1] = dxoB[2]; dxoB[2] = O[2][3] - O[2][1];
         if (j >= Ny) break;
         const double wa = O[1][1], wb = O[1][2];
-        const double fj = __ldg(&p.rt.frow[j]);
+        const double fj = srow[0][ly];
         double ra = fma(-p.lin_drag, wa, fj), rb = fma(-p.lin_drag, wb, fj);              // f - r omega
         const bool interior = (j != 0 && j != Ny - 1);
         if (interior) {
             double dyo[4], dyp[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) { dyo[c] = O[2][c] - O[0][c]; dyp[c] = P[2][c] - P[0][c]; }
-            const double ap = __ldg(&p.rt.st_ap[j]), am = __ldg(&p.rt.st_am[j]), cj = __ldg(&p.rt.st_cj[j]);
+            const double ap = srow[1][ly], am = srow[2][ly], cj = srow[3][ly];
             ra = stage_rhs_interior(ra, wa, P[1][0], P[1][2], P[0][1], P[2][1], dyp[0], dyp[1], dyp[2], dxpA,
                                     O[1][0], O[1][2], O[0][1], O[2][1], dyo[0], dyo[1], dyo[2], dxoA, nu_dx2, ap, am, cj);
             rb = stage_rhs_interior(rb, wb, P[1][1], P[1][3], P[0][2], P[2][2], dyp[1], dyp[2], dyp[3], dxpB,
@@ -394,6 +396,7 @@ __device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTim
 static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_constant__ StageMaps maps, StageParams p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t bars[2];
+    __shared__ double srow[4][ST_TY];
     // the boxes land at 128-byte aligned shared addresses
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     const int Nx = p.Nx, Ny = p.Ny;
@@ -432,6 +435,11 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
         const int x0 = tx * ST_TX, y0 = ty * ST_TY;
         double* sp = reinterpret_cast<double*>(smem_raw + b * SB_BUF);
         double* so = reinterpret_cast<double*>(smem_raw + b * SB_BUF + SB_FIELD);
+        if (threadIdx.x < 4 * ST_TY) {                   // the tile rows' table values (read by stage_tile2)
+            const int q = threadIdx.x / ST_TY, r = threadIdx.x % ST_TY, jr = min(y0 + r, Ny - 1);
+            const double* tab = q == 0 ? p.rt.frow : (q == 1 ? p.rt.st_ap : (q == 2 ? p.rt.st_am : p.rt.st_cj));
+            srow[q][r] = __ldg(&tab[jr]);
+        }
         if (tx == 0 || tx == tiles_x - 1) {
             // periodic halo columns: box column 1 is x = -1, box column ST_TX + 2 is x = Nx
             for (int r = threadIdx.x; r < SB_H; r += blockDim.x) {
@@ -448,7 +456,7 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
             }
         }
         __syncthreads();
-        stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0);
+        stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0, srow);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
         __syncthreads();
     }
