@@ -455,19 +455,31 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
         p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
         // the split step for the pair (k, M - k) (see k_fft_fwd)
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-        for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+        auto split = [&](int k, const cpx<float>& wk) {
             const int kb = (k == 0 ? 0 : M - k);
             const cpx<float> a = buf[ip_idx<M>(k)];
             const cpx<float> b = buf[ip_idx<M>(kb)];
             const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
             const cpx<float> df = {0.5f * (a.x - b.x), 0.5f * (a.y + b.y)};
-            const cpx<float> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
+            const cpx<float> X = cadd(sm, cmul(wk, mul_mi(df)));
             dst[k] = make_double2((double)X.x, (double)X.y);
             if (k < M / 2) {
                 const int m = M - k;
-                const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<float>{df.y, df.x}));
+                const cpx<float> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
+                const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(wm, cpx<float>{df.y, df.x}));
                 dst[m] = make_double2((double)Y.x, (double)Y.y);
             }
+        };
+        if constexpr (M == 16 * IP_NT) {                // one table load per thread (see k_fft_fwd)
+            const cpx<float> wt = ldtw(p.wN, threadIdx.x);
+#pragma unroll
+            for (int i = 0; i <= 8; ++i) {
+                const int k = (int)threadIdx.x + IP_NT * i;
+                if (k > M / 2) break;
+                split(k, i == 0 ? wt : cmul(wt, w32<float>(i)));
+            }
+        } else {
+            for (int k = threadIdx.x; k <= M / 2; k += IP_NT) split(k, ldtw(p.wN, k));
         }
         __syncthreads();                                // the split reads before the next row's pass 0
     }
@@ -512,6 +524,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
             const int t = (int)threadIdx.x;
             cpx<float> v[R0];
             if (t < NB0) {
+                const cpx<float> wt = ldtw(p.wN, t);    // W_{2M}^{t + NB0 r} = W_{2M}^t e^{-i pi r/16}
 #pragma unroll
                 for (int r = 0; r < R0; ++r) {
                     const int n = t + NB0 * r;
@@ -519,7 +532,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
                     const cpx<float> a = {av.x, av.y}, b = {bv.x, -bv.y};
                     const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
                     const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
-                    v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
+                    v[r] = cadd(E, mul_pi(cmulc(D, r == 0 ? wt : cmul(wt, w32<float>(r)))));
                 }
             }
             __syncthreads();                         // the whole row read before the butterflies overwrite it

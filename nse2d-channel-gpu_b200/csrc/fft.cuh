@@ -81,6 +81,24 @@ template <typename T> NSE_HD cpx<T> mul_w16(cpx<T> a, int j, bool inv) {
     if (inv) wi = -wi;
     return {a.x * wr - a.y * wi, a.x * wi + a.y * wr};
 }
+// e^{-i pi r / 16}, r = 0..15, from cos and sin of pi/16, pi/8, 3 pi/16, pi/4 (the doubles
+// nearest the exact values): the factor W_{2M}^{(M/16) r} that relates the split/merge twiddles
+// W_{2M}^n of the points n = t + (M/16) r to W_{2M}^t, whatever M.
+template <typename T> NSE_HD cpx<T> w32(int r) {
+    const T c1 = (T)0.98078528040323044912618223613424, s1 = (T)0.19509032201612826784828486847702;
+    const T c2 = (T)0.92387953251128675612818318939679, s2 = (T)0.38268343236508977172845998403040;
+    const T c3 = (T)0.83146961230254523707878837761791, s3 = (T)0.55557023301960222474283081394853;
+    const T h = (T)0.70710678118654752440084436210485;
+    switch (r & 15) {
+        case 0: return {(T)1, (T)0};   case 1: return {c1, -s1};   case 2: return {c2, -s2};
+        case 3: return {c3, -s3};      case 4: return {h, -h};     case 5: return {s3, -c3};
+        case 6: return {s2, -c2};      case 7: return {s1, -c1};   case 8: return {(T)0, (T)-1};
+        case 9: return {-s1, -c1};     case 10: return {-s2, -c2}; case 11: return {-s3, -c3};
+        case 12: return {-h, -h};      case 13: return {-c3, -s3}; case 14: return {-c2, -s2};
+        default: return {-c1, -s1};
+    }
+}
+
 template <typename T, bool INV> NSE_HD void dft16(cpx<T>* v) {
     cpx<T> y[4][4];
 #pragma unroll

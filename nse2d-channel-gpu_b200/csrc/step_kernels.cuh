@@ -574,20 +574,33 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
         //   X_k = s/2 + W^k (-i d)/2,   X_{M-k} = conj(s)/2 + W^{M-k} (i conj d)/2
         // (k = 0 pairs Z_0 with itself and gives X_0 and X_M; k = M/2 is its own pair).
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-#pragma unroll 2
-        for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+        auto split = [&](int k, const cpx<double>& wk) {
             const int kb = (k == 0 ? 0 : M - k);
             const cpx<double> a = buf[ip_idx<M>(k)];
             const cpx<double> b = buf[ip_idx<M>(kb)];
             const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
             const cpx<double> df = {0.5 * (a.x - b.x), 0.5 * (a.y + b.y)};     // d/2
-            const cpx<double> X = cadd(sm, cmul(ldtw(p.wN, k), mul_mi(df)));
+            const cpx<double> X = cadd(sm, cmul(wk, mul_mi(df)));
             dst[k] = make_double2(X.x, X.y);
             if (k < M / 2) {
                 const int m = M - k;                                           // m = M when k = 0
-                const cpx<double> Y = cadd(cpx<double>{sm.x, -sm.y}, cmul(ldtw(p.wN, m), cpx<double>{df.y, df.x}));
+                const cpx<double> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
+                const cpx<double> Y = cadd(cpx<double>{sm.x, -sm.y}, cmul(wm, cpx<double>{df.y, df.x}));
                 dst[m] = make_double2(Y.x, Y.y);
             }
+        };
+        if constexpr (M == 16 * IP_NT) {
+            // k = t + IP_NT i: W_{2M}^k = W_{2M}^t e^{-i pi i/16} (one table load per thread)
+            const cpx<double> wt = ldtw(p.wN, threadIdx.x);
+#pragma unroll
+            for (int i = 0; i <= 8; ++i) {
+                const int k = (int)threadIdx.x + IP_NT * i;
+                if (k > M / 2) break;
+                split(k, i == 0 ? wt : cmul(wt, w32<double>(i)));
+            }
+        } else {
+#pragma unroll 2
+            for (int k = threadIdx.x; k <= M / 2; k += IP_NT) split(k, ldtw(p.wN, k));
         }
         __syncthreads();
     }
@@ -667,13 +680,16 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             const int t = b0 + (int)threadIdx.x;
             if (NB0 % IP_NT != 0 && t >= NB0) break;
             cpx<double> v[R0];
+            // W_{2M}^n for n = t + NB0 r is W_{2M}^t e^{-i pi r/16} (one table load per thread)
+            const cpx<double> wt = ldtw(p.wN, t);
 #pragma unroll
             for (int r = 0; r < R0; ++r) {
                 const int n = t + NB0 * r;
                 const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
                 const cpx<double> sm = {0.5 * (av.x + bv.x), 0.5 * (av.y - bv.y)};
                 const cpx<double> df = {0.5 * (av.x - bv.x), 0.5 * (av.y + bv.y)};
-                v[r] = cadd(sm, mul_pi(cmulc(df, ldtw(p.wN, n))));
+                const cpx<double> wn = (R0 == 16) ? (r == 0 ? wt : cmul(wt, w32<double>(r))) : ldtw(p.wN, n);
+                v[r] = cadd(sm, mul_pi(cmulc(df, wn)));
             }
             dftR<double, R0, true>(v);
             const int p0 = dit16_pos<M>(t);
