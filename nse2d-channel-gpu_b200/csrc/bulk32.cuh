@@ -492,7 +492,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
     const int Nx = p.Nx, Ny = p.Ny;
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
-    constexpr float scale = 1.0f / (float)M;
+    constexpr float scale = 0.5f / (float)M;            // the merge forms 2 Z_n (see k_ifft_thom)
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     // staged rows (M = 16 IP_NT): one pass-0 butterfly per thread, and the row fits in the buffer
     constexpr bool kStageRow = (NB0 == IP_NT) && (ip_size(M) >= M + 1);
@@ -530,8 +530,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
                     const int n = t + NB0 * r;
                     const float2 av = sx[n], bv = sx[M - n];
                     const cpx<float> a = {av.x, av.y}, b = {bv.x, -bv.y};
-                    const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
-                    const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
+                    const cpx<float> E = {a.x + b.x, a.y + b.y};
+                    const cpx<float> D = {a.x - b.x, a.y - b.y};
                     v[r] = cadd(E, mul_pi(cmulc(D, r == 0 ? wt : cmul(wt, w32<float>(r)))));
                 }
             }
@@ -553,8 +553,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
                     const int n = t + NB0 * r;
                     const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
                     const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
-                    const cpx<float> E = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y)};
-                    const cpx<float> D = {0.5f * (a.x - b.x), 0.5f * (a.y - b.y)};
+                    const cpx<float> E = {a.x + b.x, a.y + b.y};
+                    const cpx<float> D = {a.x - b.x, a.y - b.y};
                     v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));
                 }
                 dftR<float, R0, true>(v);

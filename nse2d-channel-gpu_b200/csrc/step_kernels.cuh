@@ -660,7 +660,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     __shared__ bool thom_now;
     const int Nx = p.Nx, Ny = p.Ny;
-    constexpr double scale = 1.0 / (double)M;
+    constexpr double scale = 0.5 / (double)M;          // the merge forms 2 Z_n (see below)
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
@@ -671,9 +671,10 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             for (int i = threadIdx.x; i < Nx; i += IP_NT) dst[i] = v;
             continue;
         }
-        // pass 0 from global with the merge: thread t forms Z_n, n = t + NB0 r, from X_n and
-        // X_{M-n} (s = X_n + conj X_{M-n}, d = X_n - conj X_{M-n}, Z_n = s/2 + i d conj(W^n)/2)
-        // and transforms them in registers
+        // pass 0 from global with the merge: thread t forms 2 Z_n, n = t + NB0 r, from X_n and
+        // X_{M-n} (s = X_n + conj X_{M-n}, d = X_n - conj X_{M-n}, 2 Z_n = s + i d conj(W^n)) and
+        // transforms them in registers. The factor 2 is exact, it scales every later value by
+        // exactly 2, and the output scale 1/(2M) removes it, so the bits are those of Z_n.
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
 #pragma unroll 1
         for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
@@ -686,8 +687,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             for (int r = 0; r < R0; ++r) {
                 const int n = t + NB0 * r;
                 const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
-                const cpx<double> sm = {0.5 * (av.x + bv.x), 0.5 * (av.y - bv.y)};
-                const cpx<double> df = {0.5 * (av.x - bv.x), 0.5 * (av.y + bv.y)};
+                const cpx<double> sm = {av.x + bv.x, av.y - bv.y};
+                const cpx<double> df = {av.x - bv.x, av.y + bv.y};
                 const cpx<double> wn = (R0 == 16) ? (r == 0 ? wt : cmul(wt, w32<double>(r))) : ldtw(p.wN, n);
                 v[r] = cadd(sm, mul_pi(cmulc(df, wn)));
             }
