@@ -574,12 +574,13 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
         //   X_k = s/2 + W^k (-i d)/2,   X_{M-k} = conj(s)/2 + W^{M-k} (i conj d)/2
         // (k = 0 pairs Z_0 with itself and gives X_0 and X_M; k = M/2 is its own pair).
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+        // wk is W^k / 2: the halving of d moves into the twiddle (exact, the same bits)
         auto split = [&](int k, const cpx<double>& wk) {
             const int kb = (k == 0 ? 0 : M - k);
             const cpx<double> a = buf[ip_idx<M>(k)];
             const cpx<double> b = buf[ip_idx<M>(kb)];
             const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
-            const cpx<double> df = {0.5 * (a.x - b.x), 0.5 * (a.y + b.y)};     // d/2
+            const cpx<double> df = {a.x - b.x, a.y + b.y};                     // d
             const cpx<double> X = cadd(sm, cmul(wk, mul_mi(df)));
             dst[k] = make_double2(X.x, X.y);
             if (k < M / 2) {
@@ -591,7 +592,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
         };
         if constexpr (M == 16 * IP_NT) {
             // k = t + IP_NT i: W_{2M}^k = W_{2M}^t e^{-i pi i/16} (one table load per thread)
-            const cpx<double> wt = ldtw(p.wN, threadIdx.x);
+            const cpx<double> w1 = ldtw(p.wN, threadIdx.x);
+            const cpx<double> wt = {0.5 * w1.x, 0.5 * w1.y};
 #pragma unroll
             for (int i = 0; i <= 8; ++i) {
                 const int k = (int)threadIdx.x + IP_NT * i;
@@ -600,7 +602,10 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
             }
         } else {
 #pragma unroll 2
-            for (int k = threadIdx.x; k <= M / 2; k += IP_NT) split(k, ldtw(p.wN, k));
+            for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
+                const cpx<double> w1 = ldtw(p.wN, k);
+                split(k, cpx<double>{0.5 * w1.x, 0.5 * w1.y});
+            }
         }
         __syncthreads();
     }
