@@ -667,6 +667,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     const int Nx = p.Nx, Ny = p.Ny;
     constexpr double scale = 0.5 / (double)M;          // the merge forms 2 Z_n (see below)
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
+    constexpr bool kPairLanes = (NB0 == IP_NT) && (R0 == 16) && (IP_NT == 128);   // M = 2048
     int j0, j1;
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     for (int j = j0; j < j1; ++j) {                                   // a contiguous band of rows
@@ -681,6 +682,47 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
         // transforms them in registers. The factor 2 is exact, it scales every later value by
         // exactly 2, and the output scale 1/(2M) removes it, so the bits are those of Z_n.
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
+        if constexpr (kPairLanes) {
+            // Butterfly b of a thread: lanes 0..15 of warp w take b = 16 w + l, lanes 16..31 the
+            // mirrors 128 - b (lane 16 of warp 0, whose mirror would be b = 0 again, takes b = 64).
+            // The mirror point of n = b + 128 r is M - n = (128 - b) + 128 (15 - r), a point of the
+            // partner lane (l ^ 16): each thread loads only its own 16 points and gets the mirrors
+            // by shuffle. b = 64 is its own mirror (r <-> 15 - r); b = 0 mirrors r to 16 - r, and
+            // r = 0 to X_M, which it loads.
+            const int w = (int)threadIdx.x >> 5, l = (int)threadIdx.x & 31;
+            int b = (l < 16) ? 16 * w + l : 128 - (16 * w + l - 16);
+            if (b == 128) b = 64;
+            double2 x[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) x[r] = __ldcs(X + b + 128 * r);
+            const double2 xM = (b == 0) ? __ldcs(X + M) : make_double2(0.0, 0.0);
+            // W_{2M}^n for n = b + 128 r is W_{2M}^b e^{-i pi r/16} (one table load per thread)
+            const cpx<double> wt = ldtw(p.wN, b);
+            auto merge = [&](const double2& av, const double2& bv, int r) {
+                const cpx<double> sm = {av.x + bv.x, av.y - bv.y};
+                const cpx<double> df = {av.x - bv.x, av.y + bv.y};
+                const cpx<double> wn = (r == 0) ? wt : cmul(wt, w32<double>(r));
+                return cadd(sm, mul_pi(cmulc(df, wn)));
+            };
+            cpx<double> v[16];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int r2 = 15 - r;
+                double2 ma, mb;                          // the mirrors of the points r and 15 - r
+                ma.x = __shfl_xor_sync(0xffffffffu, x[r2].x, 16);
+                ma.y = __shfl_xor_sync(0xffffffffu, x[r2].y, 16);
+                mb.x = __shfl_xor_sync(0xffffffffu, x[r].x, 16);
+                mb.y = __shfl_xor_sync(0xffffffffu, x[r].y, 16);
+                if (b == 64) { ma = x[r2]; mb = x[r]; }
+                if (b == 0) { ma = (r == 0) ? xM : x[16 - r]; mb = x[r + 1]; }
+                v[r] = merge(x[r], ma, r);
+                v[r2] = merge(x[r2], mb, r2);
+            }
+            dftR<double, 16, true>(v);
+            const int p0 = dit16_pos<M>(b);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+        } else {
 #pragma unroll 1
         for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
             const int t = b0 + (int)threadIdx.x;
@@ -701,6 +743,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
             const int p0 = dit16_pos<M>(t);
 #pragma unroll
             for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+        }
         }
         __syncthreads();
         p16_passes_from<double, M, 1, true, IP_NT>(buf, p.tw);
