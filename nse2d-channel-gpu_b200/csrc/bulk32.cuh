@@ -568,10 +568,17 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
             }
         }
         __syncthreads();
-        p16_passes_from<float, M, 1, true, IP_NT>(buf, p.tw);
-        for (int n = threadIdx.x; n < M; n += IP_NT) {
-            const cpx<float> z = buf[ip_idx<M>(n)];
-            reinterpret_cast<float2*>(dst)[n] = make_float2(z.x * scale, z.y * scale);
+        if constexpr (p16_plan<M>::P >= 2) {
+            // the last pass stores z_n straight from registers (see k_ifft_thom)
+            p16_passes_to<float, M, 1, true, IP_NT>(buf, p.tw, [&](int n, const cpx<float>& z) {
+                reinterpret_cast<float2*>(dst)[n] = make_float2(z.x * scale, z.y * scale);
+            });
+        } else {
+            p16_passes_from<float, M, 1, true, IP_NT>(buf, p.tw);
+            for (int n = threadIdx.x; n < M; n += IP_NT) {
+                const cpx<float> z = buf[ip_idx<M>(n)];
+                reinterpret_cast<float2*>(dst)[n] = make_float2(z.x * scale, z.y * scale);
+            }
         }
         __syncthreads();
     }

@@ -95,8 +95,18 @@ template <typename T, bool INV> __device__ __forceinline__ cpx<T> p16_tw(cpx<T> 
     return INV ? cmulc(a, w) : cmul(a, w);
 }
 
+// One pass q >= 1 of the plan over the buffer; its outputs go to out(position, value), by
+// default back into the buffer.
+template <typename T, int M, int Q, bool INV, int NT, typename Out>
+__device__ __forceinline__ void p16_pass_to(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw, Out out);
+
 template <typename T, int M, int Q, bool INV, int NT>
 __device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw) {
+    p16_pass_to<T, M, Q, INV, NT>(buf, tw, [&](int pos, const cpx<T>& v) { buf[ip_idx<M>(pos)] = v; });
+}
+
+template <typename T, int M, int Q, bool INV, int NT, typename Out>
+__device__ __forceinline__ void p16_pass_to(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw, Out out) {
     constexpr int R = p16_plan<M>::R(Q), LP = p16_plan<M>::LP(Q), NB = M / R, OFF = p16_plan<M>::off(Q);
 #pragma unroll 1
     for (int b0 = 0; b0 < NB; b0 += NT) {
@@ -136,7 +146,7 @@ __device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>*
         }
         dftR<T, R, INV>(v);
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[ip_idx<M>(base + r * LP)] = v[r];
+        for (int r = 0; r < R; ++r) out(base + r * LP, v[r]);
     }
 }
 
@@ -146,6 +156,21 @@ __device__ __forceinline__ void p16_passes_from(cpx<T>* buf, const cpx<T>* tw) {
         p16_pass<T, M, Q, INV, NT>(buf, tw);
         __syncthreads();
         p16_passes_from<T, M, Q + 1, INV, NT>(buf, tw);
+    }
+}
+
+// Passes Q .. P-1 where the last one hands its outputs (natural order) to out(position, value)
+// instead of writing them back: the caller stores them to global memory from registers.
+// Needs P >= 2 and Q >= 1.
+template <typename T, int M, int Q, bool INV, int NT, typename Out>
+__device__ __forceinline__ void p16_passes_to(cpx<T>* buf, const cpx<T>* tw, Out out) {
+    constexpr int P = p16_plan<M>::P;
+    if constexpr (Q < P - 1) {
+        p16_pass<T, M, Q, INV, NT>(buf, tw);
+        __syncthreads();
+        p16_passes_to<T, M, Q + 1, INV, NT>(buf, tw, out);
+    } else if constexpr (Q == P - 1) {
+        p16_pass_to<T, M, Q, INV, NT>(buf, tw, out);
     }
 }
 

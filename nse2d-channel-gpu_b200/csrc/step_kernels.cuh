@@ -746,10 +746,17 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
         }
         }
         __syncthreads();
-        p16_passes_from<double, M, 1, true, IP_NT>(buf, p.tw);
-        for (int n = threadIdx.x; n < M; n += IP_NT) {
-            const cpx<double> z = buf[ip_idx<M>(n)];
-            reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
+        if constexpr (p16_plan<M>::P >= 2) {
+            // the last pass stores z_n = x_2n + i x_2n+1 straight from registers
+            p16_passes_to<double, M, 1, true, IP_NT>(buf, p.tw, [&](int n, const cpx<double>& z) {
+                reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
+            });
+        } else {
+            p16_passes_from<double, M, 1, true, IP_NT>(buf, p.tw);
+            for (int n = threadIdx.x; n < M; n += IP_NT) {
+                const cpx<double> z = buf[ip_idx<M>(n)];
+                reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
+            }
         }
         __syncthreads();
         if (p.do_thom) {
