@@ -452,34 +452,30 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
             for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
         __syncthreads();
-        p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
-        // the split step for the pair (k, M - k) (see k_fft_fwd)
-        double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-        auto split = [&](int k, const cpx<float>& wk) {             // wk = W^k / 2 (see k_fft_fwd)
-            const int kb = (k == 0 ? 0 : M - k);
-            const cpx<float> a = buf[ip_idx<M>(k)];
-            const cpx<float> b = buf[ip_idx<M>(kb)];
-            const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
-            const cpx<float> df = {a.x - b.x, a.y + b.y};
-            const cpx<float> X = cadd(sm, cmul(wk, mul_mi(df)));
-            dst[k] = make_double2((double)X.x, (double)X.y);
-            if (k < M / 2) {
-                const int m = M - k;
-                const cpx<float> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
-                const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(wm, cpx<float>{df.y, df.x}));
-                dst[m] = make_double2((double)Y.x, (double)Y.y);
-            }
-        };
-        if constexpr (M == 16 * IP_NT) {                // one table load per thread (see k_fft_fwd)
-            const cpx<float> w1 = ldtw(p.wN, threadIdx.x);
-            const cpx<float> wt = {0.5f * w1.x, 0.5f * w1.y};
-#pragma unroll
-            for (int i = 0; i <= 8; ++i) {
-                const int k = (int)threadIdx.x + IP_NT * i;
-                if (k > M / 2) break;
-                split(k, i == 0 ? wt : cmul(wt, w32<float>(i)));
-            }
+        if constexpr (M == 16 * IP_NT) {                // the fused last pass and split (see k_fft_fwd)
+            double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+            p16_pass<float, M, 1, false, IP_NT>(buf, p.tw);
+            __syncthreads();
+            fwd_last_pass_split<float, M>(buf, p.tw, p.wN, dst);
         } else {
+            p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
+            // the split step for the pair (k, M - k) (see k_fft_fwd)
+            double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+            auto split = [&](int k, const cpx<float>& wk) {             // wk = W^k / 2 (see k_fft_fwd)
+                const int kb = (k == 0 ? 0 : M - k);
+                const cpx<float> a = buf[ip_idx<M>(k)];
+                const cpx<float> b = buf[ip_idx<M>(kb)];
+                const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
+                const cpx<float> df = {a.x - b.x, a.y + b.y};
+                const cpx<float> X = cadd(sm, cmul(wk, mul_mi(df)));
+                dst[k] = make_double2((double)X.x, (double)X.y);
+                if (k < M / 2) {
+                    const int m = M - k;
+                    const cpx<float> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
+                    const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(wm, cpx<float>{df.y, df.x}));
+                    dst[m] = make_double2((double)Y.x, (double)Y.y);
+                }
+            };
             for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
                 const cpx<float> w1 = ldtw(p.wN, k);
                 split(k, cpx<float>{0.5f * w1.x, 0.5f * w1.y});

@@ -105,46 +105,56 @@ __device__ __forceinline__ void p16_pass(cpx<T>* __restrict__ buf, const cpx<T>*
     p16_pass_to<T, M, Q, INV, NT>(buf, tw, [&](int pos, const cpx<T>& v) { buf[ip_idx<M>(pos)] = v; });
 }
 
+// Butterfly b of pass q >= 1: loads its R points from the buffer, applies the twiddles and the
+// R-point DFT; v[r] is then the output at position base + r LP (returned in base).
+template <typename T, int M, int Q, bool INV>
+__device__ __forceinline__ int p16_bfly(const cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw, int b,
+                                        cpx<T> (&v)[p16_plan<M>::R(Q)]) {
+    constexpr int R = p16_plan<M>::R(Q), LP = p16_plan<M>::LP(Q), OFF = p16_plan<M>::off(Q);
+    const int mm = b & (LP - 1);
+    const int base = (b - mm) * R + mm;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[ip_idx<M>(base + r * LP)];
+    if (mm > 0) {
+        const int t = OFF + 4 * mm;
+        const cpx<T> w1 = ldtw(tw, t);
+        if constexpr (R == 2) {
+            v[1] = p16_tw<T, INV>(v[1], w1);
+        } else {
+            const cpx<T> w2 = ldtw(tw, t + 1), w3 = cmul(w1, w2);
+#pragma unroll
+            for (int r = 1; r < R; ++r) {                  // low digit a = r mod 4
+                const int a = r & 3;
+                if (a) v[r] = p16_tw<T, INV>(v[r], a == 1 ? w1 : (a == 2 ? w2 : w3));
+            }
+            if constexpr (R >= 8) {                        // high digit b = r / 4
+                const cpx<T> w4 = ldtw(tw, t + 2);
+                cpx<T> w8 = w4, w12 = w4;
+                if constexpr (R == 16) {
+                    w8 = ldtw(tw, t + 3);
+                    w12 = cmul(w4, w8);
+                }
+#pragma unroll
+                for (int r = 4; r < R; ++r) {
+                    const int hb = r >> 2;
+                    v[r] = p16_tw<T, INV>(v[r], hb == 1 ? w4 : (hb == 2 ? w8 : w12));
+                }
+            }
+        }
+    }
+    dftR<T, R, INV>(v);
+    return base;
+}
+
 template <typename T, int M, int Q, bool INV, int NT, typename Out>
 __device__ __forceinline__ void p16_pass_to(cpx<T>* __restrict__ buf, const cpx<T>* __restrict__ tw, Out out) {
-    constexpr int R = p16_plan<M>::R(Q), LP = p16_plan<M>::LP(Q), NB = M / R, OFF = p16_plan<M>::off(Q);
+    constexpr int R = p16_plan<M>::R(Q), LP = p16_plan<M>::LP(Q), NB = M / R;
 #pragma unroll 1
     for (int b0 = 0; b0 < NB; b0 += NT) {
         const int b = b0 + (int)threadIdx.x;
         if (NB % NT != 0 && b >= NB) break;
-        const int mm = b & (LP - 1);
-        const int base = (b - mm) * R + mm;
         cpx<T> v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = buf[ip_idx<M>(base + r * LP)];
-        if (mm > 0) {
-            const int t = OFF + 4 * mm;
-            const cpx<T> w1 = ldtw(tw, t);
-            if constexpr (R == 2) {
-                v[1] = p16_tw<T, INV>(v[1], w1);
-            } else {
-                const cpx<T> w2 = ldtw(tw, t + 1), w3 = cmul(w1, w2);
-#pragma unroll
-                for (int r = 1; r < R; ++r) {                  // low digit a = r mod 4
-                    const int a = r & 3;
-                    if (a) v[r] = p16_tw<T, INV>(v[r], a == 1 ? w1 : (a == 2 ? w2 : w3));
-                }
-                if constexpr (R >= 8) {                        // high digit b = r / 4
-                    const cpx<T> w4 = ldtw(tw, t + 2);
-                    cpx<T> w8 = w4, w12 = w4;
-                    if constexpr (R == 16) {
-                        w8 = ldtw(tw, t + 3);
-                        w12 = cmul(w4, w8);
-                    }
-#pragma unroll
-                    for (int r = 4; r < R; ++r) {
-                        const int hb = r >> 2;
-                        v[r] = p16_tw<T, INV>(v[r], hb == 1 ? w4 : (hb == 2 ? w8 : w12));
-                    }
-                }
-            }
-        }
-        dftR<T, R, INV>(v);
+        const int base = p16_bfly<T, M, Q, INV>(buf, tw, b, v);
 #pragma unroll
         for (int r = 0; r < R; ++r) out(base + r * LP, v[r]);
     }

@@ -539,6 +539,51 @@ __device__ __forceinline__ float2 ld_na(const float2* p) {
 constexpr int IP_NT = 128;
 __host__ __device__ constexpr size_t fft_smem_bytes(int M) { return (size_t)ip_size(M) * 16; }
 
+// The last pass of the forward transform at M = 16 IP_NT (= 2048) fused with the split step.
+// The last pass (radix 8, LP = 256) has butterflies mm = 0..255 holding Z_{mm + 256 r}; thread t
+// takes mm = t and its mirror 256 - t (thread 0: 0 and 128), so that every pair (Z_k, Z_{M-k})
+// of the split is in one thread's registers:
+//   t >= 1: k = t + 256 r with Z_{M-k} = B[7 - r], and k = 256 - t + 256 r with Z_{M-k} = A[7 - r];
+//   t = 0:  k = 256 r with Z_{M-k} = A[(8 - r) & 7] (r = 0 is the X_0 / X_M pair, and k = 1024
+//           pairs with itself), and k = 128 + 256 r with Z_{M-k} = B[7 - r];  r = 0..3.
+// X_k and X_{M-k} leave from registers; the split twiddles W_2M^k come from W_2M^t and the
+// e^{-i pi j/16} constants. The buffer is only read here.
+template <typename T, int M>
+__device__ __forceinline__ void fwd_last_pass_split(const cpx<T>* buf, const cpx<T>* tw, const cpx<T>* wN,
+                                                    double2* dst) {
+    static_assert(M == 16 * IP_NT && p16_plan<M>::P == 3 && p16_plan<M>::R(2) == 8 && p16_plan<M>::LP(2) == 256,
+                  "the fused split is written for M = 2048 (passes 16, 16, 8)");
+    const int t = threadIdx.x;
+    cpx<T> A[8], B[8];
+    p16_bfly<T, M, 2, false>(buf, tw, t, A);
+    p16_bfly<T, M, 2, false>(buf, tw, t == 0 ? 128 : 256 - t, B);
+    // X_k = s/2 + (W^k/2)(-i d), X_{M-k} = conj(s)/2 + (-conj(W^k)/2)(i conj d) with
+    // s = Z_k + conj Z_{M-k}, d = Z_k - conj Z_{M-k}; wk is W^k / 2
+    auto split = [&](int k, const cpx<T>& a, const cpx<T>& b, const cpx<T>& wk) {
+        const cpx<T> sm = {(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+        const cpx<T> df = {a.x - b.x, a.y + b.y};
+        const cpx<T> X = cadd(sm, cmul(wk, mul_mi(df)));
+        dst[k] = make_double2((double)X.x, (double)X.y);
+        if (k < M / 2) {
+            const cpx<T> wm = {-wk.x, wk.y};
+            const cpx<T> Y = cadd(cpx<T>{sm.x, -sm.y}, cmul(wm, cpx<T>{df.y, df.x}));
+            dst[M - k] = make_double2((double)Y.x, (double)Y.y);
+        }
+    };
+    const cpx<T> w1 = ldtw(wN, t);
+    const cpx<T> wh = {(T)0.5 * w1.x, (T)0.5 * w1.y};                 // W^t / 2 (exact halving)
+    const cpx<T> whc = {wh.x, -wh.y};                                   // conj(W^t) / 2
+    const cpx<T> half = {(T)0.5, (T)0};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const cpx<T> bA = (t == 0) ? A[(8 - r) & 7] : B[7 - r];
+        split(t + 256 * r, A[r], bA, r == 0 ? wh : cmul(wh, w32<T>(2 * r)));
+        const cpx<T> wB = (t == 0) ? cmul(half, w32<T>(1 + 2 * r)) : cmul(whc, w32<T>(2 + 2 * r));
+        split((t == 0 ? 128 : 256 - t) + 256 * r, B[r], (t == 0) ? B[7 - r] : A[7 - r], wB);
+    }
+    if (t == 0) split(M / 2, A[4], A[4], cmul(half, w32<T>(8)));
+}
+
 // Forward real FFT of rows row0 .. row0 + nrows - 1: rows 1..Ny-2 in the Poisson solve (the
 // reference's pack + cuFFT forward, src/poisson.cuh:93-96), all rows for the 1-D spectra:
 // a row is read as M complex points z_n = x_2n + i x_2n+1, scattered by cp.async into the
@@ -569,45 +614,39 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
             for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         }
         __syncthreads();
-        p16_passes_from<double, M, 1, false, IP_NT>(buf, p.tw);
-        // X_k and X_{M-k} from one pair: with s = Z_k + conj Z_{M-k}, d = Z_k - conj Z_{M-k},
-        //   X_k = s/2 + W^k (-i d)/2,   X_{M-k} = conj(s)/2 + W^{M-k} (i conj d)/2
-        // (k = 0 pairs Z_0 with itself and gives X_0 and X_M; k = M/2 is its own pair).
         double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
-        // wk is W^k / 2: the halving of d moves into the twiddle (exact, the same bits)
-        auto split = [&](int k, const cpx<double>& wk) {
-            const int kb = (k == 0 ? 0 : M - k);
-            const cpx<double> a = buf[ip_idx<M>(k)];
-            const cpx<double> b = buf[ip_idx<M>(kb)];
-            const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
-            const cpx<double> df = {a.x - b.x, a.y + b.y};                     // d
-            const cpx<double> X = cadd(sm, cmul(wk, mul_mi(df)));
-            dst[k] = make_double2(X.x, X.y);
-            if (k < M / 2) {
-                const int m = M - k;                                           // m = M when k = 0
-                const cpx<double> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
-                const cpx<double> Y = cadd(cpx<double>{sm.x, -sm.y}, cmul(wm, cpx<double>{df.y, df.x}));
-                dst[m] = make_double2(Y.x, Y.y);
-            }
-        };
         if constexpr (M == 16 * IP_NT) {
-            // k = t + IP_NT i: W_{2M}^k = W_{2M}^t e^{-i pi i/16} (one table load per thread)
-            const cpx<double> w1 = ldtw(p.wN, threadIdx.x);
-            const cpx<double> wt = {0.5 * w1.x, 0.5 * w1.y};
-#pragma unroll
-            for (int i = 0; i <= 8; ++i) {
-                const int k = (int)threadIdx.x + IP_NT * i;
-                if (k > M / 2) break;
-                split(k, i == 0 ? wt : cmul(wt, w32<double>(i)));
-            }
+            p16_pass<double, M, 1, false, IP_NT>(buf, p.tw);
+            __syncthreads();
+            fwd_last_pass_split<double, M>(buf, p.tw, p.wN, dst);
         } else {
+            p16_passes_from<double, M, 1, false, IP_NT>(buf, p.tw);
+            // X_k and X_{M-k} from one pair: with s = Z_k + conj Z_{M-k}, d = Z_k - conj Z_{M-k},
+            //   X_k = s/2 + W^k (-i d)/2,   X_{M-k} = conj(s)/2 + W^{M-k} (i conj d)/2
+            // (k = 0 pairs Z_0 with itself and gives X_0 and X_M; k = M/2 is its own pair).
+            // wk is W^k / 2: the halving of d moves into the twiddle (exact, the same bits)
+            auto split = [&](int k, const cpx<double>& wk) {
+                const int kb = (k == 0 ? 0 : M - k);
+                const cpx<double> a = buf[ip_idx<M>(k)];
+                const cpx<double> b = buf[ip_idx<M>(kb)];
+                const cpx<double> sm = {0.5 * (a.x + b.x), 0.5 * (a.y - b.y)};     // s/2
+                const cpx<double> df = {a.x - b.x, a.y + b.y};                     // d
+                const cpx<double> X = cadd(sm, cmul(wk, mul_mi(df)));
+                dst[k] = make_double2(X.x, X.y);
+                if (k < M / 2) {
+                    const int m = M - k;                                           // m = M when k = 0
+                    const cpx<double> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
+                    const cpx<double> Y = cadd(cpx<double>{sm.x, -sm.y}, cmul(wm, cpx<double>{df.y, df.x}));
+                    dst[m] = make_double2(Y.x, Y.y);
+                }
+            };
 #pragma unroll 2
             for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
                 const cpx<double> w1 = ldtw(p.wN, k);
                 split(k, cpx<double>{0.5 * w1.x, 0.5 * w1.y});
             }
         }
-        __syncthreads();
+        __syncthreads();                                 // the buffer read before the next row's pass 0
     }
 }
 
