@@ -181,10 +181,9 @@ int  nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s);
  * pointers), without a context and without allocating any device memory. No counterpart in
  * the reference. It is for callers that may not allocate: code whose device memory is all
  * handed out by its own pool, or that cannot afford the device-wide synchronisation of a
- * cudaMalloc/cudaFree pair in its loop. The reduction's scratch is a fixed array inside the
- * library, room for NSE2D_MAXUV_NOALLOC_MAX_BLOCKS per-CTA partials (24 KiB) plus a small
- * control block; the launch uses at most that many CTAs, which stride over the rows, so
- * every Ny fits. Nx must be in [2, 2^30] and Ny >= 3, and both pointers 8-byte aligned (any
+ * cudaMalloc/cudaFree pair in its loop. The reduction's scratch is a small control block
+ * inside the library (the CTAs combine their maxima there by atomic max); the launch uses at
+ * most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, which stride over the rows, so every grid fits. Nx must be in [2, 2^30] and Ny >= 3, and both pointers 8-byte aligned (any
  * Nx and offset work; 16-byte loads are used where Nx is even and psi 16-byte aligned); other
  * arguments are rejected with an error.
  * The first call on a device (with that device current) looks up the scratch address and

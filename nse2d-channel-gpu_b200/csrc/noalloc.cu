@@ -8,12 +8,12 @@
 // its other streams. The context API cannot serve it: nse2d_create allocates the fields and
 // the workspace of the whole time step.
 //
-// How: the reduction kernel is the time step's own k_maxuv_dt (one partial triple per CTA,
-// the last CTA folds them). Its partials and its control block live in g_maxuv_scratch, a
-// fixed file-scope device array, instead of the context's buffers. The first call on a
-// device, with that device current, looks up the array's address with cudaGetSymbolAddress
-// and caches it; that first call should come before any stream capture on the device.
-// Every call clears the control block (the last-CTA counter and the non-finite flag must
+// How: the reduction kernel is the time step's own k_maxuv_dt (the CTAs combine their maxima
+// by atomic max in a control block, and the last CTA reads them). That control block lives in
+// g_maxuv_scratch, a fixed file-scope device variable, instead of the context's. The first call
+// on a device, with that device current, looks up its address with cudaGetSymbolAddress and
+// caches it; that first call should come before any stream capture on the device. Every call
+// clears the control block (the maxima, the last-CTA counter and the non-finite flag must
 // start at zero) with cudaMemsetAsync. One scratch array serves every caller on a device,
 // so calls that overlap in time on one device, from two streams or two host threads, race.
 #include <cstdint>
@@ -29,8 +29,7 @@ namespace nse2d {
 namespace {
 constexpr int kMaxUvNoAllocBlocks = NSE2D_MAXUV_NOALLOC_MAX_BLOCKS;
 struct MaxUvScratch {
-    Ctl ctl;                                     // last-CTA counter, non-finite flag, results
-    double blocks[3 * kMaxUvNoAllocBlocks];      // per-CTA partial maxima
+    Ctl ctl;                                     // atomic maxima, last-CTA counter, non-finite flag, results
 };
 constexpr int kMaxDevices = 64;
 
@@ -103,11 +102,11 @@ extern "C" int nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node,
     MaxUvScratch* sc = slot.scratch;
     NSE_CUDA_TRY(cudaMemsetAsync(&sc->ctl, 0, sizeof(Ctl), s));
     MaxParams p{};
-    p.psi = d_psi; p.a_node = d_a_node; p.blocks = sc->blocks; p.ctl = &sc->ctl;
+    p.psi = d_psi; p.a_node = d_a_node; p.ctl = &sc->ctl;
     p.Nx = Nx; p.Ny = Ny; p.adapt = 0; p.set_dt = 0;
     p.inv_dx = inv_dx; p.inv_deta = inv_deta;
-    // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, one partial slot each; the CTAs stride over
-    // the (column strip, row band) items, so every grid is covered by that fixed number of slots.
+    // At most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs; they stride over the (column strip, row band)
+    // items, so every grid is covered, and combine their maxima atomically in the control block.
     int grid = 1;
     maxuv_plan(p, slot.per_sm * slot.num_sms, kMaxUvNoAllocBlocks, grid);
     // 16-byte loads only where every row and column pair is 16-byte aligned; a caller's psi may

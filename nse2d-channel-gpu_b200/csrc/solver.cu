@@ -636,13 +636,13 @@ int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s) {
 
 int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
     MaxParams p{};
-    p.psi = psi; p.a_node = c->rt.a_node; p.blocks = c->red_blocks; p.ctl = c->ctl;
+    p.psi = psi; p.a_node = c->rt.a_node; p.ctl = c->ctl;
     p.Nx = c->Nx; p.Ny = c->Ny; p.adapt = c->cfg.adapt; p.set_dt = set_dt ? 1 : 0;
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
     p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
     p.dt_max = c->cfg.dt_max;
     int grid = 1;
-    maxuv_plan(p, c->maxuv_ctas, (int)(c->red_capacity / 3), grid);   // one partial triple per CTA
+    maxuv_plan(p, c->maxuv_ctas, c->maxuv_ctas, grid);
     k_maxuv_dt<true><<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;

@@ -177,7 +177,7 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
     if (c->cfg.adapt) {
         Max32Params q{};
         MaxParams& p = q.base;
-        p.a_node = c->rt.a_node; p.blocks = c->red_blocks; p.ctl = c->ctl;
+        p.a_node = c->rt.a_node; p.ctl = c->ctl;
         p.Nx = c->Nx; p.Ny = c->Ny; p.adapt = 1; p.set_dt = 1;
         p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
         p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
@@ -185,7 +185,7 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
         q.psi = c->psif;
         q.dpsibar = c->rc32 + (size_t)RC_DPB * c->Ny;
         int grid = 1;
-        maxuv_plan(p, c->maxuv32_ctas, (int)(c->red_capacity / 3), grid, MX32_COLS);
+        maxuv_plan(p, c->maxuv32_ctas, c->maxuv32_ctas, grid, MX32_COLS);
         k_maxuv32<<<grid, 256, 0, s>>>(q);
         NSE_CUDA_TRY(cudaGetLastError());
         if (mark()) return -1;

@@ -1526,7 +1526,6 @@ static __global__ void __launch_bounds__(256) k_thom(ThomParams p) {
 struct MaxParams {
     const double* psi;
     const double* a_node;
-    double* blocks;          // [gridDim.x][3]
     Ctl* ctl;
     int Nx, Ny, adapt, set_dt;
     int nstrips, nbands, band_rows;   // work items of k_maxuv_dt (maxuv_plan)
@@ -1543,8 +1542,9 @@ __device__ __forceinline__ double warp_max_nn(double v) {
 }
 
 // The block maxima of one reduction CTA (warp shuffles, then the warp maxima in shared memory),
-// the last-CTA fold of all CTAs' partials by one warp, and dt from the reference's formula
-// with the output trimming (src/main.cu:439-480). All threads call it.
+// combined across CTAs by atomic maxima in the control block; the last CTA (a last-block
+// counter) reads and resets them and computes dt from the reference's formula with the output
+// trimming (src/main.cu:439-480). All threads call it.
 __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, double vm, double vmm, int nonfinite) {
     __shared__ double s[3][32];
     __shared__ bool last;
@@ -1558,9 +1558,11 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
         vmm = lane < nw ? s[2][lane] : 0.0;
         um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
         if (lane == 0) {
-            p.blocks[blockIdx.x * 3 + 0] = um;
-            p.blocks[blockIdx.x * 3 + 1] = vm;
-            p.blocks[blockIdx.x * 3 + 2] = vmm;
+            // non-negative doubles order as their bit patterns: atomic maxima on the patterns
+            unsigned long long* acc = p.ctl->mx_acc;
+            atomicMax(&acc[0], (unsigned long long)__double_as_longlong(um));
+            atomicMax(&acc[1], (unsigned long long)__double_as_longlong(vm));
+            atomicMax(&acc[2], (unsigned long long)__double_as_longlong(vmm));
             if (anynf) atomicOr(&p.ctl->nonfinite, 1);
             __threadfence();
             const unsigned int done = atomicAdd(&p.ctl->blocks_done, 1u);
@@ -1568,17 +1570,12 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
         }
     }
     __syncthreads();
-    if (!last || warp != 0) return;
+    if (!last || threadIdx.x != 0) return;
     __threadfence();
-    um = 0.0; vm = 0.0; vmm = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) {
-        um = nn_max(um, __ldcg(&p.blocks[b * 3 + 0]));
-        vm = nn_max(vm, __ldcg(&p.blocks[b * 3 + 1]));
-        vmm = nn_max(vmm, __ldcg(&p.blocks[b * 3 + 2]));
-    }
-    um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
-    if (lane != 0) return;
     Ctl* ctl = p.ctl;
+    um = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[0], 0ull));     // read and reset
+    vm = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[1], 0ull));
+    vmm = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[2], 0ull));
     ctl->blocks_done = 0;
     ctl->umax = um; ctl->vmax = vm; ctl->vmaxm = vmm;
     if (!p.set_dt || !p.adapt) return;
