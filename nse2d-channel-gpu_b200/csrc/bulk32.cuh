@@ -494,9 +494,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
     band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
     constexpr float scale = 0.5f / (float)M;            // the merge forms 2 Z_n (see k_ifft_thom)
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
-    // staged rows (M = 16 IP_NT): one pass-0 butterfly per thread, and the row fits in the buffer
-    constexpr bool kStageRow = (NB0 == IP_NT) && (ip_size(M) >= M + 1);
-    constexpr int kRowLoads = (M + 1 + IP_NT - 1) / IP_NT;
+    constexpr bool kPairLanes = (NB0 == IP_NT) && (R0 == 16) && (IP_NT == 128);   // M = 2048
     for (int j = j0; j < j1; ++j) {
         float* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {                    // psi' = 0 on the walls
@@ -505,43 +503,49 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
         }
         // pass 0 from global with the merge (see k_ifft_thom)
         const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
-        if constexpr (kStageRow) {
-            // the row X_0 .. X_M, rounded to FP32, first into shared memory (contiguous, every
-            // load of a thread in flight at once), so that the merge reads X_n and X_{M-n} there
-            float2* sx = reinterpret_cast<float2*>(buf);
-            double2 tmp[kRowLoads];
+        if constexpr (kPairLanes) {
+            // mirror lanes, as in k_ifft_thom: lanes 0..15 of warp w take butterflies 16 w + l,
+            // lanes 16..31 the mirrors 128 - b (64 for lane 16 of warp 0); each lane loads its
+            // own 16 points (rounded to FP32) and takes the mirror points X_{M-n} by shuffle
+            const int w = (int)threadIdx.x >> 5, l = (int)threadIdx.x & 31;
+            int b = (l < 16) ? 16 * w + l : 128 - (16 * w + l - 16);
+            if (b == 128) b = 64;
+            float2 x[16];
 #pragma unroll
-            for (int u = 0; u < kRowLoads; ++u) {
-                const int k = (int)threadIdx.x + IP_NT * u;
-                if (k <= M) tmp[u] = __ldcs(X + k);
+            for (int r = 0; r < 16; ++r) {
+                const double2 d = __ldcs(X + b + 128 * r);
+                x[r] = make_float2((float)d.x, (float)d.y);
             }
+            float2 xM = make_float2(0.f, 0.f);
+            if (b == 0) {
+                const double2 d = __ldcs(X + M);
+                xM = make_float2((float)d.x, (float)d.y);
+            }
+            const cpx<float> wt = ldtw(p.wN, b);        // W_{2M}^{b + 128 r} = W_{2M}^b e^{-i pi r/16}
+            auto merge = [&](const float2& av, const float2& bv, int r) {
+                const cpx<float> a = {av.x, av.y}, c = {bv.x, -bv.y};
+                const cpx<float> E = {a.x + c.x, a.y + c.y};
+                const cpx<float> D = {a.x - c.x, a.y - c.y};
+                return cadd(E, mul_pi(cmulc(D, r == 0 ? wt : cmul(wt, w32<float>(r)))));
+            };
+            cpx<float> v[16];
 #pragma unroll
-            for (int u = 0; u < kRowLoads; ++u) {
-                const int k = (int)threadIdx.x + IP_NT * u;
-                if (k <= M) sx[k] = make_float2((float)tmp[u].x, (float)tmp[u].y);
+            for (int r = 0; r < 8; ++r) {
+                const int r2 = 15 - r;
+                float2 ma, mb;                           // the mirrors of the points r and 15 - r
+                ma.x = __shfl_xor_sync(0xffffffffu, x[r2].x, 16);
+                ma.y = __shfl_xor_sync(0xffffffffu, x[r2].y, 16);
+                mb.x = __shfl_xor_sync(0xffffffffu, x[r].x, 16);
+                mb.y = __shfl_xor_sync(0xffffffffu, x[r].y, 16);
+                if (b == 64) { ma = x[r2]; mb = x[r]; }
+                if (b == 0) { ma = (r == 0) ? xM : x[16 - r]; mb = x[r + 1]; }
+                v[r] = merge(x[r], ma, r);
+                v[r2] = merge(x[r2], mb, r2);
             }
-            __syncthreads();
-            const int t = (int)threadIdx.x;
-            cpx<float> v[R0];
-            if (t < NB0) {
-                const cpx<float> wt = ldtw(p.wN, t);    // W_{2M}^{t + NB0 r} = W_{2M}^t e^{-i pi r/16}
+            dftR<float, 16, true>(v);
+            const int p0 = dit16_pos<M>(b);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) {
-                    const int n = t + NB0 * r;
-                    const float2 av = sx[n], bv = sx[M - n];
-                    const cpx<float> a = {av.x, av.y}, b = {bv.x, -bv.y};
-                    const cpx<float> E = {a.x + b.x, a.y + b.y};
-                    const cpx<float> D = {a.x - b.x, a.y - b.y};
-                    v[r] = cadd(E, mul_pi(cmulc(D, r == 0 ? wt : cmul(wt, w32<float>(r)))));
-                }
-            }
-            __syncthreads();                         // the whole row read before the butterflies overwrite it
-            if (t < NB0) {
-                dftR<float, R0, true>(v);
-                const int p0 = dit16_pos<M>(t);
-#pragma unroll
-                for (int q = 0; q < R0; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
-            }
+            for (int q = 0; q < 16; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
         } else {
 #pragma unroll 1
             for (int b0 = 0; b0 < NB0; b0 += IP_NT) {
