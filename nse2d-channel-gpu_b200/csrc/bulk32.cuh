@@ -373,6 +373,13 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
         const int b = k & 1;
         const int next = tile + gridDim.x;
         if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        const int x0 = tx * S32_TX, y0 = ty * S32_TY;
+        for (int e = threadIdx.x; e < RC32_N * S32_TY; e += blockDim.x) {   // the tile rows' constants
+            const int q = e / S32_TY, r = e % S32_TY;
+            srow[q][r] = __ldg(&p.rc[(size_t)q * Ny + min(y0 + r, Ny - 1)]);
+        }
+        // this barrier also orders the row constants above before their reads
         const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
         if (!ok) {
             if (threadIdx.x == 0) {
@@ -381,14 +388,8 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
             }
             return;
         }
-        const int tx = tile % tiles_x, ty = tile / tiles_x;
-        const int x0 = tx * S32_TX, y0 = ty * S32_TY;
         float* sp = reinterpret_cast<float*>(smem_raw + b * S32_BUF);
         float* so = reinterpret_cast<float*>(smem_raw + b * S32_BUF + S32_FIELD);
-        for (int e = threadIdx.x; e < RC32_N * S32_TY; e += blockDim.x) {   // the tile rows' constants
-            const int q = e / S32_TY, r = e % S32_TY;
-            srow[q][r] = __ldg(&p.rc[(size_t)q * Ny + min(y0 + r, Ny - 1)]);
-        }
         if (tx == 0 || tx == tiles_x - 1) {
             // periodic halo columns: box column 3 is x = -1, box column S32_TX + 4 is x = Nx
             for (int r = threadIdx.x; r < S32_H; r += blockDim.x) {
@@ -403,8 +404,8 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
                     so[r * S32_W + S32_TX + 4] = __ldg(&p.w_in[(size_t)gy * Nx]);
                 }
             }
+            __syncthreads();                             // tx is the same for the whole CTA
         }
-        __syncthreads();
         stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0, srow);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
         __syncthreads();

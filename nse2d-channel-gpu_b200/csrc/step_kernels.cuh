@@ -423,6 +423,14 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
         const int b = k & 1;
         const int next = tile + gridDim.x;
         if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        const int x0 = tx * ST_TX, y0 = ty * ST_TY;
+        if (threadIdx.x < 4 * ST_TY) {                   // the tile rows' table values (read by stage_tile2)
+            const int q = threadIdx.x / ST_TY, r = threadIdx.x % ST_TY, jr = min(y0 + r, Ny - 1);
+            const double* tab = q == 0 ? p.rt.frow : (q == 1 ? p.rt.st_ap : (q == 2 ? p.rt.st_am : p.rt.st_cj));
+            srow[q][r] = __ldg(&tab[jr]);
+        }
+        // this barrier also orders the table values above before their reads
         const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
         if (!ok) {
             if (threadIdx.x == 0) {
@@ -431,15 +439,8 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
             }
             return;
         }
-        const int tx = tile % tiles_x, ty = tile / tiles_x;
-        const int x0 = tx * ST_TX, y0 = ty * ST_TY;
         double* sp = reinterpret_cast<double*>(smem_raw + b * SB_BUF);
         double* so = reinterpret_cast<double*>(smem_raw + b * SB_BUF + SB_FIELD);
-        if (threadIdx.x < 4 * ST_TY) {                   // the tile rows' table values (read by stage_tile2)
-            const int q = threadIdx.x / ST_TY, r = threadIdx.x % ST_TY, jr = min(y0 + r, Ny - 1);
-            const double* tab = q == 0 ? p.rt.frow : (q == 1 ? p.rt.st_ap : (q == 2 ? p.rt.st_am : p.rt.st_cj));
-            srow[q][r] = __ldg(&tab[jr]);
-        }
         if (tx == 0 || tx == tiles_x - 1) {
             // periodic halo columns: box column 1 is x = -1, box column ST_TX + 2 is x = Nx
             for (int r = threadIdx.x; r < SB_H; r += blockDim.x) {
@@ -454,8 +455,8 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
                     so[r * SB_W + ST_TX + 2] = __ldg(&p.w_in[(size_t)gy * Nx]);
                 }
             }
+            __syncthreads();                             // tx is the same for the whole CTA
         }
-        __syncthreads();
         stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0, srow);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
         __syncthreads();
