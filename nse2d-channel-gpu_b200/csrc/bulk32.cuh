@@ -347,7 +347,7 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
 static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_constant__ Stage32Maps maps, Stage32Params p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ float srow[RC32_N][S32_TY];
+    __shared__ float srow[2][RC32_N][S32_TY];          // per buffer: the row constants of its tile
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     const int Nx = p.Nx, Ny = p.Ny;
     const int tiles_x = Nx / S32_TX, ntiles = tiles_x * ((Ny + S32_TY - 1) / S32_TY);
@@ -369,25 +369,22 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
     const float dt = (float)p.ctl->dt;
     int k = 0;
     if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    // one barrier per tile, as in k_stage_tma
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
         const int b = k & 1;
         const int next = tile + gridDim.x;
-        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
         const int tx = tile % tiles_x, ty = tile / tiles_x;
         const int x0 = tx * S32_TX, y0 = ty * S32_TY;
         for (int e = threadIdx.x; e < RC32_N * S32_TY; e += blockDim.x) {   // the tile rows' constants
             const int q = e / S32_TY, r = e % S32_TY;
-            srow[q][r] = __ldg(&p.rc[(size_t)q * Ny + min(y0 + r, Ny - 1)]);
+            srow[b][q][r] = __ldg(&p.rc[(size_t)q * Ny + min(y0 + r, Ny - 1)]);
         }
-        // this barrier also orders the row constants above before their reads
         const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
-        if (!ok) {
-            if (threadIdx.x == 0) {
-                atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
-                if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
-            }
+        if (!ok) {                                       // nothing else is in flight
+            if (threadIdx.x == 0) atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
             return;
         }
+        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
         float* sp = reinterpret_cast<float*>(smem_raw + b * S32_BUF);
         float* so = reinterpret_cast<float*>(smem_raw + b * S32_BUF + S32_FIELD);
         if (tx == 0 || tx == tiles_x - 1) {
@@ -406,9 +403,9 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
             }
             __syncthreads();                             // tx is the same for the whole CTA
         }
-        stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0, srow);
+        stage32_tile4(p, dt, sp, so, reinterpret_cast<const float*>(smem_raw + b * S32_BUF + 2 * S32_FIELD), x0, y0,
+                      srow[b]);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
-        __syncthreads();
     }
 }
 

@@ -263,8 +263,8 @@ static __global__ void __launch_bounds__(256) k_stage(StageParams p) {
 // (68 columns x 34 rows, FP64); rows outside [0, Ny) and columns outside [0, Nx) arrive as
 // zeros, and the periodic columns -1 and Nx of the first and last tile column are patched
 // with plain loads once the box has landed. A wait that does not complete within
-// kTmaWaitLimit polls sets bit 1 of the control block's error flags and ends the CTA (after
-// waiting, again bounded, for its other copy in flight).
+// kTmaWaitLimit polls sets bit 1 of the control block's error flags and ends the CTA (the next
+// tile's copy is issued only after that wait, so no other copy is in flight).
 constexpr int SB_W = ST_TX + 4, SB_H = ST_TY + 2;
 constexpr int SB_FIELD = ((SB_H * SB_W * 8 + 127) / 128) * 128;     // bytes per field, 128-byte aligned
 constexpr int SB_WN = ST_TX * ST_TY * 8;                          // omega^n tile (128-byte multiple)
@@ -396,7 +396,7 @@ __device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTim
 static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_constant__ StageMaps maps, StageParams p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ double srow[4][ST_TY];
+    __shared__ double srow[2][4][ST_TY];                // per buffer: the row tables of its tile
     // the boxes land at 128-byte aligned shared addresses
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     const int Nx = p.Nx, Ny = p.Ny;
@@ -419,26 +419,26 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
     const StageTime st = stage_time(p);
     int k = 0;
     if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    // One barrier per tile: it finds this tile's box landed, orders the table values staged
+    // before it, and tells thread 0 that every thread is done with the other buffer (the
+    // previous tile, whose reads each thread fenced against the async proxy), so that the next
+    // tile's box may be issued into it.
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
         const int b = k & 1;
         const int next = tile + gridDim.x;
-        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
         const int tx = tile % tiles_x, ty = tile / tiles_x;
         const int x0 = tx * ST_TX, y0 = ty * ST_TY;
         if (threadIdx.x < 4 * ST_TY) {                   // the tile rows' table values (read by stage_tile2)
             const int q = threadIdx.x / ST_TY, r = threadIdx.x % ST_TY, jr = min(y0 + r, Ny - 1);
             const double* tab = q == 0 ? p.rt.frow : (q == 1 ? p.rt.st_ap : (q == 2 ? p.rt.st_am : p.rt.st_cj));
-            srow[q][r] = __ldg(&tab[jr]);
+            srow[b][q][r] = __ldg(&tab[jr]);
         }
-        // this barrier also orders the table values above before their reads
         const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1));
-        if (!ok) {
-            if (threadIdx.x == 0) {
-                atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
-                if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
-            }
+        if (!ok) {                                       // nothing else is in flight
+            if (threadIdx.x == 0) atomicOr(const_cast<int*>(&p.ctl->nonfinite), 2);
             return;
         }
+        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
         double* sp = reinterpret_cast<double*>(smem_raw + b * SB_BUF);
         double* so = reinterpret_cast<double*>(smem_raw + b * SB_BUF + SB_FIELD);
         if (tx == 0 || tx == tiles_x - 1) {
@@ -457,9 +457,9 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
             }
             __syncthreads();                             // tx is the same for the whole CTA
         }
-        stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0, srow);
+        stage_tile2(p, st, sp, so, reinterpret_cast<const double*>(smem_raw + b * SB_BUF + 2 * SB_FIELD), x0, y0,
+                    srow[b]);
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
-        __syncthreads();
     }
 }
 
