@@ -9,7 +9,8 @@
 // FP64 and fixed (the x-means of the initial state; psibar carries the wall values, so psi' is 0
 // on both walls and tiny next to them), and the fluctuations w', psi' stored and stepped in FP32.
 // Since the base is steady, w' obeys the same Shu-Osher combines with the full rhs.
-//   - Stage (k_stage32): the Arakawa sum S of the full fields is S'(psi', w') plus base terms
+//   - Stage (k_stage32_tma; k_stage32 below 256 columns): the Arakawa sum S of the full fields
+//     is S'(psi', w') plus base terms
 //     that are FP64 row differences times x-differences of the fluctuations (the x-differences
 //     of the base vanish):
 //       -2 D psibar Dx w'_j - d+ psibar Dx w'_{j+1} - d- psibar Dx w'_{j-1}

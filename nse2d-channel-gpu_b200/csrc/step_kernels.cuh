@@ -1,9 +1,10 @@
 // Device kernels of one SSPRK(3,3) step (FP64). Written for this project.
 //
 // Per stage s (reference loop src/main.cu:482-538):
-//   k_stage       2-D tiles: omega^(s+1) = RK combine of omega^(s) + dt rhs(psi, omega^(s)),
+//   k_stage_tma   2-D tiles: omega^(s+1) = RK combine of omega^(s) + dt rhs(psi, omega^(s)),
 //                 rhs = -J_arakawa + nu lap + f(y) - r omega (+ MMS forcing). psi and omega
-//                 tiles with a one-cell halo are staged in shared memory.
+//                 tiles with a one-cell halo arrive in shared memory by TMA (k_stage, with
+//                 plain loads, below 128 columns).
 //   k_fft_fwd     forward real FFT of every interior row of omega^(s+1) -> omega-hat [Ny][Hp].
 //   k_thomas_cluster  y-direction tridiagonal solve of every kx column, in place
 //                 (omega-hat -> psi-hat). One thread-block cluster owns 8 kx columns and
