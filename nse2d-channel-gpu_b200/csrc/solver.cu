@@ -519,15 +519,14 @@ template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) 
     return 0;
 }
 
-// Inverse transforms: contiguous bands of L = ceil(Ny / wave) rows, one wave of CTAs (adjacent
-// rows of the spectral buffer are adjacent in memory; strided rows measured slower). The Thom
-// closure is applied by the CTA that writes the second row of each wall.
+// Inverse transforms: one wave of CTAs over contiguous bands of floor or ceil(Ny / wave) rows
+// (adjacent rows of the spectral buffer are adjacent in memory; strided rows measured slower).
+// The Thom closure is applied by the CTA that writes the second row of each wall.
 template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
     const size_t sm = fft_smem(M);
     int wave = 0;
     if (fft_wave(k_ifft_thom<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
-    p.rows_per_cta = (c->Ny + wave - 1) / wave;
-    const int grid = std::max(1, c->Ny / p.rows_per_cta);          // the last band takes the remainder
+    const int grid = std::max(1, std::min(wave, c->Ny));           // bands of Ny / grid rows (even split)
     k_ifft_thom<M><<<grid, IP_NT, sm, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
     return 0;

@@ -500,7 +500,6 @@ struct FftParams {
     const cpx<double>* tw;   // per-pass twiddles of the radix-16 plan (p16_twiddle_table)
     const cpx<double>* wN;   // M + 1 twiddles e^{-2 pi i k/Nx} of the split/merge step
     int Nx, Ny, Hp;
-    int rows_per_cta;        // inverse: rows of a band
     int row0, nrows;         // forward: transform rows row0 .. row0 + nrows - 1
     // inverse only: Thom closure (src/ops.cu:102-158) and the closure_diag wall bookkeeping
     double* w;               // omega^(s+1): wall rows rewritten
@@ -710,7 +709,10 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     constexpr bool kPairLanes = (NB0 == IP_NT) && (R0 == 16) && (IP_NT == 128);   // M = 2048
     int j0, j1;
-    band_of(blockIdx.x, gridDim.x, p.rows_per_cta, Ny, j0, j1);
+    // an even split of the rows over one wave of CTAs: bands of floor or ceil(Ny / grid) rows,
+    // the longer ones spread over the grid, so that every SM gets about the same number of rows
+    j0 = (int)(((long long)blockIdx.x * Ny) / gridDim.x);
+    j1 = (int)(((long long)(blockIdx.x + 1) * Ny) / gridDim.x);
     for (int j = j0; j < j1; ++j) {                                   // a contiguous band of rows
         double* dst = p.psi + (size_t)j * Nx;
         if (j == 0 || j == Ny - 1) {
