@@ -619,7 +619,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
 // power of two >= 4): lanes 1..30 own a warp's 120 columns, lanes 0 and 31 hold their outer
 // neighbours, and the next four rows are in flight while the current ones are reduced.
 struct Max32Params {
-    MaxParams base;          // a_node, partials, control block, dt constants, items (base.psi unused)
+    MaxParams base;          // a_node, control block, dt constants, items (base.psi unused)
     const float* psi;        // psi'
     const float* dpsibar;    // [Ny]: psibar_{j+1} - psibar_{j-1} (the RC_DPB row constant)
 };
