@@ -119,6 +119,13 @@ int  nse2d_get_field(nse2d_ctx* ctx, int which, double* host, cudaStream_t s);
  * the next output time); otherwise the dt of nse2d_set_dt / dt_init is used. use_graph:
  * replay one captured CUDA graph per step. */
 int  nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s);
+/* The tridiagonal solve of the Poisson step: clusters != 0 selects the one-pass form on
+ * persistent thread-block clusters (the default where it can be resident: fastest for a
+ * channel that has the device to itself), 0 the two-pass form on plain grids (which shares
+ * the device with concurrent work). Both give the reference's solve to round-off, not the
+ * same bits. Synchronises the device when the form changes (the step graph is captured
+ * again). */
+int  nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters);
 /* As nse2d_step without a graph, and the last step also stores its stage-3 rhs in the
  * context (field 4), which the next nse2d_diagnostics(t0_row = 0) pairs with omega for the
  * dOmega_rhs column (src/main.cu:586). */
@@ -214,7 +221,9 @@ int  nse2d_scalar(nse2d_ctx* ctx, int which, double* out);
 /* Many independent channels advanced by one graph launch: members are existing contexts (each
  * with its own grid, physics, state and adaptive dt), which must outlive the ensemble. The
  * graph's WHILE node repeats one step of every member; members are dealt round-robin onto
- * `groups` concurrent branches. Results do not depend on the grouping. */
+ * `groups` concurrent branches. Results do not depend on the grouping. Creating the ensemble
+ * sets its members to the two-pass tridiagonal solve (nse2d_set_tridiag_form(m, 0)), whose
+ * plain grids share the device with the other branches. */
 typedef struct nse2d_ensemble nse2d_ensemble;
 int  nse2d_ensemble_create(nse2d_ctx* const* members, int n, nse2d_ensemble** out);
 int  nse2d_ensemble_destroy(nse2d_ensemble* e);

@@ -120,6 +120,11 @@ int nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s) {
     return run_steps(ctx->c, nsteps, use_graph != 0, s, false);
 }
 
+int nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters) {
+    CHECK_CTX(ctx);
+    return set_tridiag_form(ctx->c, clusters != 0);
+}
+
 int nse2d_step_store_rhs(nse2d_ctx* ctx, int nsteps, cudaStream_t s) {
     CHECK_CTX(ctx);
     return run_steps(ctx->c, nsteps, false, s, true);

@@ -129,7 +129,8 @@ struct Context {
     unsigned int* tcount = nullptr;  // [groups] arrival counters (zero between solves)
     // one-pass cluster solve (k_thomas_cluster<L>): CTAs per cluster, rows per segment, resident
     // clusters (the persistent grid), dynamic shared memory, TMA maps of omega-hat and cp
-    bool thomas_cluster = false;
+    bool thomas_cluster = false;   // the form the step uses (nse2d_set_tridiag_form)
+    bool thomas_cluster_ok = false;  // the cluster form can be resident on this device
     int tc_cluster = 0, tc_L = 0, tc_nclusters = 0;
     size_t tc_smem = 0;
     CUtensorMap tm_hat{}, tm_cp{};

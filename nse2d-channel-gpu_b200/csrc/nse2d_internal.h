@@ -23,6 +23,9 @@ const char* thomas_kernel_name(const Context* c, int i);
 int launch_thomas_part(Context* c, int i, cudaStream_t s, bool homog = false);
 // FP32-bulk variant (csrc/solver32.cu)
 int setup32(Context* c);
+// Select the cluster (clusters != 0, where available) or the two-pass tridiagonal solve; drops
+// the context's captured step graphs when the form changes (solver.cu).
+int set_tridiag_form(Context* c, bool clusters);
 // 2-D tensor map of a [Ny][Nx] FP64 (or FP32) field with a bw x bh box (solver.cu).
 int encode_map_2d(CUtensorMap* map, const void* base, bool f32, int Nx, int Ny, int bw, int bh);
 void destroy32(Context* c);

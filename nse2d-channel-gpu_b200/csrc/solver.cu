@@ -372,6 +372,7 @@ int context_create(const Config& cfg, Context** out) {
             int nclusters = 0;
             if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &lc) == cudaSuccess && nclusters > 0) {
                 c->thomas_cluster = true;
+                c->thomas_cluster_ok = true;
                 c->tc_cluster = C;
                 c->tc_L = L;
                 c->tc_smem = smem;
@@ -604,6 +605,18 @@ int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
     maps.hat = c->tm_hat;
     maps.cp = c->tm_cp;
     NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, thomas_cluster_kernel(c->tc_L), maps, thomas_params(c, homog)));
+    return 0;
+}
+
+int set_tridiag_form(Context* c, bool clusters) {
+    const bool use = clusters && c->thomas_cluster_ok;
+    if (use == c->thomas_cluster) return 0;
+    // the captured graphs hold the other form's kernels: wait for any launch of them, then drop
+    // them (they are captured again at the next step)
+    NSE_CUDA_TRY(cudaDeviceSynchronize());
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
+    c->thomas_cluster = use;
     return 0;
 }
 

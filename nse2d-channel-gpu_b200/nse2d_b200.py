@@ -72,6 +72,7 @@ def load(path=LIB_PATH):
         "nse2d_field_ptr": (I, [P, I, ctypes.POINTER(P)]),
         "nse2d_get_field": (I, [P, I, P, P]),
         "nse2d_step": (I, [P, I, I, P]),
+        "nse2d_set_tridiag_form": (I, [P, I]),
         "nse2d_step_store_rhs": (I, [P, I, P]),
         "nse2d_launches_per_step": (I, [P]),
         "nse2d_step_timed": (I, [P, I, P, P]),
@@ -355,6 +356,11 @@ class Solver:
     # ---- time stepping ----
     def step(self, nsteps=1, use_graph=False, stream=None):
         _check(self.lib.nse2d_step(self.h, int(nsteps), 1 if use_graph else 0, _stream(stream)))
+
+    def set_tridiag_form(self, clusters):
+        """True: the one-pass cluster tridiagonal solve (the default where it fits); False: the
+        two-pass form, which shares the device with concurrent work (ensemble members use it)."""
+        _check(self.lib.nse2d_set_tridiag_form(self.h, 1 if clusters else 0))
 
     def step_store_rhs(self, nsteps=1, stream=None):
         _check(self.lib.nse2d_step_store_rhs(self.h, int(nsteps), _stream(stream)))

@@ -1,6 +1,7 @@
 """Batched ensembles (nse2d_ensemble_*) on a B200: one graph launch advances every member, and the
 result of each member equals that member stepped alone, to the bit, whatever the grouping of the
-members into concurrent branches."""
+members into concurrent branches. Ensemble members take the two-pass tridiagonal solve, so the
+solo runs they are compared with do too."""
 import numpy as np
 import pytest
 
@@ -34,6 +35,8 @@ def make(nse, m, seed):
 def test_ensemble_matches_solo_runs(nse, cuda):
     ens_m = [make(nse, m, 10 + i) for i, m in enumerate(MEMBERS)]
     solo = [make(nse, m, 10 + i) for i, m in enumerate(MEMBERS)]
+    for s in solo:
+        s.set_tridiag_form(False)
     e = nse.Ensemble(ens_m)
     groups, ms = e.autotune(trial_steps=2)
     assert 1 <= groups <= len(MEMBERS) and ms > 0
@@ -54,3 +57,23 @@ def test_ensemble_matches_solo_runs(nse, cuda):
     for a, b in zip(ens_m, solo):
         assert np.array_equal(a.fields()[0], b.fields()[0])
     e.close()
+
+
+def test_tridiag_forms_agree(nse, cuda):
+    """The cluster and the two-pass tridiagonal solves of the same channel agree to round-off, and
+    switching the form between steps (the step graph is captured again) keeps stepping."""
+    m = MEMBERS[4]
+    a, b = make(nse, m, 3), make(nse, m, 3)
+    b.set_tridiag_form(False)
+    a.step(5, use_graph=True)
+    b.step(5, use_graph=True)
+    wa, pa = a.fields()
+    wb, pb = b.fields()
+    assert np.max(np.abs(pa - pb)) <= 1e-12 * np.max(np.abs(pa))
+    assert np.max(np.abs(wa[2:-2] - wb[2:-2])) <= 1e-10 * np.max(np.abs(wa))
+    b.set_tridiag_form(True)
+    b.step(2, use_graph=True)
+    a.step(2, use_graph=True)
+    assert np.max(np.abs(a.fields()[1] - b.fields()[1])) <= 1e-12 * np.max(np.abs(pa))
+    a.close()
+    b.close()
