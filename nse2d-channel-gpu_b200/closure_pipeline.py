@@ -1,6 +1,6 @@
 """The learned-closure workflow on one GPU: DNS snapshots box-filtered to the coarse grid, the
 closure model trained on them, and the a-posteriori comparison of the coarse solve with the
-model against the DNS (its judge and its fallback).
+model against the DNS (the reference it is measured against, and its fallback).
 
 Host-side orchestration only: every field operation (time steps, the Jacobians, the filter,
 the velocities, training and inference) runs on the GPU through the C ABI (nse2d_b200).
@@ -194,8 +194,8 @@ def _stats_run(torch, solver, t_end, dt_stat, rows=None):
 
 
 def reference(torch, dns_cfg=DNS_CFG, Nxc=256, Nyc=129, seed=7, t_spinup=20.0, t_span=200.0, dt_stat=0.5, log=print):
-    """The DNS judge: spin-up from a fresh seed, the filtered state at its end (the coarse runs'
-    initial omega), then the DNS statistics over t_span."""
+    """The DNS reference: spin-up from a fresh seed, the filtered state at its end (the coarse
+    runs' initial omega), then the DNS statistics over t_span."""
     dns = nse.Solver(**dns_cfg)
     y = dns.metric(0)
     dns.set_omega(mix_omega(y, dns.Nx, dns_cfg["Lx"], 0.05, seed))
