@@ -1618,7 +1618,7 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 //
 // VEC: one 16-byte load per row (Nx even and psi 16-byte aligned); otherwise two 8-byte loads,
 // one row at a time, and any Nx >= 2 works.
-constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS, MX_U = 4;   // MX_U: rows per load batch (FP32 kernel)
+constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS;
 
 template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
