@@ -191,6 +191,51 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+class NvmlClock:
+    """SM clock and clock-event reasons of this process's GPU read in-process through NVML (a
+    read-only query): one sample when the timed region starts, then samples every ~2 ms while
+    its work runs on the device, so that even a region of a few ms has readings under load.
+    The GPU is found by its UUID, since NVML numbers every GPU of the machine."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, device_index):
+        self.samples, self.bits, self.h, self.nvml = [], 0, None, None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+        except Exception:
+            self.h = None
+
+    def sample(self):
+        if self.h is None:
+            return
+        try:
+            self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+            self.bits |= int(self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+        except Exception:
+            pass
+
+    def poll_until(self, stream, every_s=0.002):
+        """Sample until the work queued on `stream` has finished."""
+        while not stream.query():
+            self.sample()
+            time.sleep(every_s)
+        self.sample()
+
+    def result(self):
+        if self.h is None or not self.samples:
+            return {"nvml_samples": 0}
+        return {"nvml_sm_mhz": float(np.median(self.samples)), "nvml_sm_min_mhz": float(min(self.samples)),
+                "nvml_sm_max_mhz": float(self.max_mhz), "nvml_samples": len(self.samples),
+                "nvml_reasons": sorted(v for k, v in self.REASONS.items() if self.bits & k)}
+
+
 def dist_setup(backend="nccl"):
     """One process per GPU under torchrun (RANK, LOCAL_RANK, WORLD_SIZE, MASTER_* from the env).
     The ranks run independent replicas of the channel: the process group carries only the barrier
@@ -273,6 +318,7 @@ def run_ours(args, world, rank, local):
     # ---- timed region (resident state): K graph replays ----
     sampler = ClockSampler(local)
     sampler.start()
+    nv = NvmlClock(local)
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -280,10 +326,15 @@ def run_ours(args, world, rank, local):
         e0.record(stream)
         solver.step(args.steps, use_graph=True, stream=stream)
         e1.record(stream)
+    nv.poll_until(stream)                        # NVML samples while the replays run
     stream.synchronize()
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
+    clocks.update(nv.result())
+    if clocks.get("sm_mhz") is None and clocks.get("nvml_samples"):
+        clocks["sm_mhz"], clocks["sm_max_mhz"] = clocks["nvml_sm_mhz"], clocks["nvml_sm_max_mhz"]
+        clocks["reasons"] = clocks["nvml_reasons"]
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
     t_sim, dt_last, nsteps_done, umax = solver.time(stream=stream)
@@ -350,12 +401,8 @@ def run_ours(args, world, rank, local):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if P == 64 else "f32 (FP64 base profiles, spectral buffer and tridiagonal solve)",
-        "data": "synthetic (seeded Poiseuille + random vorticity over x-modes 1-64)",
-        "config": {"workload": f"channel SSPRK3 step 4096x2049 {'FP64' if P == 64 else 'FP32-bulk'}, tanh beta=2, "
-                               "Re_b=2e4, F0=0.05 n=12, drag 1e-3, adaptive dt CFL 0.5",
-                   "Nx": Nx, "Ny": Ny, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (each field 67 MB, step working set ~0.5 GB)",
-                   "graph": "one CUDA graph per step, replayed"},
+        "data": DATA,
+        "config": bench_config(P, world),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": dk["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": round(dk["achieved_gbs"] / peak, 4), "traffic": traffic, "peak_kind": peak_kind},
         "step_roofline": {"algorithmic_bytes_per_step": B_step, "achieved": round(step_gbs, 1), "peak": peak,
@@ -375,7 +422,30 @@ def run_ours(args, world, rank, local):
     return line
 
 
-def cpu_baseline(args, sample_steps=3, max_seconds=60.0):
+DATA = "synthetic (seeded Poiseuille + random vorticity over x-modes 1-64)"
+
+
+def bench_config(precision, world):
+    """The `config` object of both arms' lines (the same workload)."""
+    return {"workload": f"channel SSPRK3 step 4096x2049 {'FP64' if precision == 64 else 'FP32-bulk'}, tanh beta=2, "
+                        "Re_b=2e4, F0=0.05 n=12, drag 1e-3, adaptive dt CFL 0.5",
+            "Nx": WORKLOAD["Nx"], "Ny": WORKLOAD["Ny"],
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (each field 67 MB, step working set ~0.5 GB)",
+            "graph": "one CUDA graph per step, replayed"}
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(args, sample_steps=3, max_seconds=60.0, warmup=1, single_thread=True):
     """The oracle (C++/OpenMP CPU restatement of the reference algorithm) on the same workload."""
     ora = _load("nse2d_oracle_py", os.path.join(ORACLE, "oracle.py"))
     W = WORKLOAD
@@ -386,20 +456,32 @@ def cpu_baseline(args, sample_steps=3, max_seconds=60.0):
     y = o.metric(0)
     o.set_omega(initial_vorticity(W["Nx"], W["Ny"], W["Lx"], y, seed=1))
     t = 0.0
-    dt, _ = o.adapt_dt()
-    o.step(t, dt)                                  # warm-up step
-    t += dt
-    n = 0
-    t0 = time.perf_counter()
-    while n < sample_steps and time.perf_counter() - t0 < max_seconds:
-        dt, _ = o.adapt_dt()
-        o.step(t, dt)
-        t += dt
-        n += 1
-    el = time.perf_counter() - t0
+
+    def steps(n_max, seconds):
+        nonlocal t
+        n, t0 = 0, time.perf_counter()
+        while n < n_max and time.perf_counter() - t0 < seconds:
+            dt, _ = o.adapt_dt()
+            o.step(t, dt)
+            t += dt
+            n += 1
+        return n, time.perf_counter() - t0
+
+    steps(max(1, warmup), max_seconds)             # warm-up steps
+    n, el = steps(sample_steps, max_seconds)
+    cores = int(L.or_get_threads())
+    out = {"value": round(n / el, 4), "unit": "steps/s", "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+           "host_threads": os.cpu_count(),
+           "sample": f"{n} full SSPRK3 steps of the 4096x2049 workload (adaptive dt) after {max(1, warmup)} warm-up "
+                     f"step(s), {cores} threads"}
+    if single_thread:
+        L.or_set_threads(1)
+        n1, el1 = steps(1, max_seconds)
+        out["single_thread"] = {"value": round(n1 / el1, 4), "unit": "steps/s", "cores": 1,
+                                "sample": f"{n1} step(s) of the same run on one thread"}
+        L.or_set_threads(threads)
     o.close()
-    return {"value": round(n / el, 4), "unit": "steps/s", "cores": int(L.or_get_threads()), "kind": "port",
-            "sample": f"{n} full SSPRK3 steps of the 4096x2049 workload (adaptive dt) after 1 warm-up step"}
+    return out
 
 
 def exe_step_ms(exe, steps, warm=5):
@@ -441,7 +523,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return None
     steps = max(1, min(args.steps, args.ref_steps))
-    cb = cpu_baseline(args, sample_steps=steps, max_seconds=args.ref_seconds)
+    cb = cpu_baseline(args, sample_steps=steps, max_seconds=args.ref_seconds, warmup=min(args.warmup, 5))
     extra = {}
     if args.ref_cuda_steps > 0:
         try:
@@ -449,10 +531,8 @@ def run_reference(args, world, rank):
         except Exception as e:                                         # informational only
             extra["reference_cuda_b200"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     return {**extra, "metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": world, "steps": steps,
-            "warmup": 1, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poiseuille + random vorticity)",
-            "config": {"workload": "channel SSPRK3 step 4096x2049 FP64, tanh beta=2, Re_b=2e4, F0=0.05 n=12, "
-                                   "drag 1e-3, adaptive dt CFL 0.5", "Nx": 4096, "Ny": 2049},
+            "warmup": args.warmup, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA, "config": bench_config(64, world),
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

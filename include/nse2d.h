@@ -157,7 +157,9 @@ int  nse2d_get_time(nse2d_ctx* ctx, double* t, double* dt, long long* step, doub
  *   NSE2D_HALT_OUTPUT     t has reached min(next_snap, next_diag) (within the snap tolerance),
  *   NSE2D_HALT_STATS      the step count is a multiple of stats_every (0: never),
  *   NSE2D_HALT_END        t >= t_end - dt/2 (the reference's loop test),
- *   NSE2D_HALT_NONFINITE  a reduction saw NaN/Inf (or a bounded wait timed out),
+ *   NSE2D_HALT_NONFINITE  a bounded wait timed out, or the max reduction of an adaptive step saw
+ *                         NaN/Inf in psi for the first time since the state was set (a run halts
+ *                         once for that; nse2d_nonfinite tells the two apart),
  *   NSE2D_HALT_BUDGET     max_steps steps were taken;
  * *reason receives those bits. dt is trimmed to the output times as in the reference. At least
  * one step is taken. Synchronous. */
@@ -190,14 +192,21 @@ int  nse2d_max_uv(nse2d_ctx* ctx, double* out3, cudaStream_t s);
  * handed out by its own pool, or that cannot afford the device-wide synchronisation of a
  * cudaMalloc/cudaFree pair in its loop. The reduction's scratch is a small control block
  * inside the library (the CTAs combine their maxima there by atomic max); the launch uses at
- * most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, which stride over the rows, so every grid fits. Nx must be in [2, 2^30] and Ny >= 3, and both pointers 8-byte aligned (any
- * Nx and offset work; 16-byte loads are used where Nx is even and psi 16-byte aligned); other
- * arguments are rejected with an error.
- * The first call on a device (with that device current) looks up the scratch address and
- * should come before any stream capture on that device. Every call clears the control block
- * on stream s first. One scratch serves all callers on a device: calls that overlap in time
- * on the same device race. Synchronous: out3 (host) holds the result on return. */
+ * most NSE2D_MAXUV_NOALLOC_MAX_BLOCKS CTAs, which stride over the rows, so every grid fits.
+ * Nx must be in [2, 2^30] and Ny >= 3, and both pointers 8-byte aligned (any Nx and offset
+ * work; 16-byte loads are used where Nx is even and psi 16-byte aligned); other arguments are
+ * rejected with an error (status -1).
+ * The first call on a device (with that device current) looks up the scratch address; it is
+ * also where CUDA, which loads a library's kernels on first use, places this entry point's
+ * code and the static scratch on that device (a one-time placement by the driver): callers
+ * that must see no change of free device memory later make one call during their set-up.
+ * Every call clears the control block on stream s first. One scratch serves all callers on a
+ * device: calls that overlap in time on the same device race. Synchronous (it ends with a copy
+ * to host memory and a stream synchronisation): it must not be called while any stream of the
+ * device is being captured. Returns 0, or NSE2D_STATUS_NONFINITE when psi holds NaN or Inf
+ * (out3 then holds the maxima of the finite differences). */
 #define NSE2D_MAXUV_NOALLOC_MAX_BLOCKS 1024
+#define NSE2D_STATUS_NONFINITE 2
 int  nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node, int Nx, int Ny,
                           double inv_dx, double inv_deta, double* out3, cudaStream_t s);
 /* One diagnostics.csv row at the current state, columns umax .. Re_tau (16) followed by
@@ -208,7 +217,9 @@ int  nse2d_diagnostics(nse2d_ctx* ctx, int t0_row, double* out29, cudaStream_t s
 int  nse2d_rhs_at_state(nse2d_ctx* ctx, double t, cudaStream_t s);
 /* u, v of the context's psi into caller device arrays (src/ops.cu:47-70). */
 int  nse2d_uv(nse2d_ctx* ctx, double* d_u, double* d_v, cudaStream_t s);
-/* 1 when a max reduction met a NaN or Inf since the context was created. Synchronous. */
+/* Non-finite and timeout flags since the state was last set (nse2d_set_omega / nse2d_set_state):
+ * bit 0 a max reduction met NaN or Inf in psi, bit 1 a bounded wait of a kernel timed out.
+ * Synchronous. */
 int  nse2d_nonfinite(nse2d_ctx* ctx, int* flag, cudaStream_t s);
 /* Host copy of a metric: 0 y, 1 a_node, 2 a_edge (Ny-1), 3 dy_edge (Ny-1), 4 w_node. */
 int  nse2d_metrics(nse2d_ctx* ctx, int which, double* out);

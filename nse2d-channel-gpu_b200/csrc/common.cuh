@@ -59,6 +59,7 @@ struct Ctl {
     unsigned int thom_done[2];     // inverse transform: rows 1-2 / Ny-3..Ny-2 written (per wall)
     unsigned long long mx_acc[3];  // max reduction: atomic maxima of |u|, |v|, |v| a (bit patterns; 0 between launches)
     int nonfinite;                 // bit 0: a reduction saw NaN/Inf; bit 1: a bounded wait timed out
+    int nonfinite_halted;          // a run has already halted for bit 0 (it halts once for it)
     // run mode (nse2d_run): stop stepping when an output, a statistics step or the end is due
     int run;                       // 1 while a run is active
     int halt;                      // set at the end of the step after which the run stops

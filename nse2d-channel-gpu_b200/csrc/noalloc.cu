@@ -12,10 +12,16 @@
 // by atomic max in a control block, and the last CTA reads them). That control block lives in
 // g_maxuv_scratch, a fixed file-scope device variable, instead of the context's. The first call
 // on a device, with that device current, looks up its address with cudaGetSymbolAddress and
-// caches it; that first call should come before any stream capture on the device. Every call
-// clears the control block (the maxima, the last-CTA counter and the non-finite flag must
-// start at zero) with cudaMemsetAsync. One scratch array serves every caller on a device,
-// so calls that overlap in time on one device, from two streams or two host threads, race.
+// caches it. CUDA loads a library's kernels onto a device when they are first used (lazy
+// module loading, the default since CUDA 12.2), so that first call is also where the driver
+// places this file's code and the static scratch on the device: a one-time placement of a few
+// kilobytes by the driver, not an allocation of this entry point. A caller that must see no
+// change of free device memory after its set-up makes one call during set-up, on any grid.
+// Every call clears the control block (the maxima, the last-CTA counter and the non-finite
+// flag must start at zero) with cudaMemsetAsync. One scratch array serves every caller on a
+// device, so calls that overlap in time on one device, from two streams or two host threads,
+// race. Each call ends with a copy to pageable host memory and a stream synchronisation, so it
+// must not be called while any stream of the device is being captured into a CUDA graph.
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -115,7 +121,14 @@ extern "C" int nse2d_max_uv_noalloc(const double* d_psi, const double* d_a_node,
     if (vec) k_maxuv_dt<true><<<grid, 256, 0, s>>>(p);
     else k_maxuv_dt<false><<<grid, 256, 0, s>>>(p);
     NSE_CUDA_TRY(cudaGetLastError());
-    NSE_CUDA_TRY(cudaMemcpyAsync(out3, &sc->ctl.umax, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    Ctl h{};
+    NSE_CUDA_TRY(cudaMemcpyAsync(&h, &sc->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    out3[0] = h.umax; out3[1] = h.vmax; out3[2] = h.vmaxm;
+    if (h.nonfinite & 1) {
+        // the maxima skip NaN, so out3 alone would not show it
+        set_error("nse2d_max_uv_noalloc: psi holds NaN or Inf (out3 holds the maxima of the finite differences)");
+        return NSE2D_STATUS_NONFINITE;
+    }
     return 0;
 }

@@ -484,7 +484,13 @@ __device__ __forceinline__ void advance_time(Ctl* ctl) {
         if (fmin(ns, nd) < 1e299 && t + tol >= fmin(ns, nd)) r |= 1;
         if (ctl->stats_every > 0 && (ctl->step % ctl->stats_every) == 0) r |= 2;
         if (!(t < ctl->t_end - 0.5 * dt)) r |= 4;
-        if (ctl->nonfinite & 2) r |= 8;     // a bounded wait gave up; NaN alone runs on, as in the reference
+        if (ctl->nonfinite & 2) r |= 8;     // a bounded wait gave up
+        // the first NaN or Inf a reduction meets halts the run once, so that the host sees it; the
+        // run may then go on, as the reference's loop does with non-finite fields
+        if ((ctl->nonfinite & 1) && !ctl->nonfinite_halted) {
+            r |= 8;
+            ctl->nonfinite_halted = 1;
+        }
         if (r) {
             ctl->halt = 1;
             ctl->halt_reason = r;

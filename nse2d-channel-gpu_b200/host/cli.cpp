@@ -393,8 +393,17 @@ int main(int argc, char** argv) {
                           &reason, nullptr))
                 return fail("run");
             if (reason & NSE2D_HALT_NONFINITE) {
-                std::fprintf(stderr, "nse2d: a device wait timed out; stopping\n");
-                return 1;
+                int flag = 0;
+                if (nse2d_nonfinite(r.ctx, &flag, nullptr)) return fail("non-finite flag");
+                if (flag & 2) {
+                    std::fprintf(stderr, "nse2d: a device wait timed out; stopping\n");
+                    return 1;
+                }
+                // NaN or Inf in psi: reported once; the run goes on, as the reference's loop does
+                double tn = 0.0;
+                long long sn = 0;
+                if (nse2d_get_time(r.ctx, &tn, nullptr, &sn, nullptr, nullptr)) return fail("time");
+                LOGP("[warn] non-finite values in psi after step %lld (t=%.6f)\n", sn, tn);
             }
         }
         if (nse2d_get_time(r.ctx, &t, &dt, &step, nullptr, nullptr)) return fail("time");

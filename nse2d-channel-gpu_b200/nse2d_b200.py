@@ -133,6 +133,7 @@ def load(path=LIB_PATH):
 
 
 HALT_OUTPUT, HALT_STATS, HALT_END, HALT_NONFINITE, HALT_BUDGET = 1, 2, 4, 8, 16
+STATUS_NONFINITE = 2          # nse2d_max_uv_noalloc: psi holds NaN or Inf
 
 
 def _check(rc):
@@ -170,7 +171,8 @@ def _stream(s):
 def max_uv_noalloc(psi_dev, a_node_dev, Nx, Ny, inv_dx, inv_deta, stream=None):
     """max |u|, |v|, |v| a of a caller-owned psi [Ny, Nx] and a_node [Ny] (CUDA float64)
     through nse2d_max_uv_noalloc, which allocates no device memory. psi_dev and a_node_dev may
-    also be raw device addresses (int), such as Solver.field_ptr returns."""
+    also be raw device addresses (int), such as Solver.field_ptr returns. Raises Nse2dError when
+    the arguments are rejected or psi holds NaN or Inf."""
     def dev(a):
         return ctypes.c_void_p(a) if isinstance(a, int) else _ptr(a)
     out = (ctypes.c_double * 3)()
@@ -389,9 +391,11 @@ class Solver:
         return t.value, dt.value, st.value, tuple(um)
 
     def nonfinite(self, stream=None):
+        """Flags since the state was last set: bit 0 a max reduction met NaN/Inf in psi, bit 1
+        a bounded wait of a kernel timed out (0: neither)."""
         f = ctypes.c_int()
         _check(self.lib.nse2d_nonfinite(self.h, ctypes.byref(f), _stream(stream)))
-        return bool(f.value)
+        return int(f.value)
 
     # ---- operators ----
     def poisson_solve(self, w_dev, psi_dev, stream=None):

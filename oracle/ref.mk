@@ -7,8 +7,9 @@
 #   _ref/nse2d_ref_freeslip  the same with -DFREE_SLIP_WALLS (its WALLS=freeslip build)
 #   _ref/libnse2d_ref.so     the operators and the C-linkage test API (-DEXPORT_TEST_API
 #                            -DNSE2D_BUILD_AS_LIB, src/test_api.cu)
-# make -f ref.mk REF=/path/to/reference
-REF   ?= /root/reference
+# make -f ref.mk REF=/path/to/reference; without REF: $(NSE2D_REFERENCE_DIR), else the directory
+# "reference" beside this repository
+REF   ?= $(if $(NSE2D_REFERENCE_DIR),$(NSE2D_REFERENCE_DIR),$(abspath $(CURDIR)/../../reference))
 NVCC  ?= /usr/local/cuda/bin/nvcc
 OUT   := _ref
 SRCS  := $(addprefix $(REF)/src/,io.cu grid.cu ops.cu diag.cu poisson.cu init.cu main.cu)

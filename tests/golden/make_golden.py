@@ -1,7 +1,8 @@
 #!/usr/bin/env python3
 """Extract the golden vectors used by the parity tests from the reference's own test data.
 
-Run in a container that has the reference checked out (default /root/reference). Writes
+Run in a container that has the reference checked out (--reference DIR; default
+$NSE2D_REFERENCE_DIR, else the directory "reference" beside this repository). Writes
 tests/golden/reference_cases.json: for every case of the reference test suite
 (tests/run_tests.py:72-111 of the reference) its command line, the header of its
 diagnostics.csv and its first rows (the t = 0 row is a deterministic function of the
@@ -14,7 +15,9 @@ import json
 import os
 
 ap = argparse.ArgumentParser()
-ap.add_argument("--reference", default="/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+ap.add_argument("--reference", default=os.environ.get("NSE2D_REFERENCE_DIR")
+                or os.path.join(os.path.dirname(_REPO), "reference"))
 ap.add_argument("--rows", type=int, default=6)
 args = ap.parse_args()
 
