@@ -75,7 +75,8 @@ void nse2d_testapi_set_free_slip(int on);
 typedef struct nse2d_config {
     int    Nx, Ny;            /* Nx a power of two >= 4; Ny >= 5 */
     double Lx, h;
-    int    stretch;           /* 0 = none (uniform), 1 = tanh (src/grid.cu:33-45) */
+    int    stretch;           /* 0 = none (uniform), 1 = tanh (src/grid.cu:33-45), 2 = table
+                                 (y_table, src/grid.cu:46-78) */
     double beta;
     double Ub, Reb, nu_override;   /* nu = nu_override if >= 0, else 2 h Ub / Reb */
     double dt_init, dt_max, cfl, cvisc;
@@ -93,6 +94,8 @@ typedef struct nse2d_config {
                                  solve; no MMS forcing, no closure diagnostics). With 32, the
                                  FP64 fields behind nse2d_field_ptr are refreshed only by the
                                  calls that read them (fields, diagnostics, uv, statistics). */
+    const double* y_table;    /* stretch 2: the Ny node coordinates y_0 < ... < y_{Ny-1} (host
+                                 array, copied by nse2d_create; NULL otherwise) */
 } nse2d_config;
 
 typedef struct nse2d_ctx nse2d_ctx;
@@ -306,6 +309,28 @@ int  nse2d_cnn_train_step(nse2d_cnn* c, const double* w, const double* psi, cons
  * omega^(s); 0: it runs once per step on psi^n, omega^n and its tau is held over the three
  * stages. Precision 64. */
 int  nse2d_set_closure(nse2d_ctx* ctx, nse2d_cnn* net, int every_stage);
+
+/* ---- 5. Snapshot files (host code; no GPU) ----
+ * The reference's HDF5 snapshot layout (src/io.cu:183-259): datasets omega, psi, u, v
+ * [Ny][Nx] float64 (any subset, omega first), y [1][Ny] with attributes beta and stretch_code
+ * when stretch_tanh and y are given, root attributes t, Nx, Ny (int32), Lx, Ly, h, dx, dy, nu;
+ * written without libhdf5 (superblock 0, symbol-table root group, contiguous datasets), read as
+ * the reference reads it (src/init.cu:215-279). format 1 is the flat "bin" layout of the
+ * reference's declared SNAP_BIN (src/io.cuh:28), which it never writes. */
+typedef struct nse2d_snapshot_meta {
+    int    Nx, Ny;
+    double t, Lx, h, nu, beta;
+    int    stretch_tanh;      /* 1: tanh grid (y and its attributes are written when y != NULL) */
+    const double* y;          /* write: the Ny node coordinates, or NULL; read: set to NULL */
+    int    fields;            /* read: bits 1 omega, 2 psi, 4 u, 8 v, 16 y present */
+} nse2d_snapshot_meta;
+/* format 0: HDF5, 1: bin. At most 8 fields of Ny x Nx values each. */
+int  nse2d_snapshot_write(const char* path, int format, const nse2d_snapshot_meta* m, int nfields,
+                          const char* const* names, const double* const* fields);
+/* Either format (told apart by the file's signature). m (may be NULL) receives the metadata;
+ * with name != NULL the field ("omega", "psi", "u", "v": Ny x Nx values, stored [Ny][Nx] or
+ * transposed; "y": Ny values) is copied to out. */
+int  nse2d_snapshot_read(const char* path, nse2d_snapshot_meta* m, const char* name, double* out);
 
 const char* nse2d_last_error(void);
 

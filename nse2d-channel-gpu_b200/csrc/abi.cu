@@ -18,6 +18,7 @@ static Config to_config(const nse2d_config* a) {
     c.nforce = a->nforce; c.lin_drag = a->lin_drag; c.free_slip = a->free_slip; c.mms = a->mms;
     c.mms_A0 = a->mms_A0; c.mms_eps = a->mms_eps; c.mms_Om = a->mms_Om; c.mms_kx = a->mms_kx;
     c.closure_diag = a->closure_diag; c.precision = a->precision;
+    if (a->stretch == 2 && a->y_table) c.y_table.assign(a->y_table, a->y_table + (a->Ny > 0 ? a->Ny : 0));
     return c;
 }
 
@@ -45,6 +46,7 @@ void nse2d_config_default(nse2d_config* a) {
     a->nforce = d.nforce; a->lin_drag = d.lin_drag; a->free_slip = d.free_slip; a->mms = d.mms;
     a->mms_A0 = d.mms_A0; a->mms_eps = d.mms_eps; a->mms_Om = d.mms_Om; a->mms_kx = d.mms_kx;
     a->closure_diag = d.closure_diag; a->precision = d.precision;
+    a->y_table = nullptr;
 }
 
 int nse2d_create(const nse2d_config* cfg, nse2d_ctx** out) {

@@ -42,6 +42,10 @@ struct Config {
     double mms_A0 = 1e-3, mms_eps = 0.1, mms_Om = 1.0;
     int mms_kx = 1, closure_diag = 0;
     int precision = 64;      // 64: FP64 throughout; 32: FP32 bulk with FP64 islands
+    std::vector<double> y_table;   // stretch 2: the Ny node coordinates
+    // metrics given by the caller (Poisson2D_Z2Z::enable_mapped): a_node [Ny] and a_edge [Ny-1]
+    // replace the built ones (y and the weights stay those of the stretch)
+    std::vector<double> a_node_in, a_edge_in;
 };
 
 // Device control block: time, step size and the step's reductions. Kept on the device so

@@ -300,22 +300,28 @@ static __global__ void k_spectra_reduce(const cpx<double>* __restrict__ hat, int
 
 // One spectra sample of the current psi: u and v (into the stage buffers, free between steps),
 // the row transforms of each (into the spectral buffer), and the row reduction.
-int spectra_accumulate(Context* c, cudaStream_t s) {
+// One sample of E_u, E_v from device u, v [Ny][Nx] (16-byte aligned): the row transforms of the
+// spectral buffer, then the sums over rows of |X_k|^2 (src/diag.cu:868-898).
+int spectra_accumulate_uv(Context* c, const double* u, const double* v, cudaStream_t s) {
     if (!c->spec_acc) {
         NSE_CUDA_TRY(cudaMalloc((void**)&c->spec_acc, sizeof(double) * 2 * (size_t)c->Hp));
         NSE_CUDA_TRY(cudaMemsetAsync(c->spec_acc, 0, sizeof(double) * 2 * (size_t)c->Hp, s));
         c->spec_samples = 0;
     }
-    if (uv_from_psi(c, c->psi, c->w1, c->w2, s)) return -1;
     const double norm = 1.0 / ((double)c->Nx * (double)c->Nx * (double)c->Ny);
     const int tb = 128, gb = (c->H + tb - 1) / tb;
     for (int q = 0; q < 2; ++q) {
-        if (launch_fft_all_rows(c, q == 0 ? c->w1 : c->w2, s)) return -1;
+        if (launch_fft_all_rows(c, q == 0 ? u : v, s)) return -1;
         k_spectra_reduce<<<gb, tb, 0, s>>>(c->hat, c->Ny, c->Hp, c->H, norm, c->spec_acc + (size_t)q * c->Hp);
         NSE_CUDA_TRY(cudaGetLastError());
     }
     c->spec_samples += 1;
     return 0;
+}
+
+int spectra_accumulate(Context* c, cudaStream_t s) {
+    if (uv_from_psi(c, c->psi, c->w1, c->w2, s)) return -1;
+    return spectra_accumulate_uv(c, c->w1, c->w2, s);
 }
 
 }  // namespace nse2d

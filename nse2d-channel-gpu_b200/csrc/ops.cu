@@ -25,6 +25,9 @@ static void after_launch(const char* what) {
     }
 }
 
+void compat_check_launch(const char* what) { after_launch(what); }
+bool compat_free_slip() { return g_free_slip; }
+
 static dim3 grid2d(int Nx, int Ny, dim3 tb) { return dim3((Nx + tb.x - 1) / tb.x, (Ny + tb.y - 1) / tb.y); }
 
 // u, v with clamped j+-1 at the walls: src/ops.cu:47-63

@@ -42,22 +42,57 @@ int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>
         w_node[0] *= 0.5; w_node[Ny - 1] *= 0.5;
         return 0;
     }
-    if (c.stretch != 1) { set_error("unknown stretch code %d (0 none, 1 tanh)", c.stretch); return -1; }
-    const double b = (c.beta > 0 ? c.beta : 2.5);
-    for (int j = 0; j < Ny; ++j) {
-        const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
-        y[j] = h * std::tanh(b * e) / std::tanh(b);
-    }
-    for (int j = 0; j < Ny; ++j) {
-        const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
-        const double sech = 1.0 / std::cosh(b * e);
-        a_node[j] = 1.0 / (h * b * (sech * sech) / std::tanh(b));
+    if (c.stretch == 2) {
+        // tabulated y (src/grid.cu:46-78): a = 1 / y_eta with y_eta by differences in eta,
+        // one-sided at the walls, central inside
+        if ((int)c.y_table.size() != Ny) {
+            set_error("stretch 2 (table) needs y_table with Ny = %d values", Ny);
+            return -1;
+        }
+        y = c.y_table;
+        const double deta = 2.0 / (double)(Ny - 1);
+        for (int j = 0; j < Ny; ++j) {
+            double yeta;
+            if (j == 0) yeta = (y[1] - y[0]) / deta;
+            else if (j == Ny - 1) yeta = (y[Ny - 1] - y[Ny - 2]) / deta;
+            else yeta = (y[j + 1] - y[j - 1]) / (2.0 * deta);
+            a_node[j] = 1.0 / yeta;
+        }
+    } else if (c.stretch != 1) {
+        set_error("unknown stretch code %d (0 none, 1 tanh, 2 table)", c.stretch);
+        return -1;
+    } else {
+        const double b = (c.beta > 0 ? c.beta : 2.5);
+        for (int j = 0; j < Ny; ++j) {
+            const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
+            y[j] = h * std::tanh(b * e) / std::tanh(b);
+        }
+        for (int j = 0; j < Ny; ++j) {
+            const double e = -1.0 + 2.0 * (double)j / (double)(Ny - 1);
+            const double sech = 1.0 / std::cosh(b * e);
+            a_node[j] = 1.0 / (h * b * (sech * sech) / std::tanh(b));
+        }
     }
     for (int j = 0; j < Ny - 1; ++j) a_edge[j] = 0.5 * (a_node[j] + a_node[j + 1]);
     for (int j = 0; j < Ny - 1; ++j) dy_edge[j] = y[j + 1] - y[j];
     w_node[0] = 0.5 * dy_edge[0];
     w_node[Ny - 1] = 0.5 * dy_edge[Ny - 2];
     for (int j = 1; j < Ny - 1; ++j) w_node[j] = 0.5 * (dy_edge[j - 1] + dy_edge[j]);
+    return 0;
+}
+
+// the metrics of a context: those of the stretch, or the caller's a_node / a_edge where given
+static int context_metrics(const Config& c, std::vector<double>& y, std::vector<double>& a_node,
+                           std::vector<double>& a_edge, std::vector<double>& dy_edge, std::vector<double>& w_node) {
+    if (build_y_metrics(c, y, a_node, a_edge, dy_edge, w_node)) return -1;
+    if (!c.a_node_in.empty()) {
+        if ((int)c.a_node_in.size() != c.Ny || (int)c.a_edge_in.size() != c.Ny - 1) {
+            set_error("given metrics must have Ny and Ny-1 values");
+            return -1;
+        }
+        a_node = c.a_node_in;
+        a_edge = c.a_edge_in;
+    }
     return 0;
 }
 
@@ -236,7 +271,7 @@ int context_create(const Config& cfg, Context** out) {
     c->cfg = cfg;
     c->Nx = cfg.Nx; c->Ny = cfg.Ny; c->N = (size_t)cfg.Nx * cfg.Ny;
     c->M = cfg.Nx / 2; c->H = c->M + 1; c->Hp = (c->H + 15) / 16 * 16; c->Ni = cfg.Ny - 2;
-    if (build_y_metrics(cfg, c->h_y, c->h_a_node, c->h_a_edge, c->h_dy_edge, c->h_w_node) != 0) { delete c; return -1; }
+    if (context_metrics(cfg, c->h_y, c->h_a_node, c->h_a_edge, c->h_dy_edge, c->h_w_node) != 0) { delete c; return -1; }
     const int Ny = c->Ny;
     c->nu = (cfg.nu_override >= 0 ? cfg.nu_override : (2.0 * cfg.h * cfg.Ub) / cfg.Reb);
     c->dx = cfg.Lx / (double)c->Nx;

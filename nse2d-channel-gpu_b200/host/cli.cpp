@@ -12,10 +12,11 @@
 // time, a statistics step or t_end needs the host (with --profile, one profiled step at a
 // time). dt trimming, the snap to output times and the step counter are the device's.
 //
-// Snapshots are written in the "bin" layout of host/snapshot.h; the reference's HDF5 files
-// (src/io.cu:183-259) need libhdf5, which this build does not link. --snap_fmt h5 therefore
-// falls back to bin with a notice, --init load and --resume read bin snapshots, and --ytable
-// (an HDF5 table) is rejected.
+// Snapshots are the reference's HDF5 files (src/io.cu:183-259, written by host/h5lite without
+// libhdf5): snaps/snap_t%.6f.h5. --snap_fmt bin writes the flat "bin" layout of host/snapshot.h
+// instead (the format the reference declares but never writes), --snap_fmt both writes the two.
+// --init load and --resume read either (src/init.cu:215-279, src/main.cu:129-147), and
+// --stretch table reads y from the HDF5 file of --ytable (src/grid.cu:46-78).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -122,7 +123,7 @@ Args parse(int argc, char** argv) {
         a.ic.amp = a.rand_amp;
     }
     if (a.ic.init == "mms") a.c.mms = 1;                                  // init.cu:95
-    a.c.stretch = (a.stretch == "tanh") ? 1 : 0;
+    a.c.stretch = (a.stretch == "tanh") ? 1 : (a.stretch == "table") ? 2 : 0;
     a.ic.Nx = a.c.Nx; a.ic.Ny = a.c.Ny; a.ic.Lx = a.c.Lx; a.ic.h = a.c.h; a.ic.Ub = a.c.Ub;
     a.ic.mms_A0 = a.c.mms_A0; a.ic.mms_kx = a.c.mms_kx;
     return a;
@@ -214,8 +215,13 @@ bool write_snap(Run& r, double t, std::string& err) {
     if (r.mapped) s.y = r.y;
     ensure_dir(a.outdir + "/snaps");
     std::ostringstream fn;
-    fn << a.outdir << "/snaps/snap_t" << std::fixed << std::setprecision(6) << t << ".bin";
-    return nse2d_host::write_snapshot(fn.str(), s, err);
+    fn << a.outdir << "/snaps/snap_t" << std::fixed << std::setprecision(6) << t;
+    // the reference maps every --snap_fmt value to HDF5 (src/main.cu:126-127); bin and both are this
+    // build's additions
+    const bool bin = a.snap_fmt == "bin" || a.snap_fmt == "both", h5 = a.snap_fmt != "bin";
+    if (h5 && !nse2d_host::write_snapshot_h5(fn.str() + ".h5", s, err)) return false;
+    if (bin && !nse2d_host::write_snapshot(fn.str() + ".bin", s, err)) return false;
+    return true;
 }
 
 void write_row(const std::string& path, long long step, double t, double dt, const double* v, bool closure) {
@@ -283,13 +289,18 @@ int main(int argc, char** argv) {
     if (prog.size() >= 8 && prog.find("freeslip") != std::string::npos) a.c.free_slip = 1;
     ensure_dir(a.outdir);
     Log LOGP(a.outdir + "/progress.log");
-    if (!a.ytable.empty()) {
-        std::fprintf(stderr, "nse2d: --ytable reads an HDF5 table; this build has no HDF5\n");
+    std::vector<double> ytab;
+    if (a.stretch == "table") {                                                 // grid.cu:46-78
+        std::string terr;
+        if (a.ytable.empty()) { std::fprintf(stderr, "nse2d: --ytable required for --stretch table\n"); return 1; }
+        if (!nse2d_host::read_y_table(a.ytable, a.c.Ny, ytab, terr)) {
+            std::fprintf(stderr, "nse2d: %s: %s\n", a.ytable.c_str(), terr.c_str());
+            return 1;
+        }
+        a.c.y_table = ytab.data();
+    } else if (a.stretch != "none" && a.stretch != "uniform" && a.stretch != "tanh") {
+        std::fprintf(stderr, "nse2d: Unknown --stretch '%s'\n", a.stretch.c_str());
         return 1;
-    }
-    if (a.snap_fmt != "bin") {
-        LOGP("[io] snapshot format '%s' is not built (no HDF5); writing the bin format\n", a.snap_fmt.c_str());
-        a.snap_fmt = "bin";
     }
     if (nse2d_create(&a.c, &r.ctx)) return fail("configuration");
     r.Nx = a.c.Nx; r.Ny = a.c.Ny;
@@ -308,7 +319,7 @@ int main(int argc, char** argv) {
     std::string err;
     if (a.ic.init == "load" || a.resume) {
         if (a.load_path.empty()) {
-            std::fprintf(stderr, "nse2d: %s needs --load_path /path/to/snap_tXXXXXX.bin\n",
+            std::fprintf(stderr, "nse2d: %s needs --load_path /path/to/snap_tXXXXXX.h5\n",
                          a.resume ? "--resume" : "--init load");
             return 1;
         }

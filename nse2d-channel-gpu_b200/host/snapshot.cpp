@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <cstring>
 
+#include "h5lite.h"
+
 namespace nse2d_host {
 
 const std::vector<double>* Snapshot::field(const std::string& name) const {
@@ -34,7 +36,102 @@ bool write_snapshot(const std::string& path, const Snapshot& s, std::string& err
     return ok;
 }
 
+// The reference's HDF5 layout (src/io.cu:226-256): the fields, y with beta and stretch_code on a
+// stretched grid, then the scalar attributes in the reference's order.
+bool write_snapshot_h5(const std::string& path, const Snapshot& s, std::string& err) {
+    const size_t N = (size_t)s.Nx * s.Ny;
+    std::vector<h5lite::WriteDataset> ds;
+    for (size_t q = 0; q < s.fields.size(); ++q) {
+        if (s.fields[q].size() != N) { err = "snapshot field " + s.names[q] + " has the wrong size"; return false; }
+        ds.push_back({s.names[q], {(uint64_t)s.Ny, (uint64_t)s.Nx}, s.fields[q].data()});
+    }
+    std::vector<h5lite::WriteAttr> at;
+    auto dbl = [&](const char* n, double v) { h5lite::WriteAttr a; a.name = n; a.d = v; at.push_back(a); };
+    auto i32 = [&](const char* n, int v) { h5lite::WriteAttr a; a.name = n; a.is_int = true; a.i = v; at.push_back(a); };
+    if (s.tanh && s.beta > 0.0 && !s.y.empty()) {
+        ds.push_back({"y", {1, (uint64_t)s.Ny}, s.y.data()});
+        dbl("beta", s.beta);
+        dbl("stretch_code", 1.0);
+    }
+    dbl("t", s.t);
+    i32("Nx", s.Nx);
+    i32("Ny", s.Ny);
+    dbl("Lx", s.Lx);
+    dbl("Ly", 2.0 * s.h);
+    dbl("h", s.h);
+    dbl("dx", s.Lx / (double)s.Nx);
+    dbl("dy", (2.0 * s.h) / (double)(s.Ny - 1));
+    dbl("nu", s.nu);
+    return h5lite::write_file(path, ds, at, err);
+}
+
+static bool is_hdf5(const std::string& path) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    unsigned char m[8] = {0};
+    const bool ok = std::fread(m, 1, 8, f) == 8 && m[0] == 0x89 && std::memcmp(m + 1, "HDF\r\n\x1a\n", 7) == 0;
+    std::fclose(f);
+    return ok;
+}
+
+// src/init.cu:215-279: attributes Nx, Ny, Lx, h, nu, t; omega and psi as [Ny][Nx] or [Nx][Ny]
+static bool read_snapshot_h5(const std::string& path, Snapshot& s, std::string& err) {
+    h5lite::File f;
+    if (!f.open(path, err)) return false;
+    double v = 0;
+    s.Nx = f.attr("Nx", v) ? (int)v : -1;
+    s.Ny = f.attr("Ny", v) ? (int)v : -1;
+    s.Lx = f.attr("Lx", v) ? v : -1.0;
+    s.h = f.attr("h", v) ? v : -1.0;
+    s.nu = f.attr("nu", v) ? v : 0.0;
+    s.t = f.attr("t", v) ? v : 0.0;
+    s.beta = f.attr("beta", v) ? v : 0.0;
+    s.tanh = f.attr("stretch_code", v) && v == 1.0;
+    if (s.Nx <= 0 || s.Ny <= 1) { err = path + ": no Nx / Ny attributes"; return false; }
+    s.names.clear();
+    s.fields.clear();
+    for (const char* name : {"omega", "psi", "u", "v"}) {
+        if (!f.has(name)) continue;
+        std::vector<uint64_t> dims;
+        std::vector<double> a;
+        if (!f.read(name, dims, a, err)) return false;
+        const uint64_t Nx = (uint64_t)s.Nx, Ny = (uint64_t)s.Ny;
+        if (dims.size() == 2 && dims[0] == Ny && dims[1] == Nx) {
+            s.fields.push_back(std::move(a));
+        } else if (dims.size() == 2 && dims[0] == Nx && dims[1] == Ny) {      // stored [Nx][Ny]
+            std::vector<double> b(a.size());
+            for (uint64_t j = 0; j < Ny; ++j)
+                for (uint64_t i = 0; i < Nx; ++i) b[j * Nx + i] = a[i * Ny + j];
+            s.fields.push_back(std::move(b));
+        } else {
+            err = path + ": dataset " + name + " does not have the grid's shape";
+            return false;
+        }
+        s.names.push_back(name);
+    }
+    s.y.clear();
+    if (f.has("y")) {
+        std::vector<uint64_t> dims;
+        if (!f.read("y", dims, s.y, err)) return false;
+        if ((int)s.y.size() != s.Ny) s.y.clear();
+    }
+    return true;
+}
+
+bool read_y_table(const std::string& path, int Ny, std::vector<double>& y, std::string& err) {
+    h5lite::File f;
+    if (!f.open(path, err)) return false;
+    if (!f.has("y")) { err = "--ytable missing dataset /y"; return false; }
+    std::vector<uint64_t> dims;
+    if (!f.read("y", dims, y, err)) return false;
+    const bool col = dims.size() == 2 && dims[0] == (uint64_t)Ny && dims[1] == 1;
+    const bool row = dims.size() == 2 && dims[0] == 1 && dims[1] == (uint64_t)Ny;
+    if (!col && !row) { err = "--ytable: could not read /y array"; return false; }
+    return true;
+}
+
 bool read_snapshot(const std::string& path, Snapshot& s, std::string& err) {
+    if (is_hdf5(path)) return read_snapshot_h5(path, s, err);
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) { err = "cannot open snapshot " + path; return false; }
     char magic[8];

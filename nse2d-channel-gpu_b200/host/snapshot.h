@@ -1,7 +1,14 @@
-// Binary snapshot files (the "bin" format): the fields and metadata of the reference's HDF5
-// snapshots (src/io.cu:183-259) in a flat little-endian layout, written and read without
-// libhdf5. The reference declares a bin format (SNAP_BIN, src/io.cuh:28) but never writes one;
-// this is the layout used here and by the CPU oracle:
+// Snapshot files.
+//
+// HDF5 (the reference's format, src/io.cu:183-259, written with this project's h5lite): root
+// group datasets omega, psi (--snap_fields all / omega_psi), u, v (all), each [Ny][Nx] float64;
+// y [1][Ny] float64 with root attributes beta and stretch_code (1 tanh) when the grid is
+// stretched; root attributes t, Nx, Ny (32-bit integers), Lx, Ly, h, dx, dy, nu (float64). Read
+// back as the reference reads it (src/init.cu:215-279): omega or psi, [Ny][Nx] or its transpose.
+//
+// "bin": the same fields and metadata in a flat little-endian layout. The reference declares a
+// bin format (SNAP_BIN, src/io.cuh:28) but never writes one; this is the layout used here and by
+// the CPU oracle:
 //
 //   char[8]    "NSE2DSNP"
 //   int32[4]   version (1), Nx, Ny, number of fields F
@@ -25,7 +32,11 @@ struct Snapshot {
     const std::vector<double>* field(const std::string& name) const;
 };
 
-bool write_snapshot(const std::string& path, const Snapshot& s, std::string& err);
+bool write_snapshot(const std::string& path, const Snapshot& s, std::string& err);      // bin
+bool write_snapshot_h5(const std::string& path, const Snapshot& s, std::string& err);   // HDF5
+// either format (told apart by the file's signature)
 bool read_snapshot(const std::string& path, Snapshot& s, std::string& err);
+// the dataset "y" of an HDF5 file as a vector of Ny values ([Ny][1] or [1][Ny]): --ytable
+bool read_y_table(const std::string& path, int Ny, std::vector<double>& y, std::string& err);
 
 }  // namespace nse2d_host

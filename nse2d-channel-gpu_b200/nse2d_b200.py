@@ -39,7 +39,14 @@ class Config(ctypes.Structure):
                 ("nforce", ctypes.c_int), ("lin_drag", ctypes.c_double), ("free_slip", ctypes.c_int),
                 ("mms", ctypes.c_int), ("mms_A0", ctypes.c_double), ("mms_eps", ctypes.c_double),
                 ("mms_Om", ctypes.c_double), ("mms_kx", ctypes.c_int), ("closure_diag", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("y_table", ctypes.c_void_p)]
+
+
+class SnapshotMeta(ctypes.Structure):
+    """struct nse2d_snapshot_meta: the grid and the scalar attributes of a snapshot file."""
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("t", ctypes.c_double), ("Lx", ctypes.c_double),
+                ("h", ctypes.c_double), ("nu", ctypes.c_double), ("beta", ctypes.c_double),
+                ("stretch_tanh", ctypes.c_int), ("y", ctypes.c_void_p), ("fields", ctypes.c_int)]
 
 
 _lib = None
@@ -113,6 +120,8 @@ def load(path=LIB_PATH):
         "nse2d_cnn_gradients": (I, [P, P, P, P, P, P, P, I, P, P]),
         "nse2d_cnn_train_step": (I, [P, P, P, P, P, P, P, I, ctypes.c_float, ctypes.c_float, P, P]),
         "nse2d_set_closure": (I, [P, P, I]),
+        "nse2d_snapshot_write": (I, [ctypes.c_char_p, I, ctypes.POINTER(SnapshotMeta), I, P, P]),
+        "nse2d_snapshot_read": (I, [ctypes.c_char_p, ctypes.POINTER(SnapshotMeta), ctypes.c_char_p, P]),
         "nse2d_last_error": (ctypes.c_char_p, []),
         "nse2d_set_abort_on_error": (V, [I]),
         "nse2d_testapi_set_free_slip": (V, [I]),
@@ -146,7 +155,11 @@ def default_config(**kw):
     load().nse2d_config_default(ctypes.byref(cfg))
     for k, v in kw.items():
         if k == "stretch" and isinstance(v, str):
-            v = {"none": 0, "uniform": 0, "tanh": 1}[v]
+            v = {"none": 0, "uniform": 0, "tanh": 1, "table": 2}[v]
+        if k == "y_table":
+            # kept alive with the Config: nse2d_create copies it
+            cfg._y_table = np.ascontiguousarray(v, dtype=np.float64)
+            v = cfg._y_table.ctypes.data
         setattr(cfg, k, v)
     return cfg
 
@@ -179,6 +192,40 @@ def max_uv_noalloc(psi_dev, a_node_dev, Nx, Ny, inv_dx, inv_deta, stream=None):
     _check(load().nse2d_max_uv_noalloc(dev(psi_dev), dev(a_node_dev), int(Nx), int(Ny), float(inv_dx),
                                        float(inv_deta), out, _stream(stream)))
     return tuple(out)
+
+
+def write_snapshot(path, fields, t, Lx, h, nu, beta=0.0, y=None, fmt="h5"):
+    """Write a snapshot file: fields = {name: [Ny, Nx] float64 array} (omega, psi, u, v), in the
+    reference's HDF5 layout (fmt "h5") or the flat bin layout ("bin"); y (with beta > 0) marks a
+    tanh grid and is stored with its attributes."""
+    names = list(fields)
+    arrs = [np.ascontiguousarray(fields[k], dtype=np.float64) for k in names]
+    Ny, Nx = arrs[0].shape
+    m = SnapshotMeta(Nx=Nx, Ny=Ny, t=t, Lx=Lx, h=h, nu=nu, beta=beta, stretch_tanh=1 if y is not None else 0)
+    yy = None
+    if y is not None:
+        yy = np.ascontiguousarray(y, dtype=np.float64)
+        m.y = yy.ctypes.data
+    cn = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+    cf = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    _check(load().nse2d_snapshot_write(str(path).encode(), 0 if fmt == "h5" else 1, ctypes.byref(m), len(names),
+                                       ctypes.cast(cn, ctypes.c_void_p), ctypes.cast(cf, ctypes.c_void_p)))
+
+
+def read_snapshot(path):
+    """(meta dict, {name: array}) of a snapshot file of either format: every field present, [Ny, Nx],
+    and y when stored."""
+    m = SnapshotMeta()
+    L = load()
+    _check(L.nse2d_snapshot_read(str(path).encode(), ctypes.byref(m), None, None))
+    meta = {k: getattr(m, k) for k in ("Nx", "Ny", "t", "Lx", "h", "nu", "beta", "stretch_tanh")}
+    out = {}
+    for bit, name in ((1, "omega"), (2, "psi"), (4, "u"), (8, "v"), (16, "y")):
+        if m.fields & bit:
+            a = np.empty(m.Ny if name == "y" else (m.Ny, m.Nx))
+            _check(L.nse2d_snapshot_read(str(path).encode(), None, name.encode(), a.ctypes.data_as(ctypes.c_void_p)))
+            out[name] = a
+    return meta, out
 
 
 def gemm_bf16(A, B, bias=None, relu=False, out_f32=True, out_bf16=False, stream=None):

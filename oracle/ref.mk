@@ -7,6 +7,8 @@
 #   _ref/nse2d_ref_freeslip  the same with -DFREE_SLIP_WALLS (its WALLS=freeslip build)
 #   _ref/libnse2d_ref.so     the operators and the C-linkage test API (-DEXPORT_TEST_API
 #                            -DNSE2D_BUILD_AS_LIB, src/test_api.cu)
+#   _ref/libnse2d_refloop.so the reference's time loop driven through its own launchers
+#                            (ref_loop.cu, this directory), for field parity on seeded inputs
 # make -f ref.mk REF=/path/to/reference; without REF: $(NSE2D_REFERENCE_DIR), else the directory
 # "reference" beside this repository
 REF   ?= $(if $(NSE2D_REFERENCE_DIR),$(NSE2D_REFERENCE_DIR),$(abspath $(CURDIR)/../../reference))
@@ -16,7 +18,7 @@ SRCS  := $(addprefix $(REF)/src/,io.cu grid.cu ops.cu diag.cu poisson.cu init.cu
 FLAGS := --extended-lambda -O3 -use_fast_math -lineinfo -std=c++17 -gencode arch=compute_100a,code=sm_100a -DNO_HDF5
 LIBS  := -lcufft
 
-all: $(OUT)/nse2d_ref $(OUT)/nse2d_ref_freeslip $(OUT)/libnse2d_ref.so
+all: $(OUT)/nse2d_ref $(OUT)/nse2d_ref_freeslip $(OUT)/libnse2d_ref.so $(OUT)/libnse2d_refloop.so
 
 $(OUT):
 	mkdir -p $(OUT)
@@ -29,5 +31,8 @@ $(OUT)/nse2d_ref_freeslip: $(SRCS) | $(OUT)
 
 $(OUT)/libnse2d_ref.so: $(SRCS) $(REF)/src/test_api.cu | $(OUT)
 	$(NVCC) $(FLAGS) -DEXPORT_TEST_API -DNSE2D_BUILD_AS_LIB -Xcompiler -fPIC -shared $(SRCS) $(REF)/src/test_api.cu $(LIBS) -o $@
+
+$(OUT)/libnse2d_refloop.so: ref_loop.cu $(SRCS) | $(OUT)
+	$(NVCC) $(FLAGS) -DNSE2D_BUILD_AS_LIB -I$(REF)/src -Xcompiler -fPIC -shared ref_loop.cu $(SRCS) $(LIBS) -o $@
 
 .PHONY: all

@@ -12,6 +12,21 @@ machine that runs the tests).
    the column's scale (columns such as dOmega_rhs are small differences of O(1) sums), or 1e-13
    absolute for columns that are round-off in both (tau_w at Ub = 0). The two
    differ only by the order of the reductions and the FFT (cuFFT there, this project's here).
+3. Fields against the reference's own time loop (oracle/_ref/libnse2d_refloop.so: the
+   reference's src/main.cu:197-213 and 434-541 driven through its own launchers, built from its
+   sources by oracle/ref.mk), from the same seeded initial vorticity. The small-channel
+   configuration (256 x 257, Lx = 2 pi, tanh beta = 2, Ub = 1, Re_b = 500, Poiseuille plus a
+   seed-0 Gaussian perturbation of 1e-3 of the wall vorticity, zero at the walls, no forcing):
+   - one step at dt = 1e-3 (as configured) and at 1e-4: psi, and omega away from the walls,
+     within 1e-11 relative to the field's maximum;
+   - 1000 steps at dt = 1e-4: within 1e-8;
+   - 1000 steps at dt = 1e-3 as configured: the step lies beyond the stability limit of SSPRK(3,3)
+     for the mapped Laplacian on this grid (nu dt lambda_min = -9.7 against -2.51), so both builds
+     blow up; both must reach non-finite values within two steps of each other.
+   The wall rows are the Thom closure's (thom_gain ~1.5e6 times the round-off of psi at rows 1-2),
+   held as in the oracle parity tests. An adaptive forced channel (512 x 257, Re_b 5000, F0 0.05 at
+   mode 12, drag 1e-3) is stepped 20 times in both: dt of every step within 1e-12, fields within
+   1e-10.
 """
 import ctypes
 import os
@@ -20,7 +35,8 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ORACLE, PKG
+from conftest import ORACLE, PKG, load_oracle_module
+from test_parity_gpu import assert_fields_close, laminar_perturbed, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -116,6 +132,9 @@ CASES = {
             "--dt", "0.000125", "--tend", "0.25", "--diag_save", "0.05"],
     "poiseuille": ["--Nx", "64", "--Ny", "129", "--Ub", "1.0", "--Reb", "500.0", "--init", "laminar", "--stretch",
                    "tanh", "--beta", "2", "--tend", "1.0", "--diag_save", "0.25"],
+    "diffusion2d": ["--Nx", "64", "--Ny", "65", "--Ub", "0", "--nu", "0.01", "--init", "diffusion2d", "--amp", "0.5",
+                    "--my", "2", "--stretch", "none", "--no-adapt", "--dt", "0.001", "--tend", "0.1",
+                    "--diag_save", "0.025"],
 }
 
 
@@ -144,3 +163,98 @@ def test_runs_match_reference_executable(cuda, tmp_path, case):
         # a column that is round-off in both (e.g. tau_w of a flow with Ub = 0) is held to 1e-13
         tol = 1e-8 * np.abs(r[fin]) + max(2e-9 * scale, 1e-13)
         assert np.all(err <= tol), (name, float(np.max(err)), scale)
+
+
+refloop = load_oracle_module("ref_loop")
+need_loop = pytest.mark.skipif(not refloop.available(),
+                               reason="the reference's loop harness was not compiled here (oracle/ref.mk)")
+SMALL = dict(Nx=256, Ny=257, Lx=2 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, Reb=500.0, adapt=0)
+
+
+def _both(nse, dt, **kw):
+    cfg = dict(SMALL, dt_init=dt, **kw)
+    g = nse.Solver(**cfg)
+    r = refloop.RefLoop(**cfg)
+    w0 = laminar_perturbed(cfg["Nx"], cfg["Ny"], g.metric(0), seed=0, amp=1e-3)
+    g.set_omega(w0)
+    r.set_omega(w0)
+    return g, r
+
+
+@need_loop
+@pytest.mark.parametrize("dt", [1e-3, 1e-4])
+def test_small_channel_one_step_matches_reference_loop(nse, cuda, dt):
+    g, r = _both(nse, dt)
+    wg, pg = g.fields()
+    wr, pr = r.fields()
+    assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-12)          # the initial solve and closure
+    g.step(1)
+    r.step(1)
+    wg, pg = g.fields()
+    wr, pr = r.fields()
+    assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-11)
+    print(f"dt={dt:g}: one step, psi {relerr(pg, pr):.2e}, omega rows 2..Ny-3 "
+          f"{np.max(np.abs(wg[2:-2] - wr[2:-2])) / np.max(np.abs(wr)):.2e}")
+    g.close()
+    r.close()
+
+
+@need_loop
+def test_small_channel_1000_steps_matches_reference_loop(nse, cuda):
+    g, r = _both(nse, 1e-4)
+    g.step(1000, use_graph=True)
+    r.step(1000)
+    wg, pg = g.fields()
+    wr, pr = r.fields()
+    assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-8)
+    assert abs(g.time()[0] - r.time()[0]) < 1e-15
+    print(f"1000 steps at dt=1e-4: psi {relerr(pg, pr):.2e}, omega {relerr(wg, wr):.2e}")
+    g.close()
+    r.close()
+
+
+@need_loop
+def test_small_channel_as_configured_blows_up_in_both(nse, cuda):
+    """dt = 1e-3 for up to 1000 steps: the first step with a non-finite omega in each build."""
+    g, r = _both(nse, 1e-3)
+    first = {}
+    for n in range(1, 1001):
+        if "ours" not in first:
+            g.step(1)
+            if not np.all(np.isfinite(g.fields()[0])):
+                first["ours"] = n
+        if "reference" not in first:
+            r.step(1)
+            if not np.all(np.isfinite(r.fields()[0])):
+                first["reference"] = n
+        if len(first) == 2:
+            break
+    print(f"dt=1e-3: first non-finite omega at step {first.get('ours')} (this build), "
+          f"{first.get('reference')} (the reference's loop)")
+    assert len(first) == 2, first
+    assert abs(first["ours"] - first["reference"]) <= 2, first
+    g.close()
+    r.close()
+
+
+@need_loop
+def test_adaptive_forced_channel_matches_reference_loop(nse, cuda):
+    cfg = dict(Nx=512, Ny=257, Lx=4.0 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, Reb=5000.0, F0=0.05, nforce=12,
+               lin_drag=1e-3, adapt=1, cfl=0.5, dt_max=1e-2, dt_init=1e-3)
+    g = nse.Solver(**cfg)
+    r = refloop.RefLoop(**cfg)
+    w0 = laminar_perturbed(512, 257, g.metric(0), seed=4, amp=5e-2)
+    g.set_omega(w0)
+    r.set_omega(w0)
+    for n in range(20):
+        g.step(1)
+        r.step(1)
+        tg, dtg = g.time()[:2]
+        tr, dtr = r.time()[:2]
+        assert abs(dtg - dtr) <= 1e-12 * dtr, (n, dtg, dtr)
+        assert abs(tg - tr) <= 1e-12 * tr, (n, tg, tr)
+    wg, pg = g.fields()
+    wr, pr = r.fields()
+    assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-10)
+    g.close()
+    r.close()
