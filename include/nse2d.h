@@ -176,6 +176,17 @@ int  nse2d_run(nse2d_ctx* ctx, double next_snap, double next_diag, int stats_eve
 /* Row sums over x of u, v, u^2, v^2 and u v of the current psi (src/diag.cu:468-499), neighbours
  * clamped at the walls: out5 = [5][Ny] host array. Synchronous. */
 int  nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s);
+/* The time-weighted statistics of the reference's loop (src/main.cu:695-733) kept on the device:
+ * with every > 0, every `every` steps of nse2d_run (the step count a multiple of every) the row
+ * means over x of u, v, u^2, v^2, u v of that step's psi, weighted by the time since the last
+ * sample, are added to an accumulator inside the run's graph, so that statistics need no halt of
+ * the run (its stats_every argument may then be 0). The accumulator starts at zero and the clock
+ * at the current t with this call; every = 0 turns it off. Setting a new state (nse2d_set_omega /
+ * nse2d_set_state) turns it off. Precision 64 only. Synchronous. */
+int  nse2d_stats_device(nse2d_ctx* ctx, int every, cudaStream_t s);
+/* The accumulated statistics: out5 = [5][Ny] (the sums H[q][j] of the reference's loop; either
+ * output may be NULL) and the total weight T (profiles = H / T). Synchronous. */
+int  nse2d_stats_read(nse2d_ctx* ctx, double* out5, double* T, cudaStream_t s);
 /* Add one sample of the 1-D spectra E_u(k), E_v(k) of the current psi (src/diag.cuh:123-191,
  * src/diag.cu:868-898), with the project's own row FFT. Overwrites the stage buffers (fields 2
  * and 3); call between steps. */

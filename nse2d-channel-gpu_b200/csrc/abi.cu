@@ -250,6 +250,16 @@ int nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s) {
     return row_moments(ctx->c, out5, s);
 }
 
+int nse2d_stats_device(nse2d_ctx* ctx, int every, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return stats_device(ctx->c, every, s);
+}
+
+int nse2d_stats_read(nse2d_ctx* ctx, double* out5, double* T, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    return stats_read(ctx->c, out5, T, s);
+}
+
 int nse2d_spectra_accumulate(nse2d_ctx* ctx, cudaStream_t s) {
     CHECK_CTX(ctx);
     SYNC_FP64(ctx, false, s);

@@ -64,6 +64,10 @@ struct Ctl {
     unsigned long long mx_acc[3];  // max reduction: atomic maxima of |u|, |v|, |v| a (bit patterns; 0 between launches)
     int nonfinite;                 // bit 0: a reduction saw NaN/Inf; bit 1: a bounded wait timed out
     int nonfinite_halted;          // a run has already halted for bit 0 (it halts once for it)
+    // statistics on the device (nse2d_stats_device): every acc_every steps of a run, the row
+    // moments weighted by t - acc_last_t are added to the context's accumulator
+    int acc_every;
+    double acc_last_t, acc_T;
     // run mode (nse2d_run): stop stepping when an output, a statistics step or the end is due
     int run;                       // 1 while a run is active
     int halt;                      // set at the end of the step after which the run stops
@@ -166,6 +170,8 @@ struct Context {
     cudaGraphExec_t run_exec = nullptr;    // WHILE(no halt) { step } for nse2d_run
     double* spec_acc = nullptr;            // [2][Hp] accumulated E_u, E_v of the 1-D spectra
     double* moments = nullptr;             // [5][Ny] row sums of u, v, u^2, v^2, u v
+    double* stats_acc = nullptr;           // [5][Ny] time-weighted row means (statistics on the device)
+    bool stats_dev = false;                // the run graph accumulates the statistics
     int spec_samples = 0;
     bool closure_diag = false;
 };

@@ -5,6 +5,7 @@
 // so its last digits depend on block scheduling. Here every row is reduced by one CTA into
 // per-row partials (fixed tree order), and the rows are then summed in row order with a
 // compensated (Neumaier) sum: the result is deterministic and at least as accurate.
+#include <cstddef>
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -239,9 +240,19 @@ int diagnostics_row(Context* c, int t0_row, double* o, cudaStream_t s) {
 // One CTA per row (grid-stride over rows); u and v as the reference forms them, with the
 // neighbouring rows clamped at the walls; a fixed-order reduction, so the sums are
 // deterministic.
+// ACC: the time-weighted statistics of the run loop (src/main.cu:695-733) on the device: at a step
+// that is a multiple of ctl->acc_every, with dtw = t - acc_last_t > 0, out[q][j] += (sum / Nx) dtw,
+// the host's accumulation of the same row sums; other steps return at once.
+template <bool ACC>
 static __global__ void __launch_bounds__(256) k_row_moments(const double* __restrict__ psi, const double* __restrict__ a_node,
                                                            int Nx, int Ny, double inv_dx, double inv_deta,
-                                                           double* __restrict__ out) {
+                                                           double* __restrict__ out, const Ctl* __restrict__ ctl) {
+    double dtw = 0.0;
+    if constexpr (ACC) {
+        if (ctl->acc_every <= 0 || ctl->step % ctl->acc_every != 0) return;
+        dtw = ctl->t - ctl->acc_last_t;
+        if (!(dtw > 0.0)) return;
+    }
     __shared__ double red[5][8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int iy = blockIdx.x; iy < Ny; iy += gridDim.x) {
@@ -264,7 +275,8 @@ static __global__ void __launch_bounds__(256) k_row_moments(const double* __rest
         if (threadIdx.x < 5) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
-            out[(size_t)threadIdx.x * Ny + iy] = t;
+            if constexpr (ACC) out[(size_t)threadIdx.x * Ny + iy] += t / (double)Nx * dtw;
+            else out[(size_t)threadIdx.x * Ny + iy] = t;
         }
         __syncthreads();
     }
@@ -275,10 +287,74 @@ int row_moments(Context* c, double* out5, cudaStream_t s) {
         NSE_CUDA_TRY(cudaMalloc((void**)&c->moments, sizeof(double) * 5 * (size_t)c->Ny));
     }
     const int grid = std::min(c->Ny, 8 * c->num_sms);
-    k_row_moments<<<grid, 256, 0, s>>>(c->psi, c->rt.a_node, c->Nx, c->Ny, c->inv_dx, c->inv_deta, c->moments);
+    k_row_moments<false><<<grid, 256, 0, s>>>(c->psi, c->rt.a_node, c->Nx, c->Ny, c->inv_dx, c->inv_deta, c->moments,
+                                              c->ctl);
     NSE_CUDA_TRY(cudaGetLastError());
     NSE_CUDA_TRY(cudaMemcpyAsync(out5, c->moments, sizeof(double) * 5 * (size_t)c->Ny, cudaMemcpyDeviceToHost, s));
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// after the accumulation of a statistics step: the weight and the time of the last sample
+static __global__ void k_stats_commit(Ctl* ctl) {
+    if (threadIdx.x != 0 || ctl->acc_every <= 0 || ctl->step % ctl->acc_every != 0) return;
+    const double dtw = ctl->t - ctl->acc_last_t;
+    if (!(dtw > 0.0)) return;
+    ctl->acc_T += dtw;
+    ctl->acc_last_t = ctl->t;
+}
+
+// The statistics kernels of one step of the run loop (they return at once except at a
+// statistics step); the accumulator must exist (stats_device).
+int enqueue_stats(Context* c, cudaStream_t s) {
+    const int grid = std::min(c->Ny, 8 * c->num_sms);
+    k_row_moments<true><<<grid, 256, 0, s>>>(c->psi, c->rt.a_node, c->Nx, c->Ny, c->inv_dx, c->inv_deta, c->stats_acc,
+                                             c->ctl);
+    NSE_CUDA_TRY(cudaGetLastError());
+    k_stats_commit<<<1, 32, 0, s>>>(c->ctl);
+    NSE_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Accumulate on the device every `every` steps of the run loop (0: off), from now on: the
+// accumulators start at zero and the clock at the current t.
+int stats_device(Context* c, int every, cudaStream_t s) {
+    if (every < 0) { set_error("nse2d_stats_device: every must be >= 0"); return -1; }
+    if (every > 0 && c->prec32) {
+        set_error("nse2d_stats_device: statistics on the device need precision 64");
+        return -1;
+    }
+    if (every > 0 && !c->stats_acc) NSE_CUDA_TRY(cudaMalloc((void**)&c->stats_acc, sizeof(double) * 5 * (size_t)c->Ny));
+    if (c->stats_acc) NSE_CUDA_TRY(cudaMemsetAsync(c->stats_acc, 0, sizeof(double) * 5 * (size_t)c->Ny, s));
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->h_ctl, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    Ctl* h = c->h_ctl;
+    h->acc_every = every;
+    h->acc_last_t = h->t;
+    h->acc_T = 0.0;
+    const size_t off = offsetof(Ctl, acc_every), len = offsetof(Ctl, acc_T) + sizeof(double) - off;
+    NSE_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c->ctl) + off, reinterpret_cast<char*>(h) + off, len,
+                                 cudaMemcpyHostToDevice, s));
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    const bool on = every > 0;
+    if (on != c->stats_dev) {
+        // the run graph holds the statistics kernels only when they are on: capture it again
+        if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
+        c->stats_dev = on;
+    }
+    return 0;
+}
+
+int stats_read(Context* c, double* out5, double* T, cudaStream_t s) {
+    NSE_CUDA_TRY(cudaMemcpyAsync(c->h_ctl, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    if (out5) {
+        if (c->stats_acc)
+            NSE_CUDA_TRY(cudaMemcpyAsync(out5, c->stats_acc, sizeof(double) * 5 * (size_t)c->Ny, cudaMemcpyDeviceToHost, s));
+        else
+            for (size_t k = 0; k < 5 * (size_t)c->Ny; ++k) out5[k] = 0.0;
+    }
+    NSE_CUDA_TRY(cudaStreamSynchronize(s));
+    if (T) *T = c->h_ctl->acc_T;
     return 0;
 }
 
@@ -298,8 +374,6 @@ static __global__ void k_spectra_reduce(const cpx<double>* __restrict__ hat, int
     acc[k] += norm * wx * sum;
 }
 
-// One spectra sample of the current psi: u and v (into the stage buffers, free between steps),
-// the row transforms of each (into the spectral buffer), and the row reduction.
 // One sample of E_u, E_v from device u, v [Ny][Nx] (16-byte aligned): the row transforms of the
 // spectral buffer, then the sums over rows of |X_k|^2 (src/diag.cu:868-898).
 int spectra_accumulate_uv(Context* c, const double* u, const double* v, cudaStream_t s) {
@@ -319,6 +393,7 @@ int spectra_accumulate_uv(Context* c, const double* u, const double* v, cudaStre
     return 0;
 }
 
+// One spectra sample of the current psi: u and v into the stage buffers (free between steps).
 int spectra_accumulate(Context* c, cudaStream_t s) {
     if (uv_from_psi(c, c->psi, c->w1, c->w2, s)) return -1;
     return spectra_accumulate_uv(c, c->w1, c->w2, s);

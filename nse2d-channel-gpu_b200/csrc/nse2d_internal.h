@@ -51,6 +51,9 @@ int launch_fft_all_rows(Context* c, const double* src, cudaStream_t s);
 int run_until_halt(Context* c, cudaStream_t s);
 int row_moments(Context* c, double* out5, cudaStream_t s);
 int spectra_accumulate(Context* c, cudaStream_t s);
+int enqueue_stats(Context* c, cudaStream_t s);
+int stats_device(Context* c, int every, cudaStream_t s);
+int stats_read(Context* c, double* out5, double* T, cudaStream_t s);
 int spectra_accumulate_uv(Context* c, const double* u, const double* v, cudaStream_t s);
 // after a launch of the reference-compatible operators (ops.cu): keep a CUDA error for
 // nse2d_last_error and, unless nse2d_set_abort_on_error(0), print it and abort as the reference does

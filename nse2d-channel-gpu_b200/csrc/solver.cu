@@ -475,6 +475,7 @@ void context_destroy(Context* c) {
     destroy32(c);
     if (c->spec_acc) cudaFree(c->spec_acc);
     if (c->moments) cudaFree(c->moments);
+    if (c->stats_acc) cudaFree(c->stats_acc);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
@@ -818,6 +819,7 @@ int run_until_halt(Context* c, cudaStream_t s) {
         if (e != cudaSuccess) return fail("capture", e);
         // the step stores its stage-3 rhs, which the diagnostics row after a run pairs with omega
         int rc = enqueue_step(c, c->cap_stream, true);
+        if (rc == 0 && c->stats_dev) rc = enqueue_stats(c, c->cap_stream);
         if (rc == 0) k_loop_cond<<<1, 32, 0, c->cap_stream>>>(c->ctl, h);
         cudaGraph_t captured = nullptr;
         e = cudaStreamEndCapture(c->cap_stream, &captured);

@@ -384,9 +384,22 @@ int main(int argc, char** argv) {
     for (auto& v : H) v.assign(r.Ny, 0.0);
     std::vector<double> mom(5 * (size_t)r.Ny);
     double tauw_abs_dt_sum = 0.0, T_diag = 0.0, last_diag_t = t_start, T_accum = 0.0, last_stats_t = t_start;
-    // steps at which the host must look: statistics and spectra
-    int every = std::max(1, a.statsEvery);
-    if (a.spectraEvery > 0) every = std::gcd(every, a.spectraEvery);
+    // the time-weighted statistics accumulate on the device inside the run's graph (precision 64,
+    // not with --profile); the run then halts only where the host must write rolling profiles or
+    // take a spectra sample
+    const bool dev_stats = a.statsEvery > 0 && a.c.precision == 64 && !a.profile;
+    if (dev_stats && nse2d_stats_device(r.ctx, a.statsEvery, nullptr)) return fail("statistics");
+    long long every = 0;                                                       // halt cadence (0: none)
+    if (a.statsEvery > 0) every = dev_stats ? 0 : a.statsEvery;
+    if (dev_stats && a.profilesWriteEvery > 0) every = std::lcm((long long)a.statsEvery, (long long)a.profilesWriteEvery);
+    if (a.spectraEvery > 0) every = every ? std::gcd(every, (long long)a.spectraEvery) : a.spectraEvery;
+    auto device_stats = [&]() -> bool {                                         // H and T_accum from the device
+        std::vector<double> acc(5 * (size_t)r.Ny);
+        if (nse2d_stats_read(r.ctx, acc.data(), &T_accum, nullptr)) return false;
+        for (int q = 0; q < 5; ++q)
+            for (int j = 0; j < r.Ny; ++j) H[q][j] = acc[(size_t)q * r.Ny + j];
+        return true;
+    };
     double t = t_start, dt = a.c.dt_init;
     long long step = 0;
     const auto wall0 = std::chrono::steady_clock::now();
@@ -400,8 +413,8 @@ int main(int argc, char** argv) {
                 return fail("step");
         } else {
             int reason = 0;
-            if (nse2d_run(r.ctx, use_snap ? next_snap : 1e300, use_diag ? next_diag : 1e300, every, a.c.t_end, 20000,
-                          &reason, nullptr))
+            if (nse2d_run(r.ctx, use_snap ? next_snap : 1e300, use_diag ? next_diag : 1e300, (int)every, a.c.t_end,
+                          20000, &reason, nullptr))
                 return fail("run");
             if (reason & NSE2D_HALT_NONFINITE) {
                 int flag = 0;
@@ -436,7 +449,12 @@ int main(int argc, char** argv) {
             write_row(diag_path, step, t, dt, row, a.c.closure_diag);
             next_diag += a.diag_save;
         }
-        if (a.statsEvery > 0 && step % a.statsEvery == 0) {                    // main.cu:695-733
+        if (dev_stats && a.profilesWriteEvery > 0 && step % a.statsEvery == 0 && step % a.profilesWriteEvery == 0) {
+            if (!device_stats()) return fail("statistics");                    // main.cu:722-731
+            const double utau = (T_diag > 0) ? std::sqrt(tauw_abs_dt_sum / T_diag) : utau_now(r);
+            write_profiles(r, prof_path, utau, T_accum, H);
+        }
+        if (!dev_stats && a.statsEvery > 0 && step % a.statsEvery == 0) {      // main.cu:695-733
             const double dtw = t - last_stats_t;
             if (dtw > 0) {
                 if (nse2d_row_moments(r.ctx, mom.data(), nullptr)) return fail("statistics");
@@ -459,6 +477,7 @@ int main(int argc, char** argv) {
             g << step << "," << t << "," << dt << "," << step_ms << "," << fft_ms << "," << tri_ms << "\n";
         }
     }
+    if (dev_stats && !device_stats()) return fail("statistics");
     const double utau_mean = (T_diag > 0) ? std::sqrt(tauw_abs_dt_sum / T_diag) : utau_now(r);   // main.cu:756-770
     write_profiles(r, prof_path, utau_mean, T_accum, H);
     if (a.spectraEvery > 0) {                                                   // main.cu:777-780

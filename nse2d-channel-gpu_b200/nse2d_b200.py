@@ -98,6 +98,8 @@ def load(path=LIB_PATH):
         "nse2d_run": (I, [P, D, D, I, D, ctypes.c_longlong, P, P]),
         "nse2d_row_moments": (I, [P, P, P]),
         "nse2d_spectra_accumulate": (I, [P, P]),
+        "nse2d_stats_device": (I, [P, I, P]),
+        "nse2d_stats_read": (I, [P, P, P, P]),
         "nse2d_spectra": (I, [P, P, P, P, P, P]),
         "nse2d_max_uv_noalloc": (I, [P, P, I, I, D, D, P, P]),
         "nse2d_diagnostics": (I, [P, I, P, P]),
@@ -462,6 +464,19 @@ class Solver:
         out = np.empty((5, self.Ny))
         _check(self.lib.nse2d_row_moments(self.h, _ptr(out), _stream(stream)))
         return out
+
+    def stats_device(self, every, stream=None):
+        """Accumulate the time-weighted row statistics on the device every `every` steps of run()
+        (0: off); starts from zero at the current t."""
+        _check(self.lib.nse2d_stats_device(self.h, int(every), _stream(stream)))
+
+    def stats_read(self, stream=None):
+        """(H [5, Ny], T): the accumulated time-weighted row means of u, v, u^2, v^2, u v and the
+        total weight."""
+        out = np.empty((5, self.Ny))
+        T = ctypes.c_double()
+        _check(self.lib.nse2d_stats_read(self.h, _ptr(out), ctypes.byref(T), _stream(stream)))
+        return out, T.value
 
     def spectra_accumulate(self, stream=None):
         _check(self.lib.nse2d_spectra_accumulate(self.h, _stream(stream)))

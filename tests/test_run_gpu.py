@@ -132,3 +132,28 @@ def test_spectra_match_numpy(nse, cuda):
     np.testing.assert_allclose(kx, 2 * np.pi * np.arange(Nx // 2 + 1) / a.cfg.Lx, rtol=1e-15)
     assert np.max(np.abs(eu - acc_u / 2)) < 1e-12 * np.max(acc_u / 2)
     assert np.max(np.abs(ev - acc_v / 2)) < 1e-12 * np.max(acc_v / 2)
+
+
+def test_device_statistics_match_host_accumulation(nse, cuda):
+    """nse2d_stats_device: the time-weighted row statistics of the reference's loop
+    (src/main.cu:695-733) accumulated inside the run's graph, with no halt, equal the host's
+    accumulation of nse2d_row_moments at the same steps (H += mom / Nx * dtw) to the bit."""
+    a, b = pair(nse)
+    Nx = a.Nx
+    a.stats_device(10)
+    assert a.run(max_steps=50) == nse.HALT_BUDGET          # one launch, no statistics halts
+    H = np.zeros((5, a.Ny))
+    T, last = 0.0, 0.0
+    for k in range(5):
+        assert b.run(stats_every=10) == nse.HALT_STATS
+        t = b.time()[0]
+        dtw = t - last
+        H += b.row_moments() / Nx * dtw
+        T += dtw
+        last = t
+    Ha, Ta = a.stats_read()
+    assert Ta == T
+    assert np.array_equal(Ha, H)
+    assert np.array_equal(a.fields()[0], b.fields()[0])
+    a.stats_device(0)
+    assert a.stats_read()[1] == 0.0
