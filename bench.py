@@ -312,6 +312,9 @@ def run_ours(args, world, rank, local):
     P = args.precision
     solver = nse.Solver(precision=P, **W)
     solver.set_omega(pinned_w0.numpy(), stream=stream)
+    # the fastest kernel plan for this grid (every plan timed from this state, which is restored)
+    plan, plan_ms = solver.autotune_plan(trial_steps=args.plan_trials, stream=stream) if args.plan_trials > 0 \
+        else (solver.plan(), None)
     with torch.cuda.stream(stream):
         solver.step(args.warmup, use_graph=True, stream=stream)
     stream.synchronize()
@@ -345,6 +348,7 @@ def run_ours(args, world, rank, local):
     host_w = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
     host_psi = torch.empty((Ny, Nx), dtype=torch.float64).pin_memory()
     solver2 = nse.Solver(precision=P, **W)
+    solver2.set_plan(**plan)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -413,6 +417,9 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": replica_rate(world, args.steps, e2e_ms), "unit": "steps/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "wall_s": round(wall_e2e, 3)},
+        "plan": {**plan, "tuned_ms_per_step": plan_ms,
+                 "how": "nse2d_autotune_plan: every kernel plan timed over a few graph-replayed steps before "
+                        "the timed region (state restored), the fastest kept"},
         "gpu_launches": int(launches * args.steps),
         "clocks": clocks,
         "sim": {"t": t_sim, "dt_last": dt_last, "steps_done": nsteps_done, "umax": umax[0], "nonfinite": bad},
@@ -565,7 +572,7 @@ def run_ensemble(args):
         for m in spec:
             W = dict(Lx=2 * np.pi, h=1.0, stretch=1, beta=2.0, Ub=1.0, F0=0.05, lin_drag=1e-3, adapt=1, cfl=0.5,
                      dt_max=1e-2, dt_init=1e-3, Nx=m["Nx"], Ny=m["Ny"], Reb=m["Reb"], nforce=m["nforce"])
-            s = nse.Solver(**W)
+            s = nse.Solver(precision=args.precision, **W)
             s.set_omega(initial_vorticity(m["Nx"], m["Ny"], W["Lx"], tanh_y(m["Ny"]), seed=m["seed"]))
             sol.append(s)
         return sol
@@ -576,7 +583,10 @@ def run_ensemble(args):
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     members = build()
     ens = nse.Ensemble(members)
-    groups, _ = ens.autotune(trial_steps=3, stream=stream)
+    groups, _ = ens.autotune_plans(trial_steps=3, stream=stream)
+    plans = {}
+    for m, sm in zip(spec, members):
+        plans.setdefault(f"{m['Nx']}x{m['Ny']}", sm.plan())
     ens.step(args.warmup, stream=stream)
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
@@ -589,7 +599,8 @@ def run_ensemble(args):
     ens_ms = a.elapsed_time(b)
     ens.close()
     seq = build()
-    for s in seq:
+    for m, s in zip(spec, seq):
+        s.set_plan(**plans[f"{m['Nx']}x{m['Ny']}"])
         s.step(args.warmup, use_graph=True, stream=stream)
     torch.cuda.synchronize()
     a.record(stream)
@@ -600,16 +611,19 @@ def run_ensemble(args):
     seq_ms = a.elapsed_time(b)
     for s in members + seq:
         s.close()
-    return {"metric": "ensemble grid-point updates/s (64 channels, configuration 3, FP64)",
+    prec = "FP64" if args.precision == 64 else "FP32-bulk"
+    return {"metric": f"ensemble grid-point updates/s (64 channels, configuration 3, {prec})",
             "value": round(pts * K / (ens_ms * 1e-3), 1), "unit": "points/s", "n_gpus": 1, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ens_ms / K, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded laminar + random modes per member)",
+            "vs_baseline": None, "dtype": "f64" if args.precision == 64 else "f32 bulk (FP64 base profiles and spectra)",
+            "data": "synthetic (seeded laminar + random modes per member)", "plans": plans,
             "config": {"workload": "64 channels, (Nx,Ny) on {256,512,1024}x{129,257,513}, Re_b log-uniform "
                                    "[2e3,2e4], nforce {4,8,12}, tanh beta=2, adaptive dt", "members": len(spec),
                        "points": pts, "master_seed": ENSEMBLE_SEED, "branches": groups},
             "sequential": {"value": round(pts * K / (seq_ms * 1e-3), 1), "unit": "points/s",
                            "ms_per_step": round(seq_ms / K, 4),
-                           "how": "the same 64 channels, each replaying its own one-step graph K times, one after another"},
+                           "how": "the same 64 channels with the same plans, each replaying its own one-step graph "
+                                  "K times, one after another"},
             "speedup_vs_sequential": round(seq_ms / ens_ms, 3), "clocks": ck}
 
 
@@ -691,6 +705,8 @@ def main():
     ap.add_argument("--ref-cuda-steps", type=int, default=40,
                     help="reference arm: also time the reference's CUDA build (oracle/_ref) for K steps (0: off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plan-trials", type=int, default=20,
+                    help="steps per candidate of the kernel-plan autotuner before the timed region (0: default plan)")
     ap.add_argument("--precision", type=int, choices=[64, 32], default=64,
                     help="32: the FP32-bulk variant (its own metric line)")
     ap.add_argument("--workload", choices=["channel", "ensemble", "closure"], default="channel",

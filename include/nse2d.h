@@ -129,6 +129,25 @@ int  nse2d_step(nse2d_ctx* ctx, int nsteps, int use_graph, cudaStream_t s);
  * same bits. Synchronises the device when the form changes (the step graph is captured
  * again). */
 int  nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters);
+/* The kernel forms of a context's step (no counterpart in the reference, which has one form of
+ * each operator): stage_tma, the persistent stage kernel fed by TMA boxes (1) or the one with a
+ * CTA per tile and plain halo loads (0; grids with Nx < 128, or Nx < 256 in precision 32, have
+ * only this one); tridiag_clusters, as nse2d_set_tridiag_form; rowfft_prefetch, the row
+ * transforms whose rows are prefetched into shared memory by bulk copies (1; Nx = 4096 in
+ * precision 64 only) or read by plain loads (0). Every form gives the same step to round-off
+ * (the stage forms and the row transform forms to the bit). nse2d_set_plan falls back to the form
+ * a context can use and synchronises the device when a form changes (the step graphs are
+ * captured again); nse2d_get_plan reports the forms in use. */
+typedef struct nse2d_plan {
+    int stage_tma, tridiag_clusters, rowfft_prefetch;
+} nse2d_plan;
+int  nse2d_get_plan(nse2d_ctx* ctx, nse2d_plan* plan);
+int  nse2d_set_plan(nse2d_ctx* ctx, const nse2d_plan* plan);
+/* Times every plan the context can use over trial_steps graph-replayed steps from the current state
+ * and keeps the fastest (best and its ms per step are reported; either may be NULL). The fields
+ * and the control block are saved before and restored after, so only the plan changes; two
+ * temporary fields are allocated for that. Synchronous. */
+int  nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, double* ms_per_step, cudaStream_t s);
 /* As nse2d_step without a graph, and the last step also stores its stage-3 rhs in the
  * context (field 4), which the next nse2d_diagnostics(t0_row = 0) pairs with omega for the
  * dOmega_rhs column (src/main.cu:586). */
@@ -261,6 +280,13 @@ int  nse2d_ensemble_set_groups(nse2d_ensemble* e, int groups);
  * (1 + trial_steps per candidate). Synchronous. */
 int  nse2d_ensemble_autotune(nse2d_ensemble* e, int trial_steps, int* groups_out, double* ms_per_step_out,
                              cudaStream_t s);
+/* The branch count as nse2d_ensemble_autotune, then the kernel plans of the members (nse2d_plan):
+ * for each class of members with the same grid and precision, every form the class can switch is
+ * toggled for the whole class and kept if the timed ensemble step is faster (coordinate
+ * descent), then the branch count is tuned again. The trials are real steps of every member.
+ * nse2d_get_plan reports each member's chosen plan. Synchronous. */
+int  nse2d_ensemble_autotune_plans(nse2d_ensemble* e, int trial_steps, int* groups_out, double* ms_per_step_out,
+                                   cudaStream_t s);
 
 /* ---- 4. Learned subgrid closure (no reference counterpart) ----
  * BF16 operands on the 5th-generation tensor cores (tcgen05), FP32 accumulate. */

@@ -250,6 +250,86 @@ int nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s) {
     return row_moments(ctx->c, out5, s);
 }
 
+int nse2d_get_plan(nse2d_ctx* ctx, nse2d_plan* plan) {
+    CHECK_CTX(ctx);
+    if (!plan) { set_error("nse2d_get_plan: null plan"); return -1; }
+    const Context* c = ctx->c;
+    plan->stage_tma = (c->prec32 ? c->stage32_tma : c->stage_tma) ? 1 : 0;
+    plan->tridiag_clusters = c->thomas_cluster ? 1 : 0;
+    plan->rowfft_prefetch = c->rowfft_pf ? 1 : 0;
+    return 0;
+}
+
+int nse2d_set_plan(nse2d_ctx* ctx, const nse2d_plan* plan) {
+    CHECK_CTX(ctx);
+    if (!plan) { set_error("nse2d_set_plan: null plan"); return -1; }
+    return set_plan(ctx->c, plan->stage_tma != 0, plan->tridiag_clusters != 0, plan->rowfft_prefetch != 0);
+}
+
+// Every plan the context can use, timed over trial_steps graph-replayed steps from the current
+// state; the state (fields and control block) is saved before and restored after, so only the
+// plan changes. The fastest plan stays set.
+int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, double* ms_per_step, cudaStream_t s) {
+    CHECK_CTX(ctx);
+    if (trial_steps <= 0) { set_error("nse2d_autotune_plan: trial_steps must be positive"); return -1; }
+    Context* c = ctx->c;
+    const size_t fb = c->N * (c->prec32 ? sizeof(float) : sizeof(double));
+    void* wsrc = c->prec32 ? (void*)c->wf : (void*)c->w;
+    void* psrc = c->prec32 ? (void*)c->psif : (void*)c->psi;
+    void *wsave = nullptr, *psave = nullptr;
+    Ctl saved{};
+    NSE_CUDA_TRY(cudaMalloc(&wsave, fb));
+    if (cudaMalloc(&psave, fb) != cudaSuccess) { cudaFree(wsave); set_error("nse2d_autotune_plan: out of memory"); return -1; }
+    cudaEvent_t a = nullptr, b = nullptr;
+    int rc = 0;
+    double best_ms = 1e300;
+    nse2d_plan bp{};
+    auto save = [&]() -> int {
+        NSE_CUDA_TRY(cudaMemcpyAsync(wsave, wsrc, fb, cudaMemcpyDeviceToDevice, s));
+        NSE_CUDA_TRY(cudaMemcpyAsync(psave, psrc, fb, cudaMemcpyDeviceToDevice, s));
+        NSE_CUDA_TRY(cudaMemcpyAsync(&saved, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+        NSE_CUDA_TRY(cudaStreamSynchronize(s));
+        return 0;
+    };
+    auto restore = [&]() -> int {
+        NSE_CUDA_TRY(cudaMemcpyAsync(wsrc, wsave, fb, cudaMemcpyDeviceToDevice, s));
+        NSE_CUDA_TRY(cudaMemcpyAsync(psrc, psave, fb, cudaMemcpyDeviceToDevice, s));
+        NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &saved, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+        NSE_CUDA_TRY(cudaStreamSynchronize(s));
+        return 0;
+    };
+    const bool st_ok = c->prec32 ? c->stage32_tma_ok : c->stage_tma_ok;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) { set_error("event"); rc = -1; }
+    if (rc == 0) rc = save();
+    for (int st = st_ok ? 1 : 0; rc == 0 && st >= 0; --st)
+        for (int cl = c->thomas_cluster_ok ? 1 : 0; rc == 0 && cl >= 0; --cl)
+            for (int pf = c->rowfft_pf_ok ? 1 : 0; rc == 0 && pf >= 0; --pf) {
+                if ((rc = set_plan(c, st, cl, pf))) break;
+                if ((rc = run_steps(c, 1, true, s, false))) break;           // capture and warm
+                cudaEventRecord(a, s);
+                if ((rc = run_steps(c, trial_steps, true, s, false))) break;
+                cudaEventRecord(b, s);
+                if (cudaEventSynchronize(b) != cudaSuccess) {
+                    set_error("nse2d_autotune_plan: %s", cudaGetErrorString(cudaGetLastError()));
+                    rc = -1;
+                    break;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, a, b);
+                if (ms / trial_steps < best_ms) { best_ms = ms / trial_steps; bp = nse2d_plan{st, cl, pf}; }
+                if ((rc = restore())) break;
+            }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (rc == 0) rc = restore();
+    cudaFree(wsave);
+    cudaFree(psave);
+    if (rc) return rc;
+    if (best) *best = bp;
+    if (ms_per_step) *ms_per_step = best_ms;
+    return set_plan(c, bp.stage_tma != 0, bp.tridiag_clusters != 0, bp.rowfft_prefetch != 0);
+}
+
 int nse2d_stats_device(nse2d_ctx* ctx, int every, cudaStream_t s) {
     CHECK_CTX(ctx);
     return stats_device(ctx->c, every, s);

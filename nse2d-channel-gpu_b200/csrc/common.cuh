@@ -158,11 +158,13 @@ struct Context {
     double wall_bot32 = 0.0, wall_top32 = 0.0;
     int maxuv32_ctas = 0;          // resident CTAs of k_maxuv32 (occupancy x SMs)
     // FP32 stage kernel: TMA tensor maps of psi' and of the three w' buffers (Nx >= 256)
-    bool stage32_tma = false;
+    bool stage32_tma = false, stage32_tma_ok = false;
     int stage32_tma_grid = 0;
     CUtensorMap tm32_psi{}, tm32_w[3]{}, tm32_wn{};
+    // row transforms at Nx = 4096: the forms whose rows are prefetched by bulk copies
+    bool rowfft_pf = false, rowfft_pf_ok = false;
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
-    bool stage_tma = false;
+    bool stage_tma = false, stage_tma_ok = false;
     int stage_tma_grid = 0;
     CUtensorMap tm_psi{}, tm_w[3]{}, tm_wn{};
     cudaStream_t cap_stream = nullptr;     // private stream used only for graph capture

@@ -275,7 +275,10 @@ static __global__ void __launch_bounds__(256) k_row_moments(const double* __rest
         if (threadIdx.x < 5) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
-            if constexpr (ACC) out[(size_t)threadIdx.x * Ny + iy] += t / (double)Nx * dtw;
+            // rounded as the host rounds it (no fused multiply-add): the product, then the sum
+            if constexpr (ACC)
+                out[(size_t)threadIdx.x * Ny + iy] = __dadd_rn(out[(size_t)threadIdx.x * Ny + iy],
+                                                               __dmul_rn(t / (double)Nx, dtw));
             else out[(size_t)threadIdx.x * Ny + iy] = t;
         }
         __syncthreads();

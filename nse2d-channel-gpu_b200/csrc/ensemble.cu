@@ -34,10 +34,10 @@ struct Ensemble {
     cudaGraphExec_t exec = nullptr;
 };
 
-int ensemble_build(Ensemble* e, int groups) {
+int ensemble_build(Ensemble* e, int groups, bool force = false) {
     const int n = (int)e->m.size();
     groups = std::max(1, std::min(groups, n));
-    if (e->exec && e->groups == groups) return 0;
+    if (e->exec && e->groups == groups && !force) return 0;
     if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
     while ((int)e->branch.size() < groups) {
         cudaStream_t s;
@@ -107,6 +107,9 @@ struct nse2d_ensemble {
 
 extern "C" {
 
+int nse2d_ensemble_autotune(nse2d_ensemble* en, int trial_steps, int* groups_out, double* ms_per_step_out,
+                            cudaStream_t s);
+
 int nse2d_ensemble_create(nse2d_ctx* const* members, int n, nse2d_ensemble** out) {
     if (!members || n <= 0 || !out) { set_error("nse2d_ensemble_create: bad arguments"); return -1; }
     *out = nullptr;
@@ -155,6 +158,74 @@ int nse2d_ensemble_step(nse2d_ensemble* en, int nsteps, cudaStream_t s) {
     return ensemble_step(&en->e, nsteps, s);
 }
 
+// Coordinate descent over the kernel plans of the members: for every class of members with the
+// same grid and precision, each form the class can switch (stage kernel, tridiagonal form, row
+// transform form) is toggled for the whole class, the ensemble graph rebuilt and one ensemble
+// step timed; a toggle that is not faster is undone. Then the branch count is tuned again.
+int nse2d_ensemble_autotune_plans(nse2d_ensemble* en, int trial_steps, int* groups_out, double* ms_per_step_out,
+                                  cudaStream_t s) {
+    if (!en || trial_steps <= 0) { set_error("nse2d_ensemble_autotune_plans: bad arguments"); return -1; }
+    Ensemble& e = en->e;
+    int g0 = 0;
+    double ms0 = 0.0;
+    if (nse2d_ensemble_autotune(en, trial_steps, &g0, &ms0, s)) return -1;
+    cudaEvent_t a, b;
+    NSE_CUDA_TRY(cudaEventCreate(&a));
+    NSE_CUDA_TRY(cudaEventCreate(&b));
+    auto time_step = [&](double& ms) -> int {
+        if (ensemble_build(&e, e.groups, true) || ensemble_step(&e, 1, s)) return -1;
+        cudaEventRecord(a, s);
+        if (ensemble_step(&e, trial_steps, s)) return -1;
+        cudaEventRecord(b, s);
+        NSE_CUDA_TRY(cudaEventSynchronize(b));
+        float f = 0.f;
+        cudaEventElapsedTime(&f, a, b);
+        ms = f / trial_steps;
+        return 0;
+    };
+    struct Cls { int Nx, Ny; bool p32; std::vector<Context*> m; };
+    std::vector<Cls> cls;
+    for (Context* c : e.m) {
+        auto it = std::find_if(cls.begin(), cls.end(),
+                               [&](const Cls& k) { return k.Nx == c->Nx && k.Ny == c->Ny && k.p32 == c->prec32; });
+        if (it == cls.end()) { cls.push_back({c->Nx, c->Ny, c->prec32, {}}); it = cls.end() - 1; }
+        it->m.push_back(c);
+    }
+    auto plan_of = [](const Context* c, bool* v) {
+        v[0] = c->prec32 ? c->stage32_tma : c->stage_tma;
+        v[1] = c->thomas_cluster;
+        v[2] = c->rowfft_pf;
+    };
+    double best = 0.0;
+    int rc = time_step(best);
+    for (size_t k = 0; rc == 0 && k < cls.size(); ++k) {
+        Context* c0 = cls[k].m[0];
+        const bool ok[3] = {c0->prec32 ? c0->stage32_tma_ok : c0->stage_tma_ok, c0->thomas_cluster_ok, c0->rowfft_pf_ok};
+        for (int f = 0; rc == 0 && f < 3; ++f) {
+            if (!ok[f]) continue;
+            bool v[3];
+            plan_of(c0, v);
+            v[f] = !v[f];
+            for (Context* c : cls[k].m)
+                if ((rc = set_plan(c, v[0], v[1], v[2]))) break;
+            double ms = 0.0;
+            if (rc == 0) rc = time_step(ms);
+            if (rc == 0 && !(ms < best)) {                       // not faster: undo
+                v[f] = !v[f];
+                for (Context* c : cls[k].m)
+                    if ((rc = set_plan(c, v[0], v[1], v[2]))) break;
+            } else if (rc == 0) {
+                best = ms;
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (ensemble_build(&e, e.groups, true)) return -1;
+    return nse2d_ensemble_autotune(en, trial_steps, groups_out, ms_per_step_out, s);
+}
+
 int nse2d_ensemble_autotune(nse2d_ensemble* en, int trial_steps, int* groups_out, double* ms_per_step_out,
                             cudaStream_t s) {
     if (!en || trial_steps <= 0) { set_error("nse2d_ensemble_autotune: bad arguments"); return -1; }
@@ -170,7 +241,7 @@ int nse2d_ensemble_autotune(nse2d_ensemble* en, int trial_steps, int* groups_out
     double best_ms = 1e300;
     int rc = 0;
     for (int g : cand) {
-        if ((rc = ensemble_build(&e, g))) break;
+        if ((rc = ensemble_build(&e, g, true))) break;
         if ((rc = ensemble_step(&e, 1, s))) break;                    // warm: first launch of this graph
         cudaEventRecord(a, s);
         if ((rc = ensemble_step(&e, trial_steps, s))) break;
@@ -185,7 +256,7 @@ int nse2d_ensemble_autotune(nse2d_ensemble* en, int trial_steps, int* groups_out
     if (rc) return rc;
     if (groups_out) *groups_out = best;
     if (ms_per_step_out) *ms_per_step_out = best_ms;
-    return ensemble_build(&e, best);
+    return ensemble_build(&e, best, true);
 }
 
 }  // extern "C"

@@ -425,7 +425,8 @@ int context_create(const Config& cfg, Context** out) {
         c->maxuv_ctas = per_sm * c->num_sms;
     }
     // stage kernel: persistent TMA variant when every tile row holds two or more tiles
-    c->stage_tma = (c->Nx >= 2 * ST_TX);
+    c->stage_tma = c->stage_tma_ok = (c->Nx >= 2 * ST_TX);
+    c->rowfft_pf = c->rowfft_pf_ok = (c->M == 16 * IP_NT);
     if (c->stage_tma) {
         if (encode_field_map(&c->tm_psi, c->psi, c->Nx, Ny) || encode_field_map(&c->tm_w[0], c->w, c->Nx, Ny) ||
             encode_field_map(&c->tm_w[1], c->w1, c->Nx, Ny) || encode_field_map(&c->tm_w[2], c->w2, c->Nx, Ny) ||
@@ -548,6 +549,15 @@ template <typename K> static int fft_wave(K kern, size_t smem, int nrows, int nu
 }
 
 template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) {
+    if constexpr (M == 16 * IP_NT) if (c->rowfft_pf) {
+        // the real rows prefetched into shared memory by bulk copies (k_fft_fwd_pf)
+        const size_t sm = FftPf<M>::smem;
+        int grid = 0;
+        if (fft_wave(k_fft_fwd_pf<M>, sm, p.nrows, c->num_sms, &grid)) return -1;
+        k_fft_fwd_pf<M><<<grid, IP_NT, sm, s>>>(p);
+        NSE_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     const size_t sm = fft_smem(M);
     int grid = 0;
     if (fft_wave(k_fft_fwd<M>, sm, p.nrows, c->num_sms, &grid)) return -1;
@@ -560,6 +570,15 @@ template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) 
 // (adjacent rows of the spectral buffer are adjacent in memory; strided rows measured slower).
 // The Thom closure is applied by the CTA that writes the second row of each wall.
 template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
+    if constexpr (M == 16 * IP_NT) if (c->rowfft_pf) {
+        // the spectral rows prefetched into shared memory by bulk copies (k_ifft_thom_pf)
+        const size_t sm = IfftPf<M>::smem;
+        int wave = 0;
+        if (fft_wave(k_ifft_thom_pf<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
+        k_ifft_thom_pf<M><<<std::max(1, std::min(wave, c->Ny)), IP_NT, sm, s>>>(p);
+        NSE_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     const size_t sm = fft_smem(M);
     int wave = 0;
     if (fft_wave(k_ifft_thom<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
@@ -642,6 +661,22 @@ int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
     maps.cp = c->tm_cp;
     NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, thomas_cluster_kernel(c->tc_L), maps, thomas_params(c, homog)));
     return 0;
+}
+
+// The kernel forms of the step (each falls back to the one the context can use); drops the
+// captured graphs when anything changes.
+int set_plan(Context* c, bool stage_tma, bool clusters, bool rowfft_pf) {
+    const bool st = stage_tma && (c->prec32 ? c->stage32_tma_ok : c->stage_tma_ok);
+    const bool pf = rowfft_pf && c->rowfft_pf_ok;
+    const bool cur = c->prec32 ? c->stage32_tma : c->stage_tma;
+    if (st != cur || pf != c->rowfft_pf) {
+        NSE_CUDA_TRY(cudaDeviceSynchronize());
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
+        if (c->prec32) c->stage32_tma = st; else c->stage_tma = st;
+        c->rowfft_pf = pf;
+    }
+    return set_tridiag_form(c, clusters);
 }
 
 int set_tridiag_form(Context* c, bool clusters) {

@@ -47,7 +47,7 @@ int setup32(Context* c) {
     NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_maxuv32, 256, 0));
     c->maxuv32_ctas = std::max(per_sm, 1) * c->num_sms;
     // stage kernel: the persistent TMA form when every tile row holds two or more tiles
-    c->stage32_tma = (c->Nx >= 2 * S32_TX);
+    c->stage32_tma = c->stage32_tma_ok = (c->Nx >= 2 * S32_TX);
     if (c->stage32_tma) {
         const int Nx = c->Nx, Ny = c->Ny;
         if (encode_map_2d(&c->tm32_psi, c->psif, true, Nx, Ny, S32_W, S32_H) ||

@@ -846,6 +846,191 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     }
 }
 
+// The inverse transform at M = 2048 with the spectral rows prefetched: a bulk copy
+// (cp.async.bulk, completion on an mbarrier) brings row j+1's X_0..X_M into a shared staging
+// buffer while row j is transformed, so pass 0 reads X_n and X_{M-n} from shared memory instead
+// of waiting on global loads. Thread t takes the pass-0 butterfly t (points t + 128 r) with the
+// same merge and DFT as k_ifft_thom, so the buffer holds the same bits and psi is the same.
+// The staging buffer is read in pass 0 only; after the barrier that ends pass 0, thread 0 issues
+// the next row's copy into it. Three CTAs of 66 KB per SM. Every wait is bounded: a wait that
+// runs out sets bit 1 of the non-finite flag, no further copy is issued, and the CTA waits once
+// more (bounded) for the copy in flight before it exits.
+template <int M> struct IfftPf {
+    static constexpr size_t stage_off = ((size_t)ip_size(M) * 16 + 127) / 128 * 128;
+    static constexpr unsigned row_bytes = (unsigned)(M + 1) * 16u;
+    static constexpr size_t bar_off = (stage_off + row_bytes + 15) / 16 * 16;
+    static constexpr size_t smem = bar_off + 16;
+};
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// The forward transform at M = 2048 with its real rows prefetched the same way: a bulk copy brings
+// row j + grid's Nx reals into a shared staging buffer while row j is transformed; pass 0 reads
+// z_n = x_2n + i x_2n+1 from shared memory. The arithmetic is k_fft_fwd's (the same bits).
+template <int M> struct FftPf {
+    static constexpr size_t stage_off = ((size_t)ip_size(M) * 16 + 127) / 128 * 128;
+    static constexpr unsigned row_bytes = (unsigned)M * 16u;
+    static constexpr size_t bar_off = stage_off + row_bytes;
+    static constexpr size_t smem = bar_off + 16;
+};
+
+template <int M>
+static __global__ void __launch_bounds__(IP_NT, 3) k_fft_fwd_pf(FftParams p) {
+    static_assert(M / 16 == IP_NT && p16_plan<M>::R(0) == 16 && M == 16 * IP_NT, "one pass-0 butterfly per thread");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
+    const double2* stage = reinterpret_cast<const double2*>(smem_raw + FftPf<M>::stage_off);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + FftPf<M>::bar_off);
+    const int je = p.row0 + p.nrows;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    auto issue = [&](int j) {
+        mbar_expect_tx(bar, FftPf<M>::row_bytes);
+        bulk_load(const_cast<double2*>(stage), p.src + (size_t)j * p.Nx, FftPf<M>::row_bytes, bar);
+    };
+    const int jfirst = p.row0 + blockIdx.x;
+    if (threadIdx.x == 0 && jfirst < je) issue(jfirst);
+    unsigned parity = 0;
+    bool live = true;
+    for (int j = jfirst; j < je; j += gridDim.x) {
+        if (live) {
+            live = __syncthreads_and(mbar_wait_bounded(bar, parity));
+            if (live) parity ^= 1u;
+            else if (threadIdx.x == 0) atomicOr(&p.ctl->nonfinite, 2);
+        }
+        {
+            const int t = (int)threadIdx.x;
+            cpx<double> v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const double2 z = stage[t + IP_NT * r];
+                v[r] = {z.x, z.y};
+            }
+            dftR<double, 16, false>(v);
+            const int p0 = dit16_pos<M>(t);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+        }
+        __syncthreads();                               // pass 0 done: the staging buffer is free
+        if (threadIdx.x == 0 && live && j + (int)gridDim.x < je) {
+            fence_proxy_async_smem();
+            issue(j + (int)gridDim.x);
+        }
+        p16_pass<double, M, 1, false, IP_NT>(buf, p.tw);
+        __syncthreads();
+        fwd_last_pass_split<double, M>(buf, p.tw, p.wN, reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp));
+        __syncthreads();                               // the buffer read before the next row's pass 0
+    }
+    if (!live && threadIdx.x == 0) mbar_wait_bounded(bar, parity);   // the copy still in flight
+}
+
+template <int M>
+static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
+    static_assert(M / 16 == IP_NT && p16_plan<M>::R(0) == 16 && p16_plan<M>::P >= 2, "one pass-0 butterfly per thread");
+    extern __shared__ __align__(16) unsigned char smem_raw[];   // offsets: stage at 128 B, barrier at 16 B multiples
+    cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
+    const double2* stage = reinterpret_cast<const double2*>(smem_raw + IfftPf<M>::stage_off);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + IfftPf<M>::bar_off);
+    __shared__ bool thom_now;
+    const int Nx = p.Nx, Ny = p.Ny;
+    constexpr double scale = 0.5 / (double)M;          // the merge forms 2 Z_n
+    const int j0 = (int)(((long long)blockIdx.x * Ny) / gridDim.x);
+    const int j1 = (int)(((long long)(blockIdx.x + 1) * Ny) / gridDim.x);
+    const int jlo = max(j0, 1), jhi = min(j1, Ny - 1);   // the band's interior rows [jlo, jhi)
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+    auto issue = [&](int j) {
+        mbar_expect_tx(bar, IfftPf<M>::row_bytes);
+        bulk_load(const_cast<double2*>(stage), p.hat + (size_t)j * p.Hp, IfftPf<M>::row_bytes, bar);
+    };
+    if (threadIdx.x == 0 && jlo < jhi) issue(jlo);
+    unsigned parity = 0;
+    bool live = true;                                  // no wait has run out
+    for (int j = j0; j < j1; ++j) {
+        double* dst = p.psi + (size_t)j * Nx;
+        if (j == 0 || j == Ny - 1) {
+            const double v = (j == 0) ? p.psi_bot : p.psi_top;
+            for (int i = threadIdx.x; i < Nx; i += IP_NT) dst[i] = v;
+            continue;
+        }
+        if (live) {
+            live = __syncthreads_and(mbar_wait_bounded(bar, parity));
+            if (live) parity ^= 1u;                    // else the copy of phase `parity` is still in flight
+            else if (threadIdx.x == 0) atomicOr(&p.ctl->nonfinite, 2);
+        }
+        {
+            // pass 0: 2 Z_n = s + i d conj(W^n) from X_n, X_{M-n} (n = b + 128 r), as k_ifft_thom
+            const int b = (int)threadIdx.x;
+            const cpx<double> wt = ldtw(p.wN, b);
+            cpx<double> v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int n = b + IP_NT * r;
+                const double2 av = stage[n], bv = stage[M - n];
+                const cpx<double> sm = {av.x + bv.x, av.y - bv.y};
+                const cpx<double> df = {av.x - bv.x, av.y + bv.y};
+                const cpx<double> wn = (r == 0) ? wt : cmul(wt, w32<double>(r));
+                v[r] = cadd(sm, mul_pi(cmulc(df, wn)));
+            }
+            dftR<double, 16, true>(v);
+            const int p0 = dit16_pos<M>(b);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) buf[ip_idx<M>(p0 + q)] = v[q];
+        }
+        __syncthreads();                               // pass 0 done: the staging buffer is free
+        if (threadIdx.x == 0 && live && j + 1 < jhi) {
+            fence_proxy_async_smem();                  // the reads of the staging buffer before its next write
+            issue(j + 1);
+        }
+        p16_passes_to<double, M, 1, true, IP_NT>(buf, p.tw, [&](int n, const cpx<double>& z) {
+            reinterpret_cast<double2*>(dst)[n] = make_double2(z.x * scale, z.y * scale);
+        });
+        __syncthreads();
+        if (p.do_thom) {
+            const bool bot = (j == 1 || j == 2), top = (j == Ny - 3 || j == Ny - 2);
+            if (bot || top) {
+                __threadfence();
+                __syncthreads();
+                for (int wall = 0; wall < 2; ++wall) {
+                    if (!(wall == 0 ? bot : top)) continue;
+                    if (threadIdx.x == 0) thom_now = (atomicAdd(&p.ctl->thom_done[wall], 1u) == 1u);
+                    __syncthreads();
+                    if (thom_now) {
+                        __threadfence();
+                        thom_row<IP_NT>(p, wall == 1);
+                        if (threadIdx.x == 0) p.ctl->thom_done[wall] = 0;
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+    }
+    if (!live && threadIdx.x == 0) mbar_wait_bounded(bar, parity);   // the copy still in flight
+    if (p.advance) {
+        __shared__ bool last;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last = (atomicAdd(&p.ctl->ifft_done, 1u) == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            p.ctl->ifft_done = 0;
+            advance_time(p.ctl);
+        }
+    }
+}
+
 struct ThomasParams {
     cpx<double>* hat;        // [Ny][Hp], in place: omega-hat in, psi-hat out
     const double* cp;        // [Ni][Hp]

@@ -42,6 +42,14 @@ class Config(ctypes.Structure):
                 ("precision", ctypes.c_int), ("y_table", ctypes.c_void_p)]
 
 
+class Plan(ctypes.Structure):
+    """struct nse2d_plan: the kernel forms of a context's step."""
+    _fields_ = [("stage_tma", ctypes.c_int), ("tridiag_clusters", ctypes.c_int), ("rowfft_prefetch", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class SnapshotMeta(ctypes.Structure):
     """struct nse2d_snapshot_meta: the grid and the scalar attributes of a snapshot file."""
     _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("t", ctypes.c_double), ("Lx", ctypes.c_double),
@@ -99,6 +107,10 @@ def load(path=LIB_PATH):
         "nse2d_row_moments": (I, [P, P, P]),
         "nse2d_spectra_accumulate": (I, [P, P]),
         "nse2d_stats_device": (I, [P, I, P]),
+        "nse2d_get_plan": (I, [P, ctypes.POINTER(Plan)]),
+        "nse2d_set_plan": (I, [P, ctypes.POINTER(Plan)]),
+        "nse2d_autotune_plan": (I, [P, I, ctypes.POINTER(Plan), P, P]),
+        "nse2d_ensemble_autotune_plans": (I, [P, I, P, P, P]),
         "nse2d_stats_read": (I, [P, P, P, P]),
         "nse2d_spectra": (I, [P, P, P, P, P, P]),
         "nse2d_max_uv_noalloc": (I, [P, P, I, I, D, D, P, P]),
@@ -413,6 +425,28 @@ class Solver:
         two-pass form, which shares the device with concurrent work (ensemble members use it)."""
         _check(self.lib.nse2d_set_tridiag_form(self.h, 1 if clusters else 0))
 
+    def plan(self):
+        """The kernel forms in use: {stage_tma, tridiag_clusters, rowfft_prefetch}."""
+        pl = Plan()
+        _check(self.lib.nse2d_get_plan(self.h, ctypes.byref(pl)))
+        return pl.as_dict()
+
+    def set_plan(self, stage_tma=None, tridiag_clusters=None, rowfft_prefetch=None):
+        """Select kernel forms (None keeps the current one); forms the grid cannot use fall back."""
+        cur = self.plan()
+        pl = Plan(**{k: int(v if v is not None else cur[k]) for k, v in
+                     (("stage_tma", stage_tma), ("tridiag_clusters", tridiag_clusters),
+                      ("rowfft_prefetch", rowfft_prefetch))})
+        _check(self.lib.nse2d_set_plan(self.h, ctypes.byref(pl)))
+
+    def autotune_plan(self, trial_steps=10, stream=None):
+        """Time every plan the context can use (the state is restored) and keep the fastest;
+        returns (plan dict, ms per step)."""
+        pl, ms = Plan(), ctypes.c_double()
+        _check(self.lib.nse2d_autotune_plan(self.h, int(trial_steps), ctypes.byref(pl), ctypes.byref(ms),
+                                            _stream(stream)))
+        return pl.as_dict(), ms.value
+
     def step_store_rhs(self, nsteps=1, stream=None):
         _check(self.lib.nse2d_step_store_rhs(self.h, int(nsteps), _stream(stream)))
 
@@ -557,6 +591,14 @@ class Ensemble:
 
     def set_groups(self, groups):
         _check(self.lib.nse2d_ensemble_set_groups(self.h, int(groups)))
+
+    def autotune_plans(self, trial_steps=5, stream=None):
+        """The branch count, then the members' kernel plans by classes of equal grids (coordinate
+        descent), then the branch count again: (branches, ms per ensemble step)."""
+        g, ms = ctypes.c_int(), ctypes.c_double()
+        _check(self.lib.nse2d_ensemble_autotune_plans(self.h, int(trial_steps), ctypes.byref(g), ctypes.byref(ms),
+                                                      _stream(stream)))
+        return g.value, ms.value
 
     def autotune(self, trial_steps=5, stream=None):
         """(branches, ms per ensemble step) of the fastest grouping, which stays selected."""

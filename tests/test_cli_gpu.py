@@ -149,12 +149,13 @@ def test_stretch_table(nse, cuda, tmp_path):
     for k, exp in enumerate((y, a, 0.5 * (a[:-1] + a[1:]), de, wn)):
         assert np.array_equal(g.metric(k), exp), k
     g.close()
+    # the profiles file takes y from the grid only when beta > 0 (src/io.cu:276), as the reference does
     d = run_cli(["--Nx", str(Nx), "--Ny", str(Ny), "--Lx", repr(2 * np.pi), "--Ub", "1", "--Reb", "1000",
-                 "--init", "mix", "--amp", "0.05", "--stretch", "table", "--ytable", str(tab), "--tend", "0.05",
-                 "--diag_save", "0.05", "--snap_save", "0"], str(tmp_path / "run"))
+                 "--init", "mix", "--amp", "0.05", "--stretch", "table", "--beta", "1", "--ytable", str(tab),
+                 "--tend", "0.05", "--diag_save", "0.05", "--snap_save", "0"], str(tmp_path / "run"))
     assert len(d) == 2 and np.all(np.isfinite(d["K"]))
     prof = np.genfromtxt(tmp_path / "run" / "profiles_timeavg.csv", delimiter=",", names=True)
-    assert np.array_equal(prof["y"], y)
+    assert np.allclose(prof["y"], y, rtol=1e-8, atol=1e-9)           # the CSV prints 9 digits
     p = subprocess.run([CLI, "--Nx", "64", "--Ny", "41", "--stretch", "table", "--outdir", str(tmp_path / "x")],
                        capture_output=True, text=True, timeout=60)
     assert p.returncode != 0 and "--ytable required" in p.stderr

@@ -36,8 +36,8 @@ def cpp_symbols(path):
     syms = {}
     for ln in out.splitlines():
         parts = ln.split()
-        if len(parts) == 3 and parts[1] == "T" and parts[2].startswith("_Z"):
-            m = parts[2]
+        if len(parts) == 3 and parts[1] == "T" and parts[2].startswith("_Z") and parts[2][2:3].isdigit():
+            m = parts[2]                                # a global function (not a nested name, _ZN...)
             k = 2
             while m[k].isdigit():
                 k += 1

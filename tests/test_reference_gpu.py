@@ -36,7 +36,7 @@ import numpy as np
 import pytest
 
 from conftest import ORACLE, PKG, load_oracle_module
-from test_parity_gpu import assert_fields_close, laminar_perturbed, relerr
+from test_parity_gpu import assert_fields_close, laminar_perturbed, relerr, thom_gain
 
 pytestmark = pytest.mark.gpu
 
@@ -184,6 +184,12 @@ def _both(nse, dt, **kw):
 @need_loop
 @pytest.mark.parametrize("dt", [1e-3, 1e-4])
 def test_small_channel_one_step_matches_reference_loop(nse, cuda, dt):
+    """One step. At dt = 1e-4: psi and omega to 1e-11, the wall rows to the Thom-gain bound. At
+    dt = 1e-3, past the stability limit, the step multiplies the stiffest wall-normal mode by
+    |R(nu dt lambda_min)| = |1 + z + z^2/2 + z^3/6| ~ 115 (z = -9.7), and the Thom closure's
+    round-off in the wall rows (thom_gain ulp(psi)) reaches the first rows inside through the
+    Laplacian of stages 2 and 3: psi and omega beyond 4 rows of a wall are held to 1e-11, the 4 rows
+    next to each wall to 115 times the Thom-gain bound."""
     g, r = _both(nse, dt)
     wg, pg = g.fields()
     wr, pr = r.fields()
@@ -192,9 +198,17 @@ def test_small_channel_one_step_matches_reference_loop(nse, cuda, dt):
     r.step(1)
     wg, pg = g.fields()
     wr, pr = r.fields()
-    assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-11)
-    print(f"dt={dt:g}: one step, psi {relerr(pg, pr):.2e}, omega rows 2..Ny-3 "
-          f"{np.max(np.abs(wg[2:-2] - wr[2:-2])) / np.max(np.abs(wr)):.2e}")
+    rows = np.max(np.abs(wg - wr), axis=1) / np.max(np.abs(wr))
+    print(f"dt={dt:g}: one step, psi {relerr(pg, pr):.2e}; omega by row (first 6): "
+          + " ".join(f"{e:.1e}" for e in rows[:6]) + f"; rows 4..Ny-5 {rows[4:-4].max():.2e}")
+    if dt == 1e-4:
+        assert_fields_close(wg, pg, wr, pr, g.metric(3), 1e-11)
+    else:
+        assert relerr(pg, pr) < 1e-11
+        assert rows[4:-4].max() < 1e-11, rows[4:-4].max()
+        bound = 115.0 * thom_gain(g.metric(3)) * 8 * np.finfo(float).eps * np.max(np.abs(pr)) / np.max(np.abs(wr))
+        near = np.concatenate([rows[:4], rows[-4:]])
+        assert near.max() < bound, (near, bound)
     g.close()
     r.close()
 
