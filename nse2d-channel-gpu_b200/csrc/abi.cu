@@ -82,6 +82,7 @@ int nse2d_set_state(nse2d_ctx* ctx, const double* w, const double* psi, int wher
     h.t = t; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
     if (c->prec32 && split32(c, s)) return -1;
+    if (refresh_maxima(c, s)) return -1;
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
 }

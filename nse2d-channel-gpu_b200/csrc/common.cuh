@@ -68,6 +68,7 @@ struct Ctl {
     // moments weighted by t - acc_last_t are added to the context's accumulator
     int acc_every;
     double acc_last_t, acc_T;
+    double mx_next[3];             // max |u|, |v|, |v| a of the current psi (the next step's dt)
     // run mode (nse2d_run): stop stepping when an output, a statistics step or the end is due
     int run;                       // 1 while a run is active
     int halt;                      // set at the end of the step after which the run stops
@@ -163,6 +164,7 @@ struct Context {
     CUtensorMap tm32_psi{}, tm32_w[3]{}, tm32_wn{};
     // row transforms at Nx = 4096: the forms whose rows are prefetched by bulk copies
     bool rowfft_pf = false, rowfft_pf_ok = false;
+    unsigned int* bcount = nullptr;  // [grid + 1] band-boundary counters of the fused max reduction
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false, stage_tma_ok = false;
     int stage_tma_grid = 0;

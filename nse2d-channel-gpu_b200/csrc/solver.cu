@@ -427,6 +427,15 @@ int context_create(const Config& cfg, Context** out) {
     // stage kernel: persistent TMA variant when every tile row holds two or more tiles
     c->stage_tma = c->stage_tma_ok = (c->Nx >= 2 * ST_TX);
     c->rowfft_pf = c->rowfft_pf_ok = (c->M == 16 * IP_NT);
+    if (c->rowfft_pf_ok) {
+        // arrival counters of the band boundaries of the inverse transform (at most Ny / 2 bands)
+        const size_t nb = (size_t)Ny / 2 + 2;
+        if (cudaMalloc((void**)&c->bcount, nb * sizeof(unsigned)) != cudaSuccess ||
+            cudaMemset(c->bcount, 0, nb * sizeof(unsigned)) != cudaSuccess) {
+            set_error("cudaMalloc of the band counters failed");
+            return fail();
+        }
+    }
     if (c->stage_tma) {
         if (encode_field_map(&c->tm_psi, c->psi, c->Nx, Ny) || encode_field_map(&c->tm_w[0], c->w, c->Nx, Ny) ||
             encode_field_map(&c->tm_w[1], c->w1, c->Nx, Ny) || encode_field_map(&c->tm_w[2], c->w2, c->Nx, Ny) ||
@@ -477,9 +486,14 @@ void context_destroy(Context* c) {
     if (c->spec_acc) cudaFree(c->spec_acc);
     if (c->moments) cudaFree(c->moments);
     if (c->stats_acc) cudaFree(c->stats_acc);
+    if (c->bcount) cudaFree(c->bcount);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
+
+// The max reduction of an adaptive FP64 step runs in its stage-3 inverse transform when that is the
+// prefetching form (k_ifft_thom_pf); the stage-1 kernel then takes dt from the maxima it left.
+static bool fused_max(const Context* c) { return c->cfg.adapt && !c->prec32 && c->rowfft_pf; }
 
 // ---- launchers ----
 static StageParams stage_params(Context* c) {
@@ -490,6 +504,9 @@ static StageParams stage_params(Context* c) {
     p.nu = c->nu; p.lin_drag = c->cfg.lin_drag;
     p.mms_A0 = c->cfg.mms_A0; p.mms_eps = c->cfg.mms_eps; p.mms_Om = c->cfg.mms_Om;
     p.mms_k = 2.0 * kPiD * (double)c->cfg.mms_kx / c->cfg.Lx; p.mms_c = kPiD / (2.0 * c->cfg.h);
+    p.dt_from_max = fused_max(c) ? 1 : 0;
+    p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc; p.dx = c->dx; p.deta = c->deta; p.inv_dymin2 = c->inv_dymin2;
+    p.dt_max = c->cfg.dt_max;
     return p;
 }
 
@@ -529,6 +546,7 @@ static size_t fft_smem(int M) { return fft_smem_bytes(M); }
 
 static FftParams fft_params(Context* c) {
     FftParams p{};
+    p.a_node = c->rt.a_node; p.bcount = c->bcount; p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta;
     p.hat = c->hat; p.tw = c->tw; p.wN = c->wN; p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp;
     p.dy_edge = c->rt.dy_edge; p.w_node = c->rt.w_node; p.ctl = c->ctl; p.free_slip = c->cfg.free_slip;
     p.psi_bot = c->psi_bot; p.psi_top = c->psi_top; p.invA_full = c->invA_full;
@@ -572,10 +590,11 @@ template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) 
 template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) {
     if constexpr (M == 16 * IP_NT) if (c->rowfft_pf) {
         // the spectral rows prefetched into shared memory by bulk copies (k_ifft_thom_pf)
+        // bands of two or more rows (the fused max reduction pairs the rows at band boundaries)
         const size_t sm = IfftPf<M>::smem;
         int wave = 0;
         if (fft_wave(k_ifft_thom_pf<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
-        k_ifft_thom_pf<M><<<std::max(1, std::min(wave, c->Ny)), IP_NT, sm, s>>>(p);
+        k_ifft_thom_pf<M><<<std::max(1, std::min(wave, c->Ny / 2)), IP_NT, sm, s>>>(p);
         NSE_CUDA_TRY(cudaGetLastError());
         return 0;
     }
@@ -630,6 +649,7 @@ int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom
     FftParams p = fft_params(c);
     p.psi = psi; p.w = w; p.stage = stage; p.do_thom = do_thom ? 1 : 0; p.closure = closure ? 1 : 0;
     p.advance = advance ? 1 : 0;
+    p.fuse_max = (advance && fused_max(c)) ? 1 : 0;
     NSE_FFT_DISPATCH(fft_inv_t)
 }
 
@@ -676,7 +696,11 @@ int set_plan(Context* c, bool stage_tma, bool clusters, bool rowfft_pf) {
         if (c->prec32) c->stage32_tma = st; else c->stage_tma = st;
         c->rowfft_pf = pf;
     }
-    return set_tridiag_form(c, clusters);
+    if (set_tridiag_form(c, clusters)) return -1;
+    // the next step may take its dt from the maxima of the current psi
+    if (refresh_maxima(c, 0)) return -1;
+    NSE_CUDA_TRY(cudaDeviceSynchronize());
+    return 0;
 }
 
 int set_tridiag_form(Context* c, bool clusters) {
@@ -749,7 +773,7 @@ static int step_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev
         return 0;
     };
     if (mark()) return -1;
-    if (c->cfg.adapt) {
+    if (c->cfg.adapt && !fused_max(c)) {
         if (launch_maxuv(c, c->psi, true, s) || mark()) return -1;
     }
     double* wst[3] = {c->w1, c->w2, c->w};
@@ -774,7 +798,7 @@ int enqueue_step_timed(Context* c, cudaStream_t s, cudaEvent_t* ev, bool store_r
 // Names of the kernels of one step, in launch order (for the timed step).
 const char* step_kernel_name(const Context* c, int k) {
     if (c->prec32) return step32_kernel_name(c, k);
-    if (c->cfg.adapt) {
+    if (c->cfg.adapt && !fused_max(c)) {
         if (k == 0) return "k_maxuv_dt";
         --k;
     }
@@ -787,7 +811,17 @@ const char* step_kernel_name(const Context* c, int k) {
     return thomas_kernel_name(c, i - 2);
 }
 
-int launches_per_step(const Context* c) { return (c->cfg.adapt ? 1 : 0) + 3 * (3 + thomas_launches(c)); }
+int launches_per_step(const Context* c) {
+    if (c->prec32) return (c->cfg.adapt ? 1 : 0) + 3 * (3 + thomas_launches(c));
+    return (c->cfg.adapt && !fused_max(c) ? 1 : 0) + 3 * (3 + thomas_launches(c));
+}
+
+// max |u|, |v|, |v| a of the current psi into the control block (also as the next step's maxima):
+// after the state is set, or the kernel plan changes.
+int refresh_maxima(Context* c, cudaStream_t s) {
+    if (c->prec32 || !c->cfg.adapt) return 0;
+    return launch_maxuv(c, c->psi, false, s);
+}
 
 // nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.
 int run_steps(Context* c, int nsteps, bool use_graph, cudaStream_t s, bool store_rhs) {
@@ -876,6 +910,7 @@ int set_initial_omega(Context* c, cudaStream_t s) {
     Ctl h{};
     h.t = 0.0; h.dt = c->cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
     NSE_CUDA_TRY(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    if (refresh_maxima(c, s)) return -1;
     NSE_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
 }

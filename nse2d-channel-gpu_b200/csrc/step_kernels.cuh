@@ -37,10 +37,14 @@ struct StageParams {
     double* rhs_out;         // optional: store rhs (the stage-3 rhs read by the diagnostics)
     const double* closure;   // optional: learned subgrid term tau [Ny][Nx], rhs -= tau on interior rows
     RowTables rt;
-    const Ctl* ctl;
+    Ctl* ctl;
     int Nx, Ny, stage, mms;
     double inv_dx, inv_deta, inv_dx2, inv_deta2, nu, lin_drag;
     double mms_A0, mms_eps, mms_Om, mms_k, mms_c;
+    // dt_from_max (stage 1): dt from the maxima the previous step's inverse transform left in
+    // ctl->mx_next (adaptive_dt); CTA 0 writes it and those maxima to the control block
+    int dt_from_max;
+    double cfl, cvisc, dx, deta, inv_dymin2, dt_max;
 };
 
 // Mapped Arakawa Jacobian (src/ops.cu:305-325) and Laplacian (src/ops.cu:488-498) from the
@@ -99,6 +103,37 @@ __device__ __forceinline__ double point_rhs(const StageParams& p, int j, int i, 
     return rhs;
 }
 
+// The larger of a and b for a >= 0 that is not NaN: a compare and a select. A NaN b is skipped
+// (as fmax skips it), and an accumulator that starts at 0 never becomes NaN.
+__device__ __forceinline__ double nn_max(double a, double b) { return b > a ? b : a; }
+__device__ __forceinline__ double warp_max_nn(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nn_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double time_tol_d(double t) { return 64.0 * 2.220446049250313e-16 * fmax(1.0, fabs(t)); }
+
+// The adaptive dt of the reference (src/main.cu:439-480) from max |u| and max |v| a: CFL limits in
+// x and eta, the viscous limit, dt_max, and the trim to the next output time. Every caller (the
+// max reduction's last CTA, the stage kernel when the maxima come from the previous step's
+// inverse transform) evaluates this one function, so dt has the same bits either way.
+__device__ __forceinline__ double adaptive_dt(double umax, double vmaxm, double t, double t_next, double cfl,
+                                             double dx, double deta, double cvisc, double nu, double inv_dx2,
+                                             double inv_dymin2, double dt_max) {
+    const double dt_x = (umax > 0 ? cfl * (dx / umax) : 1e30);
+    const double dt_y = (vmaxm > 0 ? cfl * (deta / vmaxm) : 1e30);
+    const double dt_adv = fmin(dt_x, dt_y);
+    const double dt_vis = (nu > 0) ? cvisc * 0.5 / (nu * (inv_dx2 + inv_dymin2)) : 1e30;
+    double dt = fmin(dt_max, fmin(dt_adv, dt_vis));
+    if (t_next < 1e299) {
+        const double rem = t_next - t;
+        const double tol = fmax(time_tol_d(t_next), 1e-6 * dt);
+        if (rem > tol && rem < 0.5 * dt) dt = rem;
+    }
+    return dt;
+}
+
 // ---- stage kernels: 2-D tiles of ST_TX x ST_TY points, halo of psi and omega^(s) in shared memory ----
 // 256 threads = 64 columns x 4 row groups; a thread sweeps 8 consecutive rows of one column
 // with a sliding 3-row window of psi and omega in registers (6 shared loads per point).
@@ -110,7 +145,18 @@ struct StageTime {
 };
 __device__ __forceinline__ StageTime stage_time(const StageParams& p) {
     StageTime st;
-    st.dt = p.ctl->dt;
+    if (p.dt_from_max && p.stage == 1) {
+        Ctl* c = p.ctl;
+        const double um = c->mx_next[0], vm = c->mx_next[1], vmm = c->mx_next[2];
+        st.dt = adaptive_dt(um, vmm, c->t, c->next_out, p.cfl, p.dx, p.deta, p.cvisc, p.nu, p.inv_dx2, p.inv_dymin2,
+                            p.dt_max);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {   // for the later kernels and the host; no CTA of this one reads them
+            c->dt = st.dt;
+            c->umax = um; c->vmax = vm; c->vmaxm = vmm;
+        }
+    } else {
+        st.dt = p.ctl->dt;
+    }
     const double t = p.ctl->t;
     const double ts = (p.stage == 1) ? t : (p.stage == 2 ? t + st.dt : t + 0.5 * st.dt);
     st.mA = 0.0;
@@ -466,8 +512,6 @@ static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_consta
 
 // t += dt, step++, and the snap to the scheduled output times (src/main.cu:541-551): the
 // tolerance is re-evaluated after the first snap, as the reference does.
-__device__ __forceinline__ double time_tol_d(double t) { return 64.0 * 2.220446049250313e-16 * fmax(1.0, fabs(t)); }
-
 __device__ __forceinline__ void advance_time(Ctl* ctl) {
     const double dt = ctl->dt;
     double t = ctl->t + dt;
@@ -514,6 +558,12 @@ struct FftParams {
     Ctl* ctl;
     int free_slip, closure, stage, do_thom, advance;
     double psi_bot, psi_top, invA_full;
+    // fuse_max (the stage-3 launch of an adaptive step): max |u|, |v|, |v| a of the psi written,
+    // for the next step's dt; bcount [grid + 1] arrival counters of the band boundaries
+    int fuse_max;
+    const double* a_node;
+    unsigned int* bcount;
+    double inv_dx, inv_deta;
 };
 
 
@@ -866,6 +916,86 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
 
+// The max reductions take 60-column strips per warp: lanes 1..30 own two columns each, lanes 0
+// and 31 hold the outer neighbours (k_maxuv_dt, maxuv_row).
+constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS;
+
+// max |u|, |v|, |v| a and the non-finite probe of interior row j of psi, by the warps of a CTA over
+// 60-column strips, with the arithmetic of k_maxuv_dt (the same maxima to the bit). The rows
+// j-1..j+1 are read through L2 (written earlier in the same launch). Nx even, psi 16-byte aligned.
+__device__ __forceinline__ void maxuv_row(const double* __restrict__ psi, double a, int Nx, int j, double cx, double cy,
+                                          double& um, double& vm, double& vmm, double& probe) {
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5, nw = (int)blockDim.x >> 5;
+    const double* rm = psi + (size_t)(j - 1) * Nx;
+    const double* rc = rm + Nx;
+    const double* rp = rc + Nx;
+    for (int base = warp * MX_WCOLS; base < Nx; base += nw * MX_WCOLS) {
+        const int c = base + 2 * (lane - 1);
+        const bool own = lane >= 1 && lane <= 30 && c < Nx;
+        const int ca = ((c % Nx) + Nx) % Nx;
+        const double2 wm = __ldcg(reinterpret_cast<const double2*>(rm + ca));
+        const double2 wc = __ldcg(reinterpret_cast<const double2*>(rc + ca));
+        const double2 wp = __ldcg(reinterpret_cast<const double2*>(rp + ca));
+        const double xl = __shfl_up_sync(0xffffffffu, wc.y, 1);      // column c - 1
+        const double xr = __shfl_down_sync(0xffffffffu, wc.x, 1);    // column c + 2
+        if (own) {
+            const double e0 = wp.x - wm.x, e1 = wp.y - wm.y;
+            const double f0 = wc.y - xl, f1 = xr - wc.x;
+            probe += (e0 + f0) + (e1 + f1);
+            const double dym = nn_max(fabs(e0), fabs(e1)), dxm = nn_max(fabs(f0), fabs(f1));
+            const double av = dxm * cx;
+            um = nn_max(um, a * (dym * cy));
+            vm = nn_max(vm, av);
+            vmm = nn_max(vmm, av * a);
+        }
+    }
+}
+
+// The max reduction of the rows of an inverse-transform launch whose bands hold two or more rows,
+// after the CTA has stored its band [j0, j1): the CTA reduces its rows j0 < j < j1 - 1, whose
+// neighbours it wrote; the two rows next to a band boundary (jb - 1, jb) are reduced by the second
+// of the two CTAs to arrive at that boundary's counter, which then finds both bands stored (the
+// Thom closure's arrival pattern). The CTA maxima go to the control block by atomic maxima on
+// their bit patterns; NaN or Inf sets bit 0 of the non-finite flag. All threads call it.
+__device__ __forceinline__ void band_maxuv(const FftParams& p, int j0, int j1) {
+    __shared__ int bnd[2];
+    __shared__ double red[3][IP_NT / 32];
+    const int Nx = p.Nx, Ny = p.Ny;
+    const double cx = 0.5 * p.inv_dx, cy = 0.5 * p.inv_deta;
+    double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;
+    __threadfence();                                   // this CTA's rows before its boundary arrivals
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bnd[0] = (blockIdx.x > 0) && (atomicAdd(&p.bcount[blockIdx.x], 1u) == 1u);
+        bnd[1] = (blockIdx.x + 1 < gridDim.x) && (atomicAdd(&p.bcount[blockIdx.x + 1], 1u) == 1u);
+    }
+    for (int j = max(j0 + 1, 1); j <= min(j1 - 2, Ny - 2); ++j)
+        maxuv_row(p.psi, __ldg(&p.a_node[j]), Nx, j, cx, cy, um, vm, vmm, probe);
+    __syncthreads();
+    for (int k = 0; k < 2; ++k) {
+        if (!bnd[k]) continue;
+        __threadfence();                               // the neighbour band's rows after its arrival
+        const int jb = (k == 0) ? j0 : j1;
+        for (int j = jb - 1; j <= jb; ++j)
+            if (j >= 1 && j <= Ny - 2) maxuv_row(p.psi, __ldg(&p.a_node[j]), Nx, j, cx, cy, um, vm, vmm, probe);
+    }
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5;
+    um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
+    if (lane == 0) { red[0][warp] = um; red[1][warp] = vm; red[2][warp] = vmm; }
+    const int anynf = __syncthreads_or(!(probe - probe == 0.0) || !(um <= 1e300) || !(vm <= 1e300));
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 2; ++k)
+            if (bnd[k]) p.bcount[blockIdx.x + k] = 0;  // the second arrival resets the counter
+        double m[3] = {0.0, 0.0, 0.0};
+        for (int w = 0; w < IP_NT / 32; ++w)
+            for (int q = 0; q < 3; ++q) m[q] = nn_max(m[q], red[q][w]);
+        unsigned long long* acc = p.ctl->mx_acc;
+        for (int q = 0; q < 3; ++q) atomicMax(&acc[q], (unsigned long long)__double_as_longlong(m[q]));
+        if (anynf) atomicOr(&p.ctl->nonfinite, 1);
+    }
+    __syncthreads();
+}
+
 // The forward transform at M = 2048 with its real rows prefetched the same way: a bulk copy brings
 // row j + grid's Nx reals into a shared staging buffer while row j is transformed; pass 0 reads
 // z_n = x_2n + i x_2n+1 from shared memory. The arithmetic is k_fft_fwd's (the same bits).
@@ -1016,6 +1146,7 @@ static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
         }
     }
     if (!live && threadIdx.x == 0) mbar_wait_bounded(bar, parity);   // the copy still in flight
+    if (p.fuse_max) band_maxuv(p, j0, j1);
     if (p.advance) {
         __shared__ bool last;
         __syncthreads();
@@ -1025,8 +1156,13 @@ static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
         }
         __syncthreads();
         if (last && threadIdx.x == 0) {
-            p.ctl->ifft_done = 0;
-            advance_time(p.ctl);
+            __threadfence();
+            Ctl* ctl = p.ctl;
+            ctl->ifft_done = 0;
+            if (p.fuse_max)                            // the maxima of psi^(n+1), for the next step's dt
+                for (int q = 0; q < 3; ++q)
+                    ctl->mx_next[q] = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[q], 0ull));
+            advance_time(ctl);
         }
     }
 }
@@ -1727,14 +1863,6 @@ struct MaxParams {
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
 
-// The larger of a and b for a >= 0 that is not NaN: a compare and a select. A NaN b is skipped
-// (as fmax skips it), and an accumulator that starts at 0 never becomes NaN.
-__device__ __forceinline__ double nn_max(double a, double b) { return b > a ? b : a; }
-__device__ __forceinline__ double warp_max_nn(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = nn_max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
 
 // The block maxima of one reduction CTA (warp shuffles, then the warp maxima in shared memory),
 // combined across CTAs by atomic maxima in the control block; the last CTA (a last-block
@@ -1773,20 +1901,10 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
     vmm = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[2], 0ull));
     ctl->blocks_done = 0;
     ctl->umax = um; ctl->vmax = vm; ctl->vmaxm = vmm;
+    ctl->mx_next[0] = um; ctl->mx_next[1] = vm; ctl->mx_next[2] = vmm;
     if (!p.set_dt || !p.adapt) return;
-    const double umax = um, vmaxm = vmm;
-    const double dt_x = (umax > 0 ? p.cfl * (p.dx / umax) : 1e30);
-    const double dt_y = (vmaxm > 0 ? p.cfl * (p.deta / vmaxm) : 1e30);
-    const double dt_adv = fmin(dt_x, dt_y);
-    const double dt_vis = (p.nu > 0) ? p.cvisc * 0.5 / (p.nu * (p.inv_dx2 + p.inv_dymin2)) : 1e30;
-    double dt = fmin(p.dt_max, fmin(dt_adv, dt_vis));
-    const double t_next = ctl->next_out;
-    if (t_next < 1e299) {
-        const double rem = t_next - ctl->t;
-        const double tol = fmax(time_tol_d(t_next), 1e-6 * dt);
-        if (rem > tol && rem < 0.5 * dt) dt = rem;
-    }
-    ctl->dt = dt;
+    ctl->dt = adaptive_dt(um, vmm, ctl->t, ctl->next_out, p.cfl, p.dx, p.deta, p.cvisc, p.nu, p.inv_dx2, p.inv_dymin2,
+                          p.dt_max);
 }
 
 // max |u|, |v|, |v| a over the interior (src/diag.cu:702-866).
@@ -1809,7 +1927,6 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 //
 // VEC: one 16-byte load per row (Nx even and psi 16-byte aligned); otherwise two 8-byte loads,
 // one row at a time, and any Nx >= 2 works.
-constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS;
 
 template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {

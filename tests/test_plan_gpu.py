@@ -103,3 +103,31 @@ def test_ensemble_autotune_plans_matches_solo(nse, cuda):
     ens.close()
     for m, _ in members:
         m.close()
+
+
+def test_switching_row_transform_form_mid_run(nse, cuda):
+    """At Nx = 4096 an adaptive FP64 step with the prefetching row transforms takes its max
+    reduction inside the stage-3 inverse transform, and the next step's dt from the maxima it left;
+    the other form reduces at the start of the step. Switching forms between steps (the plan change
+    refreshes the maxima of the current psi) gives the same steps to the bit, and the maxima the host
+    reads are those the last step's dt came from in either form."""
+    cfg = dict(SMALL, Nx=4096, Ny=2049, Reb=2e4, nforce=12)
+    y = np.tanh(2.0 * np.linspace(-1, 1, 2049)) / np.tanh(2.0)
+    w0 = laminar_perturbed(4096, 2049, y, seed=8, amp=5e-2)
+    a = nse.Solver(**cfg)
+    a.set_plan(rowfft_prefetch=1)
+    a.set_omega(w0)
+    b = nse.Solver(**cfg)
+    b.set_plan(rowfft_prefetch=1)
+    b.set_omega(w0)
+    seq_a, seq_b = [], []
+    for k, pf in enumerate((1, 0, 1, 1, 0)):
+        a.step(1, use_graph=True)
+        b.set_plan(rowfft_prefetch=pf)
+        b.step(1, use_graph=True)
+        seq_a.append(a.time())
+        seq_b.append(b.time())
+    assert seq_a == seq_b
+    assert np.array_equal(a.fields()[0], b.fields()[0]) and np.array_equal(a.fields()[1], b.fields()[1])
+    a.close()
+    b.close()
