@@ -135,7 +135,7 @@ int  nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters);
  * only this one); tridiag_clusters, as nse2d_set_tridiag_form; rowfft_prefetch, the row
  * transforms whose rows are prefetched into shared memory by bulk copies (1; Nx = 4096 in
  * precision 64 only) or read by plain loads (0). Every form gives the same step to round-off
- * (the stage forms and the row transform forms to the bit). nse2d_set_plan falls back to the form
+ * (the two stage forms to the bit). nse2d_set_plan falls back to the form
  * a context can use and synchronises the device when a form changes (the step graphs are
  * captured again); nse2d_get_plan reports the forms in use. */
 typedef struct nse2d_plan {

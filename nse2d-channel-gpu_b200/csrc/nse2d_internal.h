@@ -38,7 +38,7 @@ const char* step32_kernel_name(const Context* c, int k);
 int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom, bool closure, cudaStream_t s,
                      bool advance = false);
 int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s);
-int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s);
+int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s, bool next_only = false);
 int poisson_solve(Context* c, const double* w, double* psi, cudaStream_t s);
 int enqueue_step(Context* c, cudaStream_t s, bool store_rhs);
 int launches_per_step(const Context* c);

@@ -741,9 +741,9 @@ int launch_thom(Context* c, double* w, const double* psi, cudaStream_t s) {
     return 0;
 }
 
-int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s) {
+int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s, bool next_only) {
     MaxParams p{};
-    p.psi = psi; p.a_node = c->rt.a_node; p.ctl = c->ctl;
+    p.psi = psi; p.a_node = c->rt.a_node; p.ctl = c->ctl; p.next_only = next_only ? 1 : 0;
     p.Nx = c->Nx; p.Ny = c->Ny; p.adapt = c->cfg.adapt; p.set_dt = set_dt ? 1 : 0;
     p.inv_dx = c->inv_dx; p.inv_deta = c->inv_deta; p.cfl = c->cfg.cfl; p.cvisc = c->cfg.cvisc;
     p.dx = c->dx; p.deta = c->deta; p.nu = c->nu; p.inv_dx2 = c->inv_dx2; p.inv_dymin2 = c->inv_dymin2;
@@ -820,7 +820,7 @@ int launches_per_step(const Context* c) {
 // after the state is set, or the kernel plan changes.
 int refresh_maxima(Context* c, cudaStream_t s) {
     if (c->prec32 || !c->cfg.adapt) return 0;
-    return launch_maxuv(c, c->psi, false, s);
+    return launch_maxuv(c, c->psi, false, s, true);
 }
 
 // nsteps steps; with use_graph the step is captured once into a CUDA graph and replayed.

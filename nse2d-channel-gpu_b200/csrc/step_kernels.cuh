@@ -900,7 +900,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
 // (cp.async.bulk, completion on an mbarrier) brings row j+1's X_0..X_M into a shared staging
 // buffer while row j is transformed, so pass 0 reads X_n and X_{M-n} from shared memory instead
 // of waiting on global loads. Thread t takes the pass-0 butterfly t (points t + 128 r) with the
-// same merge and DFT as k_ifft_thom, so the buffer holds the same bits and psi is the same.
+// same merge and DFT as k_ifft_thom; compiled in another kernel, where the compiler may fuse other
+// multiply-adds, it gives psi to round-off (not the same bits).
 // The staging buffer is read in pass 0 only; after the barrier that ends pass 0, thread 0 issues
 // the next row's copy into it. Three CTAs of 66 KB per SM. Every wait is bounded: a wait that
 // runs out sets bit 1 of the non-finite flag, no further copy is issued, and the CTA waits once
@@ -998,7 +999,7 @@ __device__ __forceinline__ void band_maxuv(const FftParams& p, int j0, int j1) {
 
 // The forward transform at M = 2048 with its real rows prefetched the same way: a bulk copy brings
 // row j + grid's Nx reals into a shared staging buffer while row j is transformed; pass 0 reads
-// z_n = x_2n + i x_2n+1 from shared memory. The arithmetic is k_fft_fwd's (the same bits).
+// z_n = x_2n + i x_2n+1 from shared memory. The arithmetic is k_fft_fwd's, in the same order.
 template <int M> struct FftPf {
     static constexpr size_t stage_off = ((size_t)ip_size(M) * 16 + 127) / 128 * 128;
     static constexpr unsigned row_bytes = (unsigned)M * 16u;
@@ -1859,6 +1860,7 @@ struct MaxParams {
     const double* a_node;
     Ctl* ctl;
     int Nx, Ny, adapt, set_dt;
+    int next_only;                    // write the maxima only as the next step's (mx_next)
     int nstrips, nbands, band_rows;   // work items of k_maxuv_dt (maxuv_plan)
     double inv_dx, inv_deta, cfl, cvisc, dx, deta, nu, inv_dx2, inv_dymin2, dt_max;
 };
@@ -1900,8 +1902,9 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
     vm = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[1], 0ull));
     vmm = __longlong_as_double((long long)atomicExch(&ctl->mx_acc[2], 0ull));
     ctl->blocks_done = 0;
-    ctl->umax = um; ctl->vmax = vm; ctl->vmaxm = vmm;
     ctl->mx_next[0] = um; ctl->mx_next[1] = vm; ctl->mx_next[2] = vmm;
+    if (p.next_only) return;
+    ctl->umax = um; ctl->vmax = vm; ctl->vmaxm = vmm;
     if (!p.set_dt || !p.adapt) return;
     ctl->dt = adaptive_dt(um, vmm, ctl->t, ctl->next_out, p.cfl, p.dx, p.deta, p.cvisc, p.nu, p.inv_dx2, p.inv_dymin2,
                           p.dt_max);

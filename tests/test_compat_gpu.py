@@ -124,8 +124,9 @@ def test_launchers_match_reference(nse, cuda):
         call(ours, a)
         call(ref, b)
         torch.cuda.synchronize()
-        err = (a - b).abs() / b.abs().clamp_min(1e-300)
-        assert float(err.max()) <= tol, (a.tolist(), b.tolist())
+        # relative to the largest value of the output (row sums of u, v come out near zero)
+        scale = max(float(b.abs().max()), 1e-300)
+        assert float((a - b).abs().max()) <= tol * scale, (a.tolist(), b.tolist())
 
     def at(t, k):
         return ctypes.c_void_p(t.data_ptr() + 8 * k)
