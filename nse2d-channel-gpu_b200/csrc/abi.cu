@@ -254,17 +254,19 @@ int nse2d_row_moments(nse2d_ctx* ctx, double* out5, cudaStream_t s) {
 int nse2d_get_plan(nse2d_ctx* ctx, nse2d_plan* plan) {
     CHECK_CTX(ctx);
     if (!plan) { set_error("nse2d_get_plan: null plan"); return -1; }
-    const Context* c = ctx->c;
-    plan->stage_tma = (c->prec32 ? c->stage32_tma : c->stage_tma) ? 1 : 0;
-    plan->tridiag_clusters = c->thomas_cluster ? 1 : 0;
-    plan->rowfft_prefetch = c->rowfft_pf ? 1 : 0;
+    const PlanForms f = get_plan(ctx->c);
+    plan->stage_tma = f.stage_tma ? 1 : 0;
+    plan->tridiag_clusters = f.clusters ? 1 : 0;
+    plan->rowfft_prefetch = f.rowfft_pf ? 1 : 0;
+    plan->max_fused = f.max_fused ? 1 : 0;
     return 0;
 }
 
 int nse2d_set_plan(nse2d_ctx* ctx, const nse2d_plan* plan) {
     CHECK_CTX(ctx);
     if (!plan) { set_error("nse2d_set_plan: null plan"); return -1; }
-    return set_plan(ctx->c, plan->stage_tma != 0, plan->tridiag_clusters != 0, plan->rowfft_prefetch != 0);
+    return set_plan(ctx->c, PlanForms{plan->stage_tma != 0, plan->tridiag_clusters != 0, plan->rowfft_prefetch != 0,
+                                      plan->max_fused != 0});
 }
 
 // Every plan the context can use, timed over trial_steps graph-replayed steps from the current
@@ -300,26 +302,28 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
         return 0;
     };
     const bool st_ok = c->prec32 ? c->stage32_tma_ok : c->stage_tma_ok;
+    const bool mf_ok = c->rowfft_pf_ok && c->cfg.adapt && !c->prec32;   // the fused max needs the prefetching form
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) { set_error("event"); rc = -1; }
     if (rc == 0) rc = save();
     for (int st = st_ok ? 1 : 0; rc == 0 && st >= 0; --st)
         for (int cl = c->thomas_cluster_ok ? 1 : 0; rc == 0 && cl >= 0; --cl)
-            for (int pf = c->rowfft_pf_ok ? 1 : 0; rc == 0 && pf >= 0; --pf) {
-                if ((rc = set_plan(c, st, cl, pf))) break;
-                if ((rc = run_steps(c, 1, true, s, false))) break;           // capture and warm
-                cudaEventRecord(a, s);
-                if ((rc = run_steps(c, trial_steps, true, s, false))) break;
-                cudaEventRecord(b, s);
-                if (cudaEventSynchronize(b) != cudaSuccess) {
-                    set_error("nse2d_autotune_plan: %s", cudaGetErrorString(cudaGetLastError()));
-                    rc = -1;
-                    break;
+            for (int pf = c->rowfft_pf_ok ? 1 : 0; rc == 0 && pf >= 0; --pf)
+                for (int mf = (pf && mf_ok) ? 1 : 0; rc == 0 && mf >= 0; --mf) {
+                    if ((rc = set_plan(c, PlanForms{st != 0, cl != 0, pf != 0, mf != 0}))) break;
+                    if ((rc = run_steps(c, 1, true, s, false))) break;           // capture and warm
+                    cudaEventRecord(a, s);
+                    if ((rc = run_steps(c, trial_steps, true, s, false))) break;
+                    cudaEventRecord(b, s);
+                    if (cudaEventSynchronize(b) != cudaSuccess) {
+                        set_error("nse2d_autotune_plan: %s", cudaGetErrorString(cudaGetLastError()));
+                        rc = -1;
+                        break;
+                    }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, a, b);
+                    if (ms / trial_steps < best_ms) { best_ms = ms / trial_steps; bp = nse2d_plan{st, cl, pf, mf}; }
+                    if ((rc = restore())) break;
                 }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, a, b);
-                if (ms / trial_steps < best_ms) { best_ms = ms / trial_steps; bp = nse2d_plan{st, cl, pf}; }
-                if ((rc = restore())) break;
-            }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     if (rc == 0) rc = restore();
@@ -328,7 +332,7 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
     if (rc) return rc;
     if (best) *best = bp;
     if (ms_per_step) *ms_per_step = best_ms;
-    return set_plan(c, bp.stage_tma != 0, bp.tridiag_clusters != 0, bp.rowfft_prefetch != 0);
+    return set_plan(c, PlanForms{bp.stage_tma != 0, bp.tridiag_clusters != 0, bp.rowfft_prefetch != 0, bp.max_fused != 0});
 }
 
 int nse2d_stats_device(nse2d_ctx* ctx, int every, cudaStream_t s) {

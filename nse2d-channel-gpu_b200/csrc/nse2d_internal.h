@@ -26,7 +26,10 @@ int setup32(Context* c);
 // Select the cluster (clusters != 0, where available) or the two-pass tridiagonal solve; drops
 // the context's captured step graphs when the form changes (solver.cu).
 int set_tridiag_form(Context* c, bool clusters);
-int set_plan(Context* c, bool stage_tma, bool clusters, bool rowfft_pf);
+// the kernel forms of a context's step (nse2d_plan)
+struct PlanForms { bool stage_tma, clusters, rowfft_pf, max_fused; };
+PlanForms get_plan(const Context* c);
+int set_plan(Context* c, const PlanForms& f);
 int refresh_maxima(Context* c, cudaStream_t s);
 // 2-D tensor map of a [Ny][Nx] FP64 (or FP32) field with a bw x bh box (solver.cu).
 int encode_map_2d(CUtensorMap* map, const void* base, bool f32, int Nx, int Ny, int bw, int bh);

@@ -493,7 +493,7 @@ void context_destroy(Context* c) {
 
 // The max reduction of an adaptive FP64 step runs in its stage-3 inverse transform when that is the
 // prefetching form (k_ifft_thom_pf); the stage-1 kernel then takes dt from the maxima it left.
-static bool fused_max(const Context* c) { return c->cfg.adapt && !c->prec32 && c->rowfft_pf; }
+static bool fused_max(const Context* c) { return c->cfg.adapt && !c->prec32 && c->rowfft_pf && c->max_fused; }
 
 // ---- launchers ----
 static StageParams stage_params(Context* c) {
@@ -685,18 +685,25 @@ int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
 
 // The kernel forms of the step (each falls back to the one the context can use); drops the
 // captured graphs when anything changes.
-int set_plan(Context* c, bool stage_tma, bool clusters, bool rowfft_pf) {
-    const bool st = stage_tma && (c->prec32 ? c->stage32_tma_ok : c->stage_tma_ok);
-    const bool pf = rowfft_pf && c->rowfft_pf_ok;
+PlanForms get_plan(const Context* c) {
+    return PlanForms{c->prec32 ? c->stage32_tma : c->stage_tma, c->thomas_cluster, c->rowfft_pf, fused_max(c)};
+}
+
+int set_plan(Context* c, const PlanForms& f) {
+    const bool st = f.stage_tma && (c->prec32 ? c->stage32_tma_ok : c->stage_tma_ok);
+    const bool pf = f.rowfft_pf && c->rowfft_pf_ok;
     const bool cur = c->prec32 ? c->stage32_tma : c->stage_tma;
-    if (st != cur || pf != c->rowfft_pf) {
+    const bool fused_before = fused_max(c);
+    const bool fused_after = c->cfg.adapt && !c->prec32 && pf && f.max_fused;
+    if (st != cur || pf != c->rowfft_pf || fused_before != fused_after) {
         NSE_CUDA_TRY(cudaDeviceSynchronize());
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
         if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
         if (c->prec32) c->stage32_tma = st; else c->stage_tma = st;
         c->rowfft_pf = pf;
     }
-    if (set_tridiag_form(c, clusters)) return -1;
+    c->max_fused = f.max_fused;
+    if (set_tridiag_form(c, f.clusters)) return -1;
     // the next step may take its dt from the maxima of the current psi
     if (refresh_maxima(c, 0)) return -1;
     NSE_CUDA_TRY(cudaDeviceSynchronize());

@@ -918,68 +918,90 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 
 // The max reductions take 60-column strips per warp: lanes 1..30 own two columns each, lanes 0
-// and 31 hold the outer neighbours (k_maxuv_dt, maxuv_row).
+// and 31 hold the outer neighbours (k_maxuv_dt, maxuv_rows).
 constexpr int MX_WCOLS = 60, MX_COLS = 8 * MX_WCOLS;
 
-// max |u|, |v|, |v| a and the non-finite probe of interior row j of psi, by the warps of a CTA over
-// 60-column strips, with the arithmetic of k_maxuv_dt (the same maxima to the bit). The rows
-// j-1..j+1 are read through L2 (written earlier in the same launch). Nx even, psi 16-byte aligned.
-__device__ __forceinline__ void maxuv_row(const double* __restrict__ psi, double a, int Nx, int j, double cx, double cy,
-                                          double& um, double& vm, double& vmm, double& probe) {
+// max |u|, |v|, |v| a and the non-finite probe of the interior rows ja..jb of psi, by the warps of a
+// CTA over 60-column strips, with the per-point arithmetic of k_maxuv_dt (the same maxima for the
+// same psi). A strip's rows ja-1..jb+1 (at most MX_RB + 2 at a time) and two strips per warp are
+// loaded before any is reduced, so up to 2 (MX_RB + 2) 16-byte loads per lane are in flight: the
+// rows were written earlier in the same launch and come from L2, where the reduction is bound by
+// latency. Nx even, psi 16-byte aligned; all threads of the CTA call it with the same ja, jb.
+constexpr int MX_RB = 8;
+__device__ __forceinline__ void maxuv_rows(const double* __restrict__ psi, const double* __restrict__ a_node, int Nx,
+                                           int ja, int jb, double cx, double cy,
+                                           double& um, double& vm, double& vmm, double& probe) {
     const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5, nw = (int)blockDim.x >> 5;
-    const double* rm = psi + (size_t)(j - 1) * Nx;
-    const double* rc = rm + Nx;
-    const double* rp = rc + Nx;
-    for (int base = warp * MX_WCOLS; base < Nx; base += nw * MX_WCOLS) {
-        const int c = base + 2 * (lane - 1);
-        const bool own = lane >= 1 && lane <= 30 && c < Nx;
-        const int ca = ((c % Nx) + Nx) % Nx;
-        const double2 wm = __ldcg(reinterpret_cast<const double2*>(rm + ca));
-        const double2 wc = __ldcg(reinterpret_cast<const double2*>(rc + ca));
-        const double2 wp = __ldcg(reinterpret_cast<const double2*>(rp + ca));
-        const double xl = __shfl_up_sync(0xffffffffu, wc.y, 1);      // column c - 1
-        const double xr = __shfl_down_sync(0xffffffffu, wc.x, 1);    // column c + 2
-        if (own) {
-            const double e0 = wp.x - wm.x, e1 = wp.y - wm.y;
-            const double f0 = wc.y - xl, f1 = xr - wc.x;
-            probe += (e0 + f0) + (e1 + f1);
-            const double dym = nn_max(fabs(e0), fabs(e1)), dxm = nn_max(fabs(f0), fabs(f1));
-            const double av = dxm * cx;
-            um = nn_max(um, a * (dym * cy));
-            vm = nn_max(vm, av);
-            vmm = nn_max(vmm, av * a);
+    for (int j = ja; j <= jb; j += MX_RB) {
+        const int n = min(MX_RB, jb - j + 1);          // rows j..j+n-1, loads of rows j-1..j+n
+        const double* r0 = psi + (size_t)(j - 1) * Nx;
+        for (int base = warp * MX_WCOLS; base < Nx; base += 2 * nw * MX_WCOLS) {
+            double2 w[2][MX_RB + 2];
+            int ca[2];
+            bool own[2];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int c = base + s * nw * MX_WCOLS + 2 * (lane - 1);
+                own[s] = lane >= 1 && lane <= 30 && c < Nx;
+                ca[s] = ((c % Nx) + Nx) % Nx;
+            }
+            const bool second = base + nw * MX_WCOLS < Nx;   // warp-uniform
+#pragma unroll
+            for (int r = 0; r < MX_RB + 2; ++r)
+                if (r < n + 2) {
+                    w[0][r] = __ldcg(reinterpret_cast<const double2*>(r0 + (size_t)r * Nx + ca[0]));
+                    if (second) w[1][r] = __ldcg(reinterpret_cast<const double2*>(r0 + (size_t)r * Nx + ca[1]));
+                }
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                if (s == 1 && !second) break;
+#pragma unroll
+                for (int r = 1; r <= MX_RB; ++r) {
+                    if (r > n) break;
+                    const double2 wm = w[s][r - 1], wc = w[s][r], wp = w[s][r + 1];
+                    const double xl = __shfl_up_sync(0xffffffffu, wc.y, 1);      // column c - 1
+                    const double xr = __shfl_down_sync(0xffffffffu, wc.x, 1);    // column c + 2
+                    if (own[s]) {
+                        const double a = __ldg(&a_node[j + r - 1]);
+                        const double e0 = wp.x - wm.x, e1 = wp.y - wm.y;
+                        const double f0 = wc.y - xl, f1 = xr - wc.x;
+                        probe += (e0 + f0) + (e1 + f1);
+                        const double dym = nn_max(fabs(e0), fabs(e1)), dxm = nn_max(fabs(f0), fabs(f1));
+                        const double av = dxm * cx;
+                        um = nn_max(um, a * (dym * cy));
+                        vm = nn_max(vm, av);
+                        vmm = nn_max(vmm, av * a);
+                    }
+                }
+            }
         }
     }
 }
 
 // The max reduction of the rows of an inverse-transform launch whose bands hold two or more rows,
-// after the CTA has stored its band [j0, j1): the CTA reduces its rows j0 < j < j1 - 1, whose
-// neighbours it wrote; the two rows next to a band boundary (jb - 1, jb) are reduced by the second
-// of the two CTAs to arrive at that boundary's counter, which then finds both bands stored (the
-// Thom closure's arrival pattern). The CTA maxima go to the control block by atomic maxima on
-// their bit patterns; NaN or Inf sets bit 0 of the non-finite flag. All threads call it.
+// after the CTA has stored its band [j0, j1). The two rows next to a band boundary (jb - 1, jb)
+// are reduced by the second of the two CTAs to arrive at that boundary's counter, which then
+// finds both bands stored (the Thom closure's arrival pattern, with no waiting); the CTA's rows
+// j0 < j < j1 - 1 have their neighbours in its own band. So a CTA reduces one contiguous range of
+// rows: from j0 - 1 (it arrived second at its lower boundary) or j0 + 1, to j1 (second at its
+// upper boundary) or j1 - 2. The CTA maxima go to the control block by atomic maxima on their bit
+// patterns; NaN or Inf sets bit 0 of the non-finite flag. All threads call it.
 __device__ __forceinline__ void band_maxuv(const FftParams& p, int j0, int j1) {
     __shared__ int bnd[2];
     __shared__ double red[3][IP_NT / 32];
-    const int Nx = p.Nx, Ny = p.Ny;
-    const double cx = 0.5 * p.inv_dx, cy = 0.5 * p.inv_deta;
+    const int Ny = p.Ny;
     double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;
     __threadfence();                                   // this CTA's rows before its boundary arrivals
     __syncthreads();
     if (threadIdx.x == 0) {
         bnd[0] = (blockIdx.x > 0) && (atomicAdd(&p.bcount[blockIdx.x], 1u) == 1u);
         bnd[1] = (blockIdx.x + 1 < gridDim.x) && (atomicAdd(&p.bcount[blockIdx.x + 1], 1u) == 1u);
+        if (bnd[0] || bnd[1]) __threadfence();         // the neighbour band's rows after its arrival
     }
-    for (int j = max(j0 + 1, 1); j <= min(j1 - 2, Ny - 2); ++j)
-        maxuv_row(p.psi, __ldg(&p.a_node[j]), Nx, j, cx, cy, um, vm, vmm, probe);
     __syncthreads();
-    for (int k = 0; k < 2; ++k) {
-        if (!bnd[k]) continue;
-        __threadfence();                               // the neighbour band's rows after its arrival
-        const int jb = (k == 0) ? j0 : j1;
-        for (int j = jb - 1; j <= jb; ++j)
-            if (j >= 1 && j <= Ny - 2) maxuv_row(p.psi, __ldg(&p.a_node[j]), Nx, j, cx, cy, um, vm, vmm, probe);
-    }
+    const int ja = max(bnd[0] ? j0 - 1 : j0 + 1, 1);
+    const int jb = min(bnd[1] ? j1 : j1 - 2, Ny - 2);
+    if (ja <= jb) maxuv_rows(p.psi, p.a_node, p.Nx, ja, jb, 0.5 * p.inv_dx, 0.5 * p.inv_deta, um, vm, vmm, probe);
     const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5;
     um = warp_max_nn(um); vm = warp_max_nn(vm); vmm = warp_max_nn(vmm);
     if (lane == 0) { red[0][warp] = um; red[1][warp] = vm; red[2][warp] = vmm; }

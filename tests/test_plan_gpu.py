@@ -139,3 +139,17 @@ def test_switching_row_transform_form_mid_run(nse, cuda):
     assert_fields_close(wa, pa, wb, pb, np.diff(y), 1e-12)
     a.close()
     b.close()
+
+
+def test_fused_max_same_bits_at_4096(nse, cuda):
+    """The max reduction inside the stage-3 inverse transform evaluates the per-point maxima of the
+    separate reduction, and the stage kernel's dt the same adaptive_dt: the same steps to the bit."""
+    cfg = dict(SMALL, Nx=4096, Ny=2049, Reb=2e4, nforce=12)
+    y = np.tanh(2.0 * np.linspace(-1, 1, 2049)) / np.tanh(2.0)
+    w0 = laminar_perturbed(4096, 2049, y, seed=6, amp=5e-2)
+    (wa, pa), ta, p = run_with(nse, cfg, w0, 3, rowfft_prefetch=1, max_fused=1)
+    assert p["rowfft_prefetch"] == 1 and p["max_fused"] == 1
+    (wb, pb), tb, p = run_with(nse, cfg, w0, 3, rowfft_prefetch=1, max_fused=0)
+    assert p["rowfft_prefetch"] == 1 and p["max_fused"] == 0
+    assert ta == tb
+    assert np.array_equal(wa, wb) and np.array_equal(pa, pb)
