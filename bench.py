@@ -681,11 +681,13 @@ def profile_steps(args):
         W["Nx"], W["Ny"] = args.nx, args.ny
     y = tanh_y(W["Ny"], W["beta"], W["h"])
     s = nse.Solver(precision=args.precision, **W)
+    if args.plan:
+        s.set_plan(**{k: int(v) for k, v in (kv.split("=") for kv in args.plan.split(","))})
     s.set_omega(initial_vorticity(W["Nx"], W["Ny"], W["Lx"], y, seed=1))
     s.step(args.profile_steps, use_graph=False)
     torch.cuda.synchronize()
     t, dt, n, m = s.time()
-    print(json.dumps({"profile_steps": n, "t": t, "dt": dt, "umax": m[0], "nonfinite": s.nonfinite()}))
+    print(json.dumps({"profile_steps": n, "t": t, "dt": dt, "umax": m[0], "nonfinite": s.nonfinite(), "plan": s.plan()}))
     s.close()
 
 
@@ -693,6 +695,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="untimed run of K plain steps for a profiler (no JSON bench line)")
+    ap.add_argument("--plan", default="",
+                    help="profile runs: kernel forms as key=value pairs, e.g. rowfft_prefetch=1,max_fused=0")
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--gpus", type=int, default=1)

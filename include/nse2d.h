@@ -137,12 +137,15 @@ int  nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters);
  * precision 64 only) or read by plain loads (0); max_fused, with the prefetching transforms in an
  * adaptive FP64 step, the max reduction of psi inside the stage-3 inverse transform and dt
  * computed by the next step's stage kernel (1) or a separate max reduction at the start of the
- * step (0). Every form gives the same step to round-off (the two stage forms and the two max
- * forms to the bit). nse2d_set_plan falls back to the form a context can use and synchronises
- * the device when a form changes (the step graphs are captured again); nse2d_get_plan reports
- * the forms in use (max_fused as it takes effect). */
+ * step (0); pdl, the FP64 step kernels launched with programmatic dependent launch (1: a
+ * kernel's CTAs become resident while the one before it finishes, and wait on the device for its
+ * completion before they read or write anything) or in plain stream order (0). Every form gives
+ * the same step to round-off (the two stage forms, the two max forms and the two launch forms
+ * to the bit). nse2d_set_plan falls back to the form a context can use and synchronises the
+ * device when a form changes (the step graphs are captured again); nse2d_get_plan reports the
+ * forms in use (max_fused as it takes effect). */
 typedef struct nse2d_plan {
-    int stage_tma, tridiag_clusters, rowfft_prefetch, max_fused;
+    int stage_tma, tridiag_clusters, rowfft_prefetch, max_fused, pdl;
 } nse2d_plan;
 int  nse2d_get_plan(nse2d_ctx* ctx, nse2d_plan* plan);
 int  nse2d_set_plan(nse2d_ctx* ctx, const nse2d_plan* plan);

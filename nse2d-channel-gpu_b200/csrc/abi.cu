@@ -259,6 +259,7 @@ int nse2d_get_plan(nse2d_ctx* ctx, nse2d_plan* plan) {
     plan->tridiag_clusters = f.clusters ? 1 : 0;
     plan->rowfft_prefetch = f.rowfft_pf ? 1 : 0;
     plan->max_fused = f.max_fused ? 1 : 0;
+    plan->pdl = f.pdl ? 1 : 0;
     return 0;
 }
 
@@ -266,7 +267,7 @@ int nse2d_set_plan(nse2d_ctx* ctx, const nse2d_plan* plan) {
     CHECK_CTX(ctx);
     if (!plan) { set_error("nse2d_set_plan: null plan"); return -1; }
     return set_plan(ctx->c, PlanForms{plan->stage_tma != 0, plan->tridiag_clusters != 0, plan->rowfft_prefetch != 0,
-                                      plan->max_fused != 0});
+                                      plan->max_fused != 0, plan->pdl != 0});
 }
 
 // Every plan the context can use, timed over trial_steps graph-replayed steps from the current
@@ -308,8 +309,9 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
     for (int st = st_ok ? 1 : 0; rc == 0 && st >= 0; --st)
         for (int cl = c->thomas_cluster_ok ? 1 : 0; rc == 0 && cl >= 0; --cl)
             for (int pf = c->rowfft_pf_ok ? 1 : 0; rc == 0 && pf >= 0; --pf)
-                for (int mf = (pf && mf_ok) ? 1 : 0; rc == 0 && mf >= 0; --mf) {
-                    if ((rc = set_plan(c, PlanForms{st != 0, cl != 0, pf != 0, mf != 0}))) break;
+                for (int mf = (pf && mf_ok) ? 1 : 0; rc == 0 && mf >= 0; --mf)
+                for (int pd = c->prec32 ? 0 : 1; rc == 0 && pd >= 0; --pd) {
+                    if ((rc = set_plan(c, PlanForms{st != 0, cl != 0, pf != 0, mf != 0, pd != 0}))) break;
                     if ((rc = run_steps(c, 1, true, s, false))) break;           // capture and warm
                     cudaEventRecord(a, s);
                     if ((rc = run_steps(c, trial_steps, true, s, false))) break;
@@ -321,7 +323,7 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
                     }
                     float ms = 0.f;
                     cudaEventElapsedTime(&ms, a, b);
-                    if (ms / trial_steps < best_ms) { best_ms = ms / trial_steps; bp = nse2d_plan{st, cl, pf, mf}; }
+                    if (ms / trial_steps < best_ms) { best_ms = ms / trial_steps; bp = nse2d_plan{st, cl, pf, mf, pd}; }
                     if ((rc = restore())) break;
                 }
     if (a) cudaEventDestroy(a);
@@ -332,7 +334,8 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
     if (rc) return rc;
     if (best) *best = bp;
     if (ms_per_step) *ms_per_step = best_ms;
-    return set_plan(c, PlanForms{bp.stage_tma != 0, bp.tridiag_clusters != 0, bp.rowfft_prefetch != 0, bp.max_fused != 0});
+    return set_plan(c, PlanForms{bp.stage_tma != 0, bp.tridiag_clusters != 0, bp.rowfft_prefetch != 0, bp.max_fused != 0,
+                                 bp.pdl != 0});
 }
 
 int nse2d_stats_device(nse2d_ctx* ctx, int every, cudaStream_t s) {

@@ -594,8 +594,20 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
             const float* r1 = p.psi + (size_t)(top ? Ny - 2 : 1) * Nx;
             const float* r2 = p.psi + (size_t)(top ? Ny - 3 : 2) * Nx;
             float* wr = p.w + (size_t)(top ? Ny - 1 : 0) * Nx;
-            for (int i = threadIdx.x; i < Nx; i += IP_NT)
-                wr[i] = p.free_slip ? base : base - (A * __ldcg(&r1[i]) + B * __ldcg(&r2[i]));
+            // the loads of 8 columns per thread in flight before any store (one CTA writes the row)
+            for (int i0 = threadIdx.x; i0 < Nx; i0 += 8 * IP_NT) {
+                float a1[8], a2[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int i = i0 + c * IP_NT;
+                    if (i < Nx) { a1[c] = __ldcg(&r1[i]); a2[c] = __ldcg(&r2[i]); }
+                }
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int i = i0 + c * IP_NT;
+                    if (i < Nx) wr[i] = p.free_slip ? base : base - (A * a1[c] + B * a2[c]);
+                }
+            }
         }
     }
     if (p.advance) {

@@ -193,27 +193,27 @@ int nse2d_ensemble_autotune_plans(nse2d_ensemble* en, int trial_steps, int* grou
     }
     auto plan_of = [](const Context* c, bool* v) {
         const PlanForms f = get_plan(c);
-        v[0] = f.stage_tma; v[1] = f.clusters; v[2] = f.rowfft_pf; v[3] = f.max_fused;
+        v[0] = f.stage_tma; v[1] = f.clusters; v[2] = f.rowfft_pf; v[3] = f.max_fused; v[4] = f.pdl;
     };
     double best = 0.0;
     int rc = time_step(best);
     for (size_t k = 0; rc == 0 && k < cls.size(); ++k) {
         Context* c0 = cls[k].m[0];
-        const bool ok[4] = {c0->prec32 ? c0->stage32_tma_ok : c0->stage_tma_ok, c0->thomas_cluster_ok, c0->rowfft_pf_ok,
-                            c0->rowfft_pf_ok && c0->cfg.adapt && !c0->prec32};
-        for (int f = 0; rc == 0 && f < 4; ++f) {
+        const bool ok[5] = {c0->prec32 ? c0->stage32_tma_ok : c0->stage_tma_ok, c0->thomas_cluster_ok, c0->rowfft_pf_ok,
+                            c0->rowfft_pf_ok && c0->cfg.adapt && !c0->prec32, !c0->prec32};
+        for (int f = 0; rc == 0 && f < 5; ++f) {
             if (!ok[f]) continue;
-            bool v[4];
+            bool v[5];
             plan_of(c0, v);
             v[f] = !v[f];
             for (Context* c : cls[k].m)
-                if ((rc = set_plan(c, PlanForms{v[0], v[1], v[2], v[3]}))) break;
+                if ((rc = set_plan(c, PlanForms{v[0], v[1], v[2], v[3], v[4]}))) break;
             double ms = 0.0;
             if (rc == 0) rc = time_step(ms);
             if (rc == 0 && !(ms < best)) {                       // not faster: undo
                 v[f] = !v[f];
                 for (Context* c : cls[k].m)
-                    if ((rc = set_plan(c, PlanForms{v[0], v[1], v[2], v[3]}))) break;
+                    if ((rc = set_plan(c, PlanForms{v[0], v[1], v[2], v[3], v[4]}))) break;
             } else if (rc == 0) {
                 best = ms;
             }

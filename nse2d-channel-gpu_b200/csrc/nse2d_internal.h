@@ -27,7 +27,7 @@ int setup32(Context* c);
 // the context's captured step graphs when the form changes (solver.cu).
 int set_tridiag_form(Context* c, bool clusters);
 // the kernel forms of a context's step (nse2d_plan)
-struct PlanForms { bool stage_tma, clusters, rowfft_pf, max_fused; };
+struct PlanForms { bool stage_tma, clusters, rowfft_pf, max_fused, pdl; };
 PlanForms get_plan(const Context* c);
 int set_plan(Context* c, const PlanForms& f);
 int refresh_maxima(Context* c, cudaStream_t s);

@@ -496,6 +496,26 @@ void context_destroy(Context* c) {
 static bool fused_max(const Context* c) { return c->cfg.adapt && !c->prec32 && c->rowfft_pf && c->max_fused; }
 
 // ---- launchers ----
+// A step kernel (each begins with pdl_begin), with the programmatic-serialisation attribute when
+// the plan asks for it; extra: another launch attribute (the cluster shape), or nullptr.
+template <typename... KArgs, typename... Args>
+static int launch_step_kernel(const Context* c, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, const cudaLaunchAttribute* extra, Args&&... args) {
+    cudaLaunchConfig_t lc{};
+    cudaLaunchAttribute at[2];
+    unsigned na = 0;
+    if (extra) at[na++] = *extra;
+    if (c->pdl) {
+        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    lc.gridDim = grid; lc.blockDim = block; lc.dynamicSmemBytes = smem; lc.stream = s;
+    lc.attrs = at; lc.numAttrs = na;
+    NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, std::forward<Args>(args)...));
+    return 0;
+}
+
 static StageParams stage_params(Context* c) {
     StageParams p{};
     p.psi = c->psi; p.rt = c->rt; p.ctl = c->ctl;
@@ -533,13 +553,11 @@ int launch_stage(Context* c, int stage, const double* w_in, const double* w_n, d
         else if (w_in == c->w1) maps.w = c->tm_w[1];
         else if (w_in == c->w2) maps.w = c->tm_w[2];
         else { set_error("launch_stage: omega^(s) is not a context buffer"); return -1; }
-        k_stage_tma<<<c->stage_tma_grid, 256, stage_tma_smem_bytes(), s>>>(maps, p);
-    } else {
-        const dim3 grid((c->Nx + ST_TX - 1) / ST_TX, (c->Ny + ST_TY - 1) / ST_TY);
-        k_stage<<<grid, 256, 0, s>>>(p);
+        return launch_step_kernel(c, k_stage_tma, dim3(c->stage_tma_grid), dim3(256), stage_tma_smem_bytes(), s, nullptr,
+                                  maps, p);
     }
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    const dim3 grid((c->Nx + ST_TX - 1) / ST_TX, (c->Ny + ST_TY - 1) / ST_TY);
+    return launch_step_kernel(c, k_stage, grid, dim3(256), 0, s, nullptr, p);
 }
 
 static size_t fft_smem(int M) { return fft_smem_bytes(M); }
@@ -572,16 +590,12 @@ template <int M> static int fft_fwd_t(Context* c, FftParams& p, cudaStream_t s) 
         const size_t sm = FftPf<M>::smem;
         int grid = 0;
         if (fft_wave(k_fft_fwd_pf<M>, sm, p.nrows, c->num_sms, &grid)) return -1;
-        k_fft_fwd_pf<M><<<grid, IP_NT, sm, s>>>(p);
-        NSE_CUDA_TRY(cudaGetLastError());
-        return 0;
+        return launch_step_kernel(c, k_fft_fwd_pf<M>, dim3(grid), dim3(IP_NT), sm, s, nullptr, p);
     }
     const size_t sm = fft_smem(M);
     int grid = 0;
     if (fft_wave(k_fft_fwd<M>, sm, p.nrows, c->num_sms, &grid)) return -1;
-    k_fft_fwd<M><<<grid, IP_NT, sm, s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_fft_fwd<M>, dim3(grid), dim3(IP_NT), sm, s, nullptr, p);
 }
 
 // Inverse transforms: one wave of CTAs over contiguous bands of floor or ceil(Ny / wave) rows
@@ -594,17 +608,14 @@ template <int M> static int fft_inv_t(Context* c, FftParams& p, cudaStream_t s) 
         const size_t sm = IfftPf<M>::smem;
         int wave = 0;
         if (fft_wave(k_ifft_thom_pf<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
-        k_ifft_thom_pf<M><<<std::max(1, std::min(wave, c->Ny / 2)), IP_NT, sm, s>>>(p);
-        NSE_CUDA_TRY(cudaGetLastError());
-        return 0;
+        return launch_step_kernel(c, k_ifft_thom_pf<M>, dim3(std::max(1, std::min(wave, c->Ny / 2))), dim3(IP_NT), sm, s,
+                                  nullptr, p);
     }
     const size_t sm = fft_smem(M);
     int wave = 0;
     if (fft_wave(k_ifft_thom<M>, sm, c->Ny, c->num_sms, &wave)) return -1;
     const int grid = std::max(1, std::min(wave, c->Ny));           // bands of Ny / grid rows (even split)
-    k_ifft_thom<M><<<grid, IP_NT, sm, s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_ifft_thom<M>, dim3(grid), dim3(IP_NT), sm, s, nullptr, p);
 }
 
 #define NSE_FFT_DISPATCH(FN)                                                       \
@@ -656,37 +667,30 @@ int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom
 // The two passes of the segmented Thomas solve: the segment maps (and, in the last CTA of each
 // column group, the carries), then the rerun of every segment from its carries.
 int launch_thomas_maps(Context* c, cudaStream_t s, bool homog) {
-    k_thomas_maps<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c, homog));
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_thomas_maps, dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
+                              thomas_smem_bytes(), s, nullptr, thomas_params(c, homog));
 }
 int launch_thomas_apply(Context* c, cudaStream_t s, bool homog) {
-    k_thomas_apply<<<c->thomas_groups * c->thomas_nsb, TS_NW * 32, thomas_smem_bytes(), s>>>(thomas_params(c, homog));
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_thomas_apply, dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
+                              thomas_smem_bytes(), s, nullptr, thomas_params(c, homog));
 }
 // The one-pass form: one cluster of tc_cluster CTAs per 8-kx column group.
 int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
-    cudaLaunchConfig_t lc{};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = c->tc_cluster; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-    lc.gridDim = dim3(c->tc_cluster * c->tc_nclusters);       // persistent: the resident clusters
-    lc.blockDim = dim3(TC_THREADS);
-    lc.dynamicSmemBytes = c->tc_smem;
-    lc.stream = s;
-    lc.attrs = at; lc.numAttrs = 1;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = c->tc_cluster; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
     ThomasMaps maps;
     maps.hat = c->tm_hat;
     maps.cp = c->tm_cp;
-    NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, thomas_cluster_kernel(c->tc_L), maps, thomas_params(c, homog)));
-    return 0;
+    // persistent: the resident clusters
+    return launch_step_kernel(c, thomas_cluster_kernel(c->tc_L), dim3(c->tc_cluster * c->tc_nclusters),
+                              dim3(TC_THREADS), c->tc_smem, s, &at, maps, thomas_params(c, homog));
 }
 
 // The kernel forms of the step (each falls back to the one the context can use); drops the
 // captured graphs when anything changes.
 PlanForms get_plan(const Context* c) {
-    return PlanForms{c->prec32 ? c->stage32_tma : c->stage_tma, c->thomas_cluster, c->rowfft_pf, fused_max(c)};
+    return PlanForms{c->prec32 ? c->stage32_tma : c->stage_tma, c->thomas_cluster, c->rowfft_pf, fused_max(c), c->pdl};
 }
 
 int set_plan(Context* c, const PlanForms& f) {
@@ -695,12 +699,14 @@ int set_plan(Context* c, const PlanForms& f) {
     const bool cur = c->prec32 ? c->stage32_tma : c->stage_tma;
     const bool fused_before = fused_max(c);
     const bool fused_after = c->cfg.adapt && !c->prec32 && pf && f.max_fused;
-    if (st != cur || pf != c->rowfft_pf || fused_before != fused_after) {
+    const bool pdl = f.pdl && !c->prec32;
+    if (st != cur || pf != c->rowfft_pf || fused_before != fused_after || pdl != c->pdl) {
         NSE_CUDA_TRY(cudaDeviceSynchronize());
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
         if (c->run_exec) { cudaGraphExecDestroy(c->run_exec); c->run_exec = nullptr; }
         if (c->prec32) c->stage32_tma = st; else c->stage_tma = st;
         c->rowfft_pf = pf;
+        c->pdl = pdl;
     }
     c->max_fused = f.max_fused;
     if (set_tridiag_form(c, f.clusters)) return -1;
@@ -757,9 +763,7 @@ int launch_maxuv(Context* c, const double* psi, bool set_dt, cudaStream_t s, boo
     p.dt_max = c->cfg.dt_max;
     int grid = 1;
     maxuv_plan(p, c->maxuv_ctas, c->maxuv_ctas, grid);
-    k_maxuv_dt<true><<<grid, 256, 0, s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_maxuv_dt<true>, dim3(grid), dim3(256), 0, s, nullptr, p);
 }
 
 // Poisson solve of the reference (src/poisson.cuh:83-118): omega -> psi.

@@ -106,6 +106,16 @@ __device__ __forceinline__ double point_rhs(const StageParams& p, int j, int i, 
 // The larger of a and b for a >= 0 that is not NaN: a compare and a select. A NaN b is skipped
 // (as fmax skips it), and an accumulator that starts at 0 never becomes NaN.
 __device__ __forceinline__ double nn_max(double a, double b) { return b > a ? b : a; }
+
+// Programmatic dependent launch: a step kernel launched with the programmatic-serialisation
+// attribute may become resident while the kernel before it in the stream is still running.
+// Every step kernel begins with pdl_begin: it waits until the grids it depends on have completed
+// and their writes are visible (a no-op for a kernel launched without the attribute), then lets
+// the next kernel be scheduled, whose CTAs take the SM resources this grid's CTAs free and wait
+// in the same way. Nothing is read or written before the wait.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
 __device__ __forceinline__ double warp_max_nn(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = nn_max(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -266,6 +276,7 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageTime
 static __global__ void __launch_bounds__(256) k_stage(StageParams p) {
     __shared__ double sp[ST_H][ST_W + 1];
     __shared__ double so[ST_H][ST_W + 1];
+    pdl_begin();
     const int Nx = p.Nx, Ny = p.Ny;
     const int x0 = blockIdx.x * ST_TX, y0 = blockIdx.y * ST_TY;
     // all halo loads of a thread are issued before any of them is stored (fixed trip count)
@@ -442,6 +453,7 @@ __device__ __forceinline__ void stage_tile2(const StageParams& p, const StageTim
 
 static __global__ void __launch_bounds__(256, 2) k_stage_tma(const __grid_constant__ StageMaps maps, StageParams p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
+    pdl_begin();
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ double srow[2][4][ST_TY];                // per buffer: the row tables of its tile
     // the boxes land at 128-byte aligned shared addresses
@@ -649,6 +661,7 @@ __device__ __forceinline__ void fwd_last_pass_split(const cpx<T>* buf, const cpx
 template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const int je = p.row0 + p.nrows;
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
@@ -708,8 +721,12 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_fft_fwd(FftParams p) {
 }
 
 // Thom wall vorticity of one wall (src/ops.cu:114-151) from the psi rows this CTA just wrote,
-// with the closure_diag enstrophy jump of the wall row (src/main.cu:271-298).
-template <int NT>
+// with the closure_diag enstrophy jump of the wall row (src/main.cu:271-298). One CTA writes the
+// whole wall row while the other CTAs of the launch finish their bands, so its loads (psi rows
+// from L2, the old wall row) are issued CH columns per thread at a time, all before any store:
+// a loop of one column per iteration would wait for L2 once per column and hold the whole launch
+// up by tens of microseconds at Nx = 4096. CH is set by the caller's register budget.
+template <int NT, int CH>
 __device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
     const int Nx = p.Nx, Ny = p.Ny;
     const double d1 = top ? p.dy_edge[Ny - 2] : p.dy_edge[0];
@@ -722,13 +739,28 @@ __device__ __forceinline__ void thom_row(const FftParams& p, bool top) {
     double* wr = p.w + (size_t)(top ? Ny - 1 : 0) * Nx;
     const double wq = p.closure ? p.w_node[top ? Ny - 1 : 0] : 0.0;
     double sb = 0.0, sa = 0.0;
-    for (int i = threadIdx.x; i < Nx; i += NT) {
-        double nv = 0.0;
-        if (!p.free_slip) nv = -(A * (__ldcg(&r1[i]) - pw) + B * (__ldcg(&r2[i]) - pw));
-        const double ov = wr[i];
-        wr[i] = nv;
-        sb += wq * ov * ov;
-        sa += wq * nv * nv;
+    for (int i0 = threadIdx.x; i0 < Nx; i0 += NT * CH) {
+        double a1[CH], a2[CH], ov[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int i = i0 + c * NT;
+            if (i < Nx) {
+                a1[c] = __ldcg(&r1[i]);
+                a2[c] = __ldcg(&r2[i]);
+                ov[c] = wr[i];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int i = i0 + c * NT;
+            if (i < Nx) {
+                double nv = 0.0;
+                if (!p.free_slip) nv = -(A * (a1[c] - pw) + B * (a2[c] - pw));
+                wr[i] = nv;
+                sb += wq * ov[c] * ov[c];
+                sa += wq * nv * nv;
+            }
+        }
     }
     if (!p.closure) return;
     __shared__ double rb[NT], ra[NT];
@@ -758,6 +790,7 @@ __host__ __device__ __forceinline__ void band_of(int b, int nb, int L, int Ny, i
 template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     __shared__ bool thom_now;
     const int Nx = p.Nx, Ny = p.Ny;
@@ -872,7 +905,7 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom(FftParams p) {
                     __syncthreads();
                     if (thom_now) {
                         __threadfence();
-                        thom_row<IP_NT>(p, wall == 1);
+                        thom_row<IP_NT, 2>(p, wall == 1);
                         if (threadIdx.x == 0) p.ctl->thom_done[wall] = 0;
                     }
                     __syncthreads();
@@ -1033,6 +1066,7 @@ template <int M>
 static __global__ void __launch_bounds__(IP_NT, 3) k_fft_fwd_pf(FftParams p) {
     static_assert(M / 16 == IP_NT && p16_plan<M>::R(0) == 16 && M == 16 * IP_NT, "one pass-0 butterfly per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const double2* stage = reinterpret_cast<const double2*>(smem_raw + FftPf<M>::stage_off);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + FftPf<M>::bar_off);
@@ -1087,6 +1121,7 @@ template <int M>
 static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
     static_assert(M / 16 == IP_NT && p16_plan<M>::R(0) == 16 && p16_plan<M>::P >= 2, "one pass-0 butterfly per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];   // offsets: stage at 128 B, barrier at 16 B multiples
+    pdl_begin();
     cpx<double>* buf = reinterpret_cast<cpx<double>*>(smem_raw);
     const double2* stage = reinterpret_cast<const double2*>(smem_raw + IfftPf<M>::stage_off);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + IfftPf<M>::bar_off);
@@ -1160,7 +1195,7 @@ static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
                     __syncthreads();
                     if (thom_now) {
                         __threadfence();
-                        thom_row<IP_NT>(p, wall == 1);
+                        thom_row<IP_NT, 8>(p, wall == 1);
                         if (threadIdx.x == 0) p.ctl->thom_done[wall] = 0;
                     }
                     __syncthreads();
@@ -1345,6 +1380,7 @@ __device__ __forceinline__ void thomas_seg_maps(const ThomasParams& p, int s, in
 
 static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = blockIdx.x / p.nsb, sb = blockIdx.x - g * p.nsb;
@@ -1458,6 +1494,7 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams 
 
 static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     __shared__ double segm[TS_NW][5 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = blockIdx.x / p.nsb, sb = blockIdx.x - g * p.nsb;
@@ -1614,6 +1651,7 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_dyn[];
+    pdl_begin();
     __shared__ __align__(8) uint64_t bars[2];            // TMA buffers
     __shared__ __align__(8) uint64_t xbar[2][2];         // [direction 0 forward | 1 backward][group parity]
     __shared__ double2 wD[TC_NW][TC_KX];                 // per-warp aggregates of a scan
@@ -1955,6 +1993,7 @@ __device__ __forceinline__ void maxuv_finish(const MaxParams& p, double um, doub
 
 template <bool VEC>
 static __global__ void __launch_bounds__(256, 3) k_maxuv_dt(MaxParams p) {
+    pdl_begin();
     const int Nx = p.Nx, Ny = p.Ny;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double um = 0.0, vm = 0.0, vmm = 0.0, probe = 0.0;

@@ -45,7 +45,7 @@ class Config(ctypes.Structure):
 class Plan(ctypes.Structure):
     """struct nse2d_plan: the kernel forms of a context's step."""
     _fields_ = [("stage_tma", ctypes.c_int), ("tridiag_clusters", ctypes.c_int), ("rowfft_prefetch", ctypes.c_int),
-                ("max_fused", ctypes.c_int)]
+                ("max_fused", ctypes.c_int), ("pdl", ctypes.c_int)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -427,12 +427,12 @@ class Solver:
         _check(self.lib.nse2d_set_tridiag_form(self.h, 1 if clusters else 0))
 
     def plan(self):
-        """The kernel forms in use: {stage_tma, tridiag_clusters, rowfft_prefetch, max_fused}."""
+        """The kernel forms in use: {stage_tma, tridiag_clusters, rowfft_prefetch, max_fused, pdl}."""
         pl = Plan()
         _check(self.lib.nse2d_get_plan(self.h, ctypes.byref(pl)))
         return pl.as_dict()
 
-    def set_plan(self, stage_tma=None, tridiag_clusters=None, rowfft_prefetch=None, max_fused=None):
+    def set_plan(self, stage_tma=None, tridiag_clusters=None, rowfft_prefetch=None, max_fused=None, pdl=None):
         """Select kernel forms (None keeps the current one; max_fused None asks for the fused max
         reduction wherever it applies); forms the grid cannot use fall back."""
         cur = self.plan()
@@ -440,7 +440,7 @@ class Solver:
             max_fused = 1
         pl = Plan(**{k: int(v if v is not None else cur[k]) for k, v in
                      (("stage_tma", stage_tma), ("tridiag_clusters", tridiag_clusters),
-                      ("rowfft_prefetch", rowfft_prefetch), ("max_fused", max_fused))})
+                      ("rowfft_prefetch", rowfft_prefetch), ("max_fused", max_fused), ("pdl", pdl))})
         _check(self.lib.nse2d_set_plan(self.h, ctypes.byref(pl)))
 
     def autotune_plan(self, trial_steps=10, stream=None):

@@ -7,7 +7,9 @@ The forms of each part of the step compute the same arithmetic:
     the same order as the plain ones, compiled in other kernels (where the compiler may fuse
     other multiply-adds): dt, maxima and fields to round-off (1e-12, the wall rows to the
     Thom-gain bound);
-  - the two tridiagonal forms reassociate the recurrences differently: round-off (1e-12).
+  - the two tridiagonal forms reassociate the recurrences differently: round-off (1e-12);
+  - the two max forms and the two launch forms (programmatic dependent launch or stream order)
+    give the same bits.
 nse2d_autotune_plan restores the state it tried the plans on (to the bit), and after
 nse2d_ensemble_autotune_plans every member steps exactly as a solo channel with its plan.
 """
@@ -152,4 +154,29 @@ def test_fused_max_same_bits_at_4096(nse, cuda):
     (wb, pb), tb, p = run_with(nse, cfg, w0, 3, rowfft_prefetch=1, max_fused=0)
     assert p["rowfft_prefetch"] == 1 and p["max_fused"] == 0
     assert ta == tb
+    assert np.array_equal(wa, wb) and np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("Nx,Ny", [(256, 129), (4096, 2049)])
+def test_programmatic_launch_same_bits(nse, cuda, Nx, Ny):
+    """With programmatic dependent launch every step kernel waits on the device for the kernel
+    before it to complete before it reads or writes anything: the same steps to the bit, through
+    plain launches, the one-step graph and the run graph (a WHILE node)."""
+    cfg = dict(SMALL, Nx=Nx, Ny=Ny, Reb=2e4 if Nx == 4096 else SMALL["Reb"], nforce=12 if Nx == 4096 else 8)
+    y = np.tanh(2.0 * np.linspace(-1, 1, Ny)) / np.tanh(2.0)
+    w0 = laminar_perturbed(Nx, Ny, y, seed=9, amp=5e-2)
+    out = {}
+    for pdl in (1, 0):
+        g = nse.Solver(**cfg)
+        g.set_plan(pdl=pdl)
+        assert g.plan()["pdl"] == pdl
+        g.set_omega(w0)
+        g.step(1, use_graph=False)
+        g.step(2, use_graph=True)
+        g.run(max_steps=3)
+        out[pdl] = (g.fields(), g.time())
+        g.close()
+    (wa, pa), ta = out[1]
+    (wb, pb), tb = out[0]
+    assert ta == tb and ta[2] == 6
     assert np.array_equal(wa, wb) and np.array_equal(pa, pb)
