@@ -48,9 +48,10 @@ __host__ __device__ constexpr int ip_size(int M) {
 //
 // Pass q >= 1 (radix R, sub-transform length LP = 16^q before it, L = R LP), for every group g
 // and m < LP: x_r = buf[g L + m + r LP] times W_L^(r m), an R-point DFT, written back in place.
-// The output is in natural order. Its twiddles come from a table of (W^m, W^2m, W^4m, W^8m),
-// m < LP; W^(r m) is applied as W^(a m) W^(4 b m) with r = a + 4 b, so that at most six
-// twiddles are live at a time.
+// The output is in natural order. Its twiddles come from four tables of W^m, W^2m, W^4m and
+// W^8m, m < LP (one after the other, so that the lanes of a warp, which take consecutive m,
+// read consecutive entries); W^(r m) is applied as W^(a m) W^(4 b m) with r = a + 4 b, so that
+// at most six twiddles are live at a time.
 // ---------------------------------------------------------------------------------------
 template <int M> struct p16_plan {
     static constexpr int m = ilog2<M>::v;
@@ -85,8 +86,8 @@ inline void p16_twiddle_table(int M, const C* tw, std::vector<C>& out) {
     const int P = (m + 3) / 4;
     for (int q = 1; q < P; ++q) {
         const int LP = 1 << (4 * q), R = 1 << ((q < P - 1) ? 4 : m - 4 * (P - 1)), L = R * LP, step = M / L;
-        for (int k = 0; k < LP; ++k)
-            for (int e = 1; e <= 8; e *= 2) out.push_back(tw[((long long)e * step * k) % M]);
+        for (int e = 1; e <= 8; e *= 2)
+            for (int k = 0; k < LP; ++k) out.push_back(tw[((long long)e * step * k) % M]);
     }
     if (out.empty()) out.push_back(tw[0]);
 }
@@ -116,22 +117,22 @@ __device__ __forceinline__ int p16_bfly(const cpx<T>* __restrict__ buf, const cp
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = buf[ip_idx<M>(base + r * LP)];
     if (mm > 0) {
-        const int t = OFF + 4 * mm;
+        const int t = OFF + mm;
         const cpx<T> w1 = ldtw(tw, t);
         if constexpr (R == 2) {
             v[1] = p16_tw<T, INV>(v[1], w1);
         } else {
-            const cpx<T> w2 = ldtw(tw, t + 1), w3 = cmul(w1, w2);
+            const cpx<T> w2 = ldtw(tw, t + LP), w3 = cmul(w1, w2);
 #pragma unroll
             for (int r = 1; r < R; ++r) {                  // low digit a = r mod 4
                 const int a = r & 3;
                 if (a) v[r] = p16_tw<T, INV>(v[r], a == 1 ? w1 : (a == 2 ? w2 : w3));
             }
             if constexpr (R >= 8) {                        // high digit b = r / 4
-                const cpx<T> w4 = ldtw(tw, t + 2);
+                const cpx<T> w4 = ldtw(tw, t + 2 * LP);
                 cpx<T> w8 = w4, w12 = w4;
                 if constexpr (R == 16) {
-                    w8 = ldtw(tw, t + 3);
+                    w8 = ldtw(tw, t + 3 * LP);
                     w12 = cmul(w4, w8);
                 }
 #pragma unroll
