@@ -17,9 +17,11 @@
 //       +2 D wbar Dx psi'_j + d+ wbar Dx psi'_{j+1} + d- wbar Dx psi'_{j-1},
 //     D f = f_{j+1} - f_{j-1}, d+ f = f_{j+1} - f_j, d- f = f_j - f_{j-1}; the base's Laplacian,
 //     forcing and drag enter as one FP64 row constant R_j.
-//   - Poisson: FP32 row transforms (k_fft_fwd32 / k_ifft_thom32) with the spectral buffer and the
-//     whole tridiagonal solve in FP64 (homogeneous Dirichlet for psi', including kx = 0, whose
-//     operator is the badly conditioned one).
+//   - Poisson: FP32 row transforms (k_fft_fwd32 / k_ifft_thom32) and an FP32 spectral buffer; the
+//     tridiagonal solve widens the spectra on load and runs in FP64 with the FP64 elimination table
+//     (homogeneous Dirichlet for psi', including kx = 0). Rounding the right-hand side and the
+//     solution to FP32 perturbs psi' by ~1e-8 relative at every kx, while an FP32 table or FP32
+//     sweeps would lose 1e-6 .. 1e-4 at the low kx, whose operators are badly conditioned.
 //   - Thom: w'_wall = [Thom(psibar) - wbar]_wall (FP64 constant) - (A psi'_1 + B psi'_2).
 //   - dt: the max reduction over FP32 psi' plus the FP64 base slope.
 // The FP64 fields of the context are filled from the split state (export) for diagnostics and
@@ -410,10 +412,10 @@ static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_cons
     }
 }
 
-// ---- FP32 row transforms, FP64 spectral buffer ----
+// ---- FP32 row transforms, FP32 spectral buffer ----
 struct Fft32Params {
     const float* src;          // forward: rows of w'
-    cpx<double>* hat;          // [Ny][Hp], FP64
+    cpx<float>* hat;           // [Ny][Hp], FP32
     float* psi;                // inverse output psi'
     float* w;                  // inverse: w'^(s+1), whose wall rows the Thom closure sets
     const cpx<float>* tw;      // per-pass twiddles of the radix-16 plan (p16_twiddle_table), FP32
@@ -452,14 +454,14 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
         }
         __syncthreads();
         if constexpr (M == 16 * IP_NT) {                // the fused last pass and split (see k_fft_fwd)
-            double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+            float2* dst = reinterpret_cast<float2*>(p.hat + (size_t)j * p.Hp);
             p16_pass<float, M, 1, false, IP_NT>(buf, p.tw);
             __syncthreads();
             fwd_last_pass_split<float, M>(buf, p.tw, p.wN, dst);
         } else {
             p16_passes_from<float, M, 1, false, IP_NT>(buf, p.tw);
             // the split step for the pair (k, M - k) (see k_fft_fwd)
-            double2* dst = reinterpret_cast<double2*>(p.hat + (size_t)j * p.Hp);
+            float2* dst = reinterpret_cast<float2*>(p.hat + (size_t)j * p.Hp);
             auto split = [&](int k, const cpx<float>& wk) {             // wk = W^k / 2 (see k_fft_fwd)
                 const int kb = (k == 0 ? 0 : M - k);
                 const cpx<float> a = buf[ip_idx<M>(k)];
@@ -467,12 +469,12 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
                 const cpx<float> sm = {0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
                 const cpx<float> df = {a.x - b.x, a.y + b.y};
                 const cpx<float> X = cadd(sm, cmul(wk, mul_mi(df)));
-                dst[k] = make_double2((double)X.x, (double)X.y);
+                dst[k] = make_float2(X.x, X.y);
                 if (k < M / 2) {
                     const int m = M - k;
                     const cpx<float> wm = {-wk.x, wk.y};                          // W^{M-k} = -conj(W^k)
                     const cpx<float> Y = cadd(cpx<float>{sm.x, -sm.y}, cmul(wm, cpx<float>{df.y, df.x}));
-                    dst[m] = make_double2((double)Y.x, (double)Y.y);
+                    dst[m] = make_float2(Y.x, Y.y);
                 }
             };
             for (int k = threadIdx.x; k <= M / 2; k += IP_NT) {
@@ -501,25 +503,19 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
             continue;
         }
         // pass 0 from global with the merge (see k_ifft_thom)
-        const double2* X = reinterpret_cast<const double2*>(p.hat + (size_t)j * p.Hp);
+        const float2* X = reinterpret_cast<const float2*>(p.hat + (size_t)j * p.Hp);
         if constexpr (kPairLanes) {
             // mirror lanes, as in k_ifft_thom: lanes 0..15 of warp w take butterflies 16 w + l,
             // lanes 16..31 the mirrors 128 - b (64 for lane 16 of warp 0); each lane loads its
-            // own 16 points (rounded to FP32) and takes the mirror points X_{M-n} by shuffle
+            // own 16 points and takes the mirror points X_{M-n} by shuffle
             const int w = (int)threadIdx.x >> 5, l = (int)threadIdx.x & 31;
             int b = (l < 16) ? 16 * w + l : 128 - (16 * w + l - 16);
             if (b == 128) b = 64;
             float2 x[16];
 #pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                const double2 d = __ldcs(X + b + 128 * r);
-                x[r] = make_float2((float)d.x, (float)d.y);
-            }
+            for (int r = 0; r < 16; ++r) x[r] = __ldcs(X + b + 128 * r);
             float2 xM = make_float2(0.f, 0.f);
-            if (b == 0) {
-                const double2 d = __ldcs(X + M);
-                xM = make_float2((float)d.x, (float)d.y);
-            }
+            if (b == 0) xM = __ldcs(X + M);
             const cpx<float> wt = ldtw(p.wN, b);        // W_{2M}^{b + 128 r} = W_{2M}^b e^{-i pi r/16}
             auto merge = [&](const float2& av, const float2& bv, int r) {
                 const cpx<float> a = {av.x, av.y}, c = {bv.x, -bv.y};
@@ -554,8 +550,8 @@ static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) 
 #pragma unroll
                 for (int r = 0; r < R0; ++r) {
                     const int n = t + NB0 * r;
-                    const double2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
-                    const cpx<float> a = {(float)av.x, (float)av.y}, b = {(float)bv.x, -(float)bv.y};
+                    const float2 av = __ldcs(X + n), bv = __ldcs(X + (M - n));
+                    const cpx<float> a = {av.x, av.y}, b = {bv.x, -bv.y};
                     const cpx<float> E = {a.x + b.x, a.y + b.y};
                     const cpx<float> D = {a.x - b.x, a.y - b.y};
                     v[r] = cadd(E, mul_pi(cmulc(D, ldtw(p.wN, n))));

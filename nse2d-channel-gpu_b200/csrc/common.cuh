@@ -144,6 +144,11 @@ struct Context {
     int tc_cluster = 0, tc_L = 0, tc_nclusters = 0;
     size_t tc_smem = 0;
     CUtensorMap tm_hat{}, tm_cp{};
+    // precision 32: the FP32 spectral buffer [Ny][Hp] and the cluster solve's map and sizes for it
+    cpx<float>* hat32 = nullptr;
+    CUtensorMap tm_hat32{};
+    size_t tc_smem32 = 0;
+    int tc_nclusters32 = 0;
     int num_sms = 0;
     int maxuv_ctas = 0;            // resident CTAs of k_maxuv_dt (occupancy x SMs)
     // learned closure: the model evaluated before every stage and its output tau [Ny][Nx]

@@ -97,21 +97,24 @@ static int context_metrics(const Config& c, std::vector<double>& y, std::vector<
 }
 
 using ThomasClusterKernel = void (*)(ThomasMaps, ThomasParams);
-static ThomasClusterKernel thomas_cluster_kernel(int L) {
+template <bool F32> static ThomasClusterKernel thomas_cluster_kernel_t(int L) {
     switch (L) {
-        case 1: return k_thomas_cluster<1>;
-        case 2: return k_thomas_cluster<2>;
-        case 4: return k_thomas_cluster<4>;
-        case 8: return k_thomas_cluster<8>;
-        case 16: return k_thomas_cluster<16>;
+        case 1: return k_thomas_cluster<1, F32>;
+        case 2: return k_thomas_cluster<2, F32>;
+        case 4: return k_thomas_cluster<4, F32>;
+        case 8: return k_thomas_cluster<8, F32>;
+        case 16: return k_thomas_cluster<16, F32>;
         default: return nullptr;
     }
 }
+static ThomasClusterKernel thomas_cluster_kernel(int L, bool f32 = false) {
+    return f32 ? thomas_cluster_kernel_t<true>(L) : thomas_cluster_kernel_t<false>(L);
+}
 
-// homog: zero wall values of psi (the FP32 variant solves for psi', which vanishes on the walls)
+// homog: the FP32-bulk step's solve, for psi' (zero on the walls) in the FP32 spectral buffer
 static ThomasParams thomas_params(const Context* c, bool homog = false) {
     ThomasParams p{};
-    p.hat = c->hat; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
+    p.hat = c->hat; p.hat32 = c->hat32; p.cp = c->cp; p.asub = c->rt.asub; p.inv_csup = c->rt.inv_csup; p.csup = c->rt.csup;
     p.tconst = c->tconst; p.tmaps = c->tmaps; p.tblk = c->tblk; p.tbcarry = c->tbcarry; p.tcount = c->tcount;
     p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.H = c->H; p.Ni = c->Ni;
     p.nseg = c->thomas_nseg; p.nsb = c->thomas_nsb;
@@ -366,8 +369,10 @@ int context_create(const Config& cfg, Context** out) {
         set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail();
     }
-    if (cudaFuncSetAttribute(k_thomas_maps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes()) ||
-        cudaFuncSetAttribute(k_thomas_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes())) {
+    if (cudaFuncSetAttribute(k_thomas_maps<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes()) ||
+        cudaFuncSetAttribute(k_thomas_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes()) ||
+        cudaFuncSetAttribute(k_thomas_maps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes()) ||
+        cudaFuncSetAttribute(k_thomas_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)thomas_smem_bytes())) {
         set_error("cudaFuncSetAttribute (Thomas shared memory) failed: %s", cudaGetErrorString(cudaGetLastError()));
         return fail();
     }
@@ -454,6 +459,30 @@ int context_create(const Config& cfg, Context** out) {
     if (cfg.precision == 32) {
         c->prec32 = true;
         if (setup32(c)) return fail();
+        // the cluster solve over the FP32 spectral buffer (setup32 allocated it)
+        if (c->thomas_cluster_ok) {
+            const int R = TC_NSEG * c->tc_L, C = c->tc_cluster;
+            const size_t smem = tc_smem_bytes(R, true);
+            ThomasClusterKernel kern = thomas_cluster_kernel(c->tc_L, true);
+            cudaLaunchConfig_t lc{};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            lc.gridDim = dim3(C * (c->Hp / TC_KX));
+            lc.blockDim = dim3(TC_THREADS);
+            lc.dynamicSmemBytes = smem;
+            lc.attrs = at; lc.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+                encode_map_2d(&c->tm_hat32, c->hat32, true, 2 * c->Hp, Ny, 2 * TC_KX, std::min(R, TC_BOX)) != 0 ||
+                cudaOccupancyMaxActiveClusters(&nclusters, kern, &lc) != cudaSuccess || nclusters < 1) {
+                // the FP64 spectra's cluster form is resident, so this one (less shared memory) is too
+                set_error("the FP32-spectra cluster solve cannot be set up: %s", cudaGetErrorString(cudaGetLastError()));
+                return fail();
+            }
+            c->tc_smem32 = smem;
+            c->tc_nclusters32 = std::min(nclusters, c->Hp / TC_KX);
+        }
     }
     Ctl h{};
     h.t = 0.0; h.dt = cfg.dt_init; h.next_out = 1e300; h.next_snap = 1e300; h.next_diag = 1e300;
@@ -667,11 +696,13 @@ int launch_ifft_thom(Context* c, double* psi, double* w, int stage, bool do_thom
 // The two passes of the segmented Thomas solve: the segment maps (and, in the last CTA of each
 // column group, the carries), then the rerun of every segment from its carries.
 int launch_thomas_maps(Context* c, cudaStream_t s, bool homog) {
-    return launch_step_kernel(c, k_thomas_maps, dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
+    return launch_step_kernel(c, homog ? k_thomas_maps<true> : k_thomas_maps<false>,
+                              dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
                               thomas_smem_bytes(), s, nullptr, thomas_params(c, homog));
 }
 int launch_thomas_apply(Context* c, cudaStream_t s, bool homog) {
-    return launch_step_kernel(c, k_thomas_apply, dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
+    return launch_step_kernel(c, homog ? k_thomas_apply<true> : k_thomas_apply<false>,
+                              dim3(c->thomas_groups * c->thomas_nsb), dim3(TS_NW * 32),
                               thomas_smem_bytes(), s, nullptr, thomas_params(c, homog));
 }
 // The one-pass form: one cluster of tc_cluster CTAs per 8-kx column group.
@@ -680,11 +711,12 @@ int launch_thomas_cluster(Context* c, cudaStream_t s, bool homog) {
     at.id = cudaLaunchAttributeClusterDimension;
     at.val.clusterDim.x = c->tc_cluster; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
     ThomasMaps maps;
-    maps.hat = c->tm_hat;
+    maps.hat = homog ? c->tm_hat32 : c->tm_hat;
     maps.cp = c->tm_cp;
     // persistent: the resident clusters
-    return launch_step_kernel(c, thomas_cluster_kernel(c->tc_L), dim3(c->tc_cluster * c->tc_nclusters),
-                              dim3(TC_THREADS), c->tc_smem, s, &at, maps, thomas_params(c, homog));
+    const int ncl = homog ? c->tc_nclusters32 : c->tc_nclusters;
+    return launch_step_kernel(c, thomas_cluster_kernel(c->tc_L, homog), dim3(c->tc_cluster * ncl), dim3(TC_THREADS),
+                              homog ? c->tc_smem32 : c->tc_smem, s, &at, maps, thomas_params(c, homog));
 }
 
 // The kernel forms of the step (each falls back to the one the context can use); drops the

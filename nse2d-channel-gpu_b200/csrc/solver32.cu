@@ -20,7 +20,8 @@ template <typename T> static int alloc(T** p, size_t n) {
 int setup32(Context* c) {
     const size_t N = c->N;
     if (alloc(&c->wf, N) || alloc(&c->w1f, N) || alloc(&c->w2f, N) || alloc(&c->psif, N) || alloc(&c->rhsf, N) ||
-        alloc(&c->wbar, (size_t)c->Ny) || alloc(&c->psibar, (size_t)c->Ny) || alloc(&c->rc32, (size_t)RC32_N * c->Ny))
+        alloc(&c->wbar, (size_t)c->Ny) || alloc(&c->psibar, (size_t)c->Ny) || alloc(&c->rc32, (size_t)RC32_N * c->Ny) ||
+        alloc(&c->hat32, (size_t)c->Ny * c->Hp))
         return -1;
     // FP32 twiddles: the FP64 values rounded, in the same per-pass layout
     const long double PI = 3.141592653589793238462643383279502884L;
@@ -72,7 +73,7 @@ int setup32(Context* c) {
 
 void destroy32(Context* c) {
     for (void* p : {(void*)c->wf, (void*)c->w1f, (void*)c->w2f, (void*)c->psif, (void*)c->rhsf, (void*)c->wbar,
-                    (void*)c->psibar, (void*)c->rc32, (void*)c->twf, (void*)c->wNf})
+                    (void*)c->psibar, (void*)c->rc32, (void*)c->twf, (void*)c->wNf, (void*)c->hat32})
         if (p) cudaFree(p);
 }
 
@@ -115,7 +116,7 @@ int export32(Context* c, bool with_rhs, cudaStream_t s) {
 
 static Fft32Params fft32_params(Context* c) {
     Fft32Params p{};
-    p.hat = c->hat; p.tw = c->twf; p.wN = c->wNf; p.dy_edge = c->rt.dy_edge; p.ctl = c->ctl;
+    p.hat = c->hat32; p.tw = c->twf; p.wN = c->wNf; p.dy_edge = c->rt.dy_edge; p.ctl = c->ctl;
     p.Nx = c->Nx; p.Ny = c->Ny; p.Hp = c->Hp; p.free_slip = c->cfg.free_slip;
     p.wall_bot = c->wall_bot32; p.wall_top = c->wall_top32;
     return p;

@@ -617,9 +617,9 @@ __host__ __device__ constexpr size_t fft_smem_bytes(int M) { return (size_t)ip_s
 //           pairs with itself), and k = 128 + 256 r with Z_{M-k} = B[7 - r];  r = 0..3.
 // X_k and X_{M-k} leave from registers; the split twiddles W_2M^k come from W_2M^t and the
 // e^{-i pi j/16} constants. The buffer is only read here.
-template <typename T, int M>
+template <typename T, int M, typename D2>
 __device__ __forceinline__ void fwd_last_pass_split(const cpx<T>* buf, const cpx<T>* tw, const cpx<T>* wN,
-                                                    double2* dst) {
+                                                    D2* dst) {
     static_assert(M == 16 * IP_NT && p16_plan<M>::P == 3 && p16_plan<M>::R(2) == 8 && p16_plan<M>::LP(2) == 256,
                   "the fused split is written for M = 2048 (passes 16, 16, 8)");
     const int t = threadIdx.x;
@@ -632,11 +632,11 @@ __device__ __forceinline__ void fwd_last_pass_split(const cpx<T>* buf, const cpx
         const cpx<T> sm = {(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
         const cpx<T> df = {a.x - b.x, a.y + b.y};
         const cpx<T> X = cadd(sm, cmul(wk, mul_mi(df)));
-        dst[k] = make_double2((double)X.x, (double)X.y);
+        dst[k] = D2{X.x, X.y};
         if (k < M / 2) {
             const cpx<T> wm = {-wk.x, wk.y};
             const cpx<T> Y = cadd(cpx<T>{sm.x, -sm.y}, cmul(wm, cpx<T>{df.y, df.x}));
-            dst[M - k] = make_double2((double)Y.x, (double)Y.y);
+            dst[M - k] = D2{Y.x, Y.y};
         }
     };
     const cpx<T> w1 = ldtw(wN, t);
@@ -1227,6 +1227,7 @@ static __global__ void __launch_bounds__(IP_NT, 3) k_ifft_thom_pf(FftParams p) {
 
 struct ThomasParams {
     cpx<double>* hat;        // [Ny][Hp], in place: omega-hat in, psi-hat out
+    cpx<float>* hat32;       // the same in FP32 (the FP32-bulk step; the arithmetic stays FP64)
     const double* cp;        // [Ni][Hp]
     const double* asub;      // [Ny]
     const double* inv_csup;  // [Ny]
@@ -1240,6 +1241,17 @@ struct ThomasParams {
     double psi_bot, psi_top;
     Ctl* ctl;                // error flags (bounded TMA waits of the cluster solve)
 };
+
+// Spectral values of the solve: FP64 storage, or FP32 storage widened on load and rounded on
+// store (F32), with FP64 arithmetic either way.
+template <bool F32> struct SpecT { using T = double; using T2 = double2; };
+template <> struct SpecT<true> { using T = float; using T2 = float2; };
+__device__ __forceinline__ double2 spec_wide(const double2& v) { return v; }
+__device__ __forceinline__ double2 spec_wide(const float2& v) { return make_double2((double)v.x, (double)v.y); }
+template <bool F32> __device__ __forceinline__ typename SpecT<F32>::T2 spec_narrow(double x, double y) {
+    if constexpr (F32) return make_float2((float)x, (float)y);
+    else return make_double2(x, y);
+}
 
 // Thomas sweeps of the reference (src/poisson.cu:70-133), split into segments of TS_ROWS rows.
 //
@@ -1336,14 +1348,30 @@ __device__ __forceinline__ void thomas_stage_warp_rows(const ThomasParams& p, un
     }
 }
 
+template <bool F32>
 __device__ __forceinline__ void thomas_issue_loads(const ThomasParams& p, int r0, int n, int g, const ThomasTile& tl) {
-    const double* hatd = reinterpret_cast<const double*>(p.hat);
     const size_t rowstride = (size_t)p.Hp * 2;
     const int lane = threadIdx.x & 31;
+    if constexpr (F32) {
+        // FP32 spectra: plain 16-byte loads of four values, widened into the FP64 tile
+        const float* hatf = reinterpret_cast<const float*>(p.hat32);
 #pragma unroll
-    for (int i = 0; i < TS_ROWS / 2; ++i) {             // 16 chunks of 16 bytes per row
-        const int ch = lane + 32 * i, row = ch >> 4, part = ch & 15;
-        if (row < n) cp_async16(&tl.v[row * 32 + part * 2], &hatd[(size_t)(r0 + row + 1) * rowstride + (size_t)g * 32 + part * 2]);
+        for (int i = 0; i < TS_ROWS / 4; ++i) {         // 8 chunks of 16 bytes per row
+            const int ch = lane + 32 * i, row = ch >> 3, part = ch & 7;
+            if (row < n) {
+                const float4 v = __ldcg(reinterpret_cast<const float4*>(
+                    &hatf[(size_t)(r0 + row + 1) * rowstride + (size_t)g * 32 + part * 4]));
+                double* d = &tl.v[row * 32 + part * 4];
+                d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+            }
+        }
+    } else {
+        const double* hatd = reinterpret_cast<const double*>(p.hat);
+#pragma unroll
+        for (int i = 0; i < TS_ROWS / 2; ++i) {         // 16 chunks of 16 bytes per row
+            const int ch = lane + 32 * i, row = ch >> 4, part = ch & 15;
+            if (row < n) cp_async16(&tl.v[row * 32 + part * 2], &hatd[(size_t)(r0 + row + 1) * rowstride + (size_t)g * 32 + part * 2]);
+        }
     }
 #pragma unroll
     for (int i = 0; i < TS_ROWS / 4; ++i) {             // 8 chunks per row
@@ -1378,6 +1406,7 @@ __device__ __forceinline__ void thomas_seg_maps(const ThomasParams& p, int s, in
     cp_async8(&e[4 * 32 + lane], &p.tmaps[((size_t)s * 2 + 1) * cols + col]);
 }
 
+template <bool F32>
 static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pdl_begin();
@@ -1393,7 +1422,7 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams 
     const int r0 = s * TS_ROWS, n = (s < p.nseg) ? min(TS_ROWS, p.Ni - r0) : 0;
     double Ps = 0.0, Vs = 0.0, Qs = 0.0;
     if (s < p.nseg) {
-        thomas_issue_loads(p, r0, n, g, tl);
+        thomas_issue_loads<F32>(p, r0, n, g, tl);
         thomas_stage_warp_rows(p, smem_raw, s);
         Ps = __ldg(&p.tconst[((size_t)s * 3 + 0) * p.Hp + kx]);
         Vs = __ldg(&p.tconst[((size_t)s * 3 + 1) * p.Hp + kx]);
@@ -1492,6 +1521,7 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_maps(ThomasParams 
     if (threadIdx.x == 0) p.tcount[g] = 0;      // ready for the next solve
 }
 
+template <bool F32>
 static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pdl_begin();
@@ -1506,7 +1536,7 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams
     const ThomasTile tl = thomas_tile(smem_raw, warp);
     const int r0 = s * TS_ROWS, n = (s < p.nseg) ? min(TS_ROWS, p.Ni - r0) : 0;
     if (s < p.nseg) {
-        thomas_issue_loads(p, r0, n, g, tl);
+        thomas_issue_loads<F32>(p, r0, n, g, tl);
         thomas_stage_warp_rows(p, smem_raw, s);
         thomas_seg_maps(p, s, kx, col, lane, segm[warp]);
     }
@@ -1533,17 +1563,18 @@ static __global__ void __launch_bounds__(TS_NW * 32) k_thomas_apply(ThomasParams
     for (int w = 0; w < TS_NW; ++w)
         if (w == warp) cw = cs[w];
     thomas_forward(p, r0, n, kx0re, cw, tl);
-    double* hatw = reinterpret_cast<double*>(p.hat);
+    using ST = typename SpecT<F32>::T;
+    ST* hatw = F32 ? reinterpret_cast<ST*>(p.hat32) : reinterpret_cast<ST*>(p.hat);
     const size_t rowstride = (size_t)p.Hp * 2;
 #pragma unroll 8
     for (int t = n - 1; t >= 0; --t) {
         x = tl.v[t * 32 + lane] - tl.cp[t * 16 + (lane >> 1)] * x;
-        if (valid) hatw[(size_t)(r0 + t + 1) * rowstride + col] = x;
+        if (valid) hatw[(size_t)(r0 + t + 1) * rowstride + col] = (ST)x;
     }
     // wall rows of psi-hat: Nx psi_bot / Nx psi_top at kx = 0, else 0 (poisson.cu:130-132)
     if (valid) {
-        if (s == 0) hatw[col] = kx0re ? (double)p.Nx * p.psi_bot : 0.0;
-        if (s == p.nseg - 1) hatw[(size_t)(p.Ny - 1) * rowstride + col] = kx0re ? (double)p.Nx * p.psi_top : 0.0;
+        if (s == 0) hatw[col] = (ST)(kx0re ? (double)p.Nx * p.psi_bot : 0.0);
+        if (s == p.nseg - 1) hatw[(size_t)(p.Ny - 1) * rowstride + col] = (ST)(kx0re ? (double)p.Nx * p.psi_top : 0.0);
     }
 }
 
@@ -1594,8 +1625,12 @@ struct ThomasMaps {
 
 // bytes of one buffer (omega-hat tile [R][8] complex + cp tile [R][8]) and of the whole
 // dynamic shared memory (two buffers, the rows' asub and 1/csup, alignment slack)
-__host__ __device__ constexpr size_t tc_buf_bytes(int R) { return (size_t)R * (16 + 8) * TC_KX; }
-__host__ __device__ constexpr size_t tc_smem_bytes(int R) { return 2 * tc_buf_bytes(R) + (size_t)R * 16 + 128; }
+// (F32: the omega-hat tile in FP32, 8 bytes per complex value)
+__host__ __device__ constexpr size_t tc_hat_bytes(bool f32) { return f32 ? 8 : 16; }
+__host__ __device__ constexpr size_t tc_buf_bytes(int R, bool f32 = false) { return (size_t)R * (tc_hat_bytes(f32) + 8) * TC_KX; }
+__host__ __device__ constexpr size_t tc_smem_bytes(int R, bool f32 = false) {
+    return 2 * tc_buf_bytes(R, f32) + (size_t)R * 16 + 128;
+}
 
 __device__ __forceinline__ void cluster_arrive_release() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
@@ -1646,7 +1681,7 @@ __device__ __forceinline__ AffMap aff_shfl_down(const AffMap& m, int off) {
                   __shfl_down_sync(0xffffffffu, m.P, off)};
 }
 
-template <int L>
+template <int L, bool F32>
 static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_cluster(const __grid_constant__ ThomasMaps maps, ThomasParams p) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
@@ -1663,7 +1698,8 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     constexpr int RB = R < TC_BOX ? R : TC_BOX;
     constexpr int NBOX = R / RB;
     unsigned char* sm = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
-    double2* rows = reinterpret_cast<double2*>(sm + 2 * tc_buf_bytes(R));   // [R] {asub, 1/csup}
+    constexpr size_t HB = tc_hat_bytes(F32), BUF = tc_buf_bytes(R, F32);
+    double2* rows = reinterpret_cast<double2*>(sm + 2 * BUF);   // [R] {asub, 1/csup}
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const int cid = blockIdx.x / C, ncl = gridDim.x / C;
     const int ngroups = p.Hp / TC_KX;
@@ -1673,12 +1709,12 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
     const int lo = q * L;
     const size_t Hp = (size_t)p.Hp;
     auto issue = [&](int grp, int b) {
-        unsigned char* dst = sm + (size_t)b * tc_buf_bytes(R);
-        mbar_expect_tx(&bars[b], (unsigned)tc_buf_bytes(R));
+        unsigned char* dst = sm + (size_t)b * BUF;
+        mbar_expect_tx(&bars[b], (unsigned)BUF);
 #pragma unroll
         for (int bx = 0; bx < NBOX; ++bx) {
-            tma_load_2d(dst + (size_t)bx * RB * 16 * TC_KX, &maps.hat, grp * 2 * TC_KX, r0 + 1 + bx * RB, &bars[b]);
-            tma_load_2d(dst + (size_t)R * 16 * TC_KX + (size_t)bx * RB * 8 * TC_KX, &maps.cp, grp * TC_KX, r0 + bx * RB, &bars[b]);
+            tma_load_2d(dst + (size_t)bx * RB * HB * TC_KX, &maps.hat, grp * 2 * TC_KX, r0 + 1 + bx * RB, &bars[b]);
+            tma_load_2d(dst + (size_t)R * HB * TC_KX + (size_t)bx * RB * 8 * TC_KX, &maps.cp, grp * TC_KX, r0 + bx * RB, &bars[b]);
         }
     };
     if (tid == 0) {
@@ -1710,13 +1746,13 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         if (!ok && tid == 0 && pending[b] < 0) pending[b] = (int)ph;
         const int kx = g * TC_KX + k;
         const bool valid = kx < p.H;
-        const double2* vt = reinterpret_cast<const double2*>(sm + (size_t)b * tc_buf_bytes(R));
-        const double* ct = reinterpret_cast<const double*>(sm + (size_t)b * tc_buf_bytes(R) + (size_t)R * 16 * TC_KX);
+        const auto* vt = reinterpret_cast<const typename SpecT<F32>::T2*>(sm + (size_t)b * BUF);
+        const double* ct = reinterpret_cast<const double*>(sm + (size_t)b * BUF + (size_t)R * HB * TC_KX);
         double2 x[L];
         double cpv[L];
 #pragma unroll
         for (int i = 0; i < L; ++i) {
-            x[i] = vt[(lo + i) * TC_KX + k];
+            x[i] = spec_wide(vt[(lo + i) * TC_KX + k]);
             cpv[i] = ct[(lo + i) * TC_KX + k];
         }
         fence_proxy_async_smem();                        // reads of buffer b before its next TMA write
@@ -1862,20 +1898,21 @@ static __global__ void __launch_bounds__(TC_THREADS, (L <= 8 ? 2 : 1)) k_thomas_
         const double2 Xb = cbuf[k];
         const double2 X = make_double2(fma(E2.P, Xb.x, E2.D.x), fma(E2.P, Xb.y, E2.D.y));
         // 3. carry term; psi-hat out
-        double2* hatw = reinterpret_cast<double2*>(p.hat);
+        using ST2 = typename SpecT<F32>::T2;
+        ST2* hatw = F32 ? reinterpret_cast<ST2*>(p.hat32) : reinterpret_cast<ST2*>(p.hat);
         double Qc = 1.0;
 #pragma unroll
         for (int i = L - 1; i >= 0; --i) {
             const int t = lo + i;
             if (t < n) {
                 Qc = -cpv[i] * Qc;
-                if (valid) hatw[(size_t)(r0 + t + 1) * Hp + kx] = make_double2(fma(Qc, X.x, x[i].x), fma(Qc, X.y, x[i].y));
+                if (valid) hatw[(size_t)(r0 + t + 1) * Hp + kx] = spec_narrow<F32>(fma(Qc, X.x, x[i].x), fma(Qc, X.y, x[i].y));
             }
         }
         // wall rows of psi-hat: Nx psi_bot / Nx psi_top at kx = 0, else 0 (poisson.cu:130-132)
         if (valid && q == 0) {
-            if (rank == 0) hatw[kx] = make_double2(kx == 0 ? (double)p.Nx * p.psi_bot : 0.0, 0.0);
-            if (rank == C - 1) hatw[(size_t)(p.Ny - 1) * Hp + kx] = make_double2(kx == 0 ? (double)p.Nx * p.psi_top : 0.0, 0.0);
+            if (rank == 0) hatw[kx] = spec_narrow<F32>(kx == 0 ? (double)p.Nx * p.psi_bot : 0.0, 0.0);
+            if (rank == C - 1) hatw[(size_t)(p.Ny - 1) * Hp + kx] = spec_narrow<F32>(kx == 0 ? (double)p.Nx * p.psi_top : 0.0, 0.0);
         }
     }
     if (tid == 0) {                                      // copies still in flight after a timeout
