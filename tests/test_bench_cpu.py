@@ -36,8 +36,11 @@ def test_kernel_byte_models():
         assert b.kernel_bytes(name, 1, Nx, Ny) == 12 * N
         assert b.kernel_bytes(name, 3, Nx, Ny) == 16 * N
     assert b.kernel_bytes("k_fft_fwd", 1, Nx, Ny) == 8 * Nx * Ni + 16 * H * Ni
-    assert b.kernel_bytes("k_fft_fwd32", 1, Nx, Ny) == 4 * Nx * Ni + 16 * H * Ni
+    # the FP32-bulk step's spectra are FP32 (8 bytes per complex value), its cp table FP64
+    assert b.kernel_bytes("k_fft_fwd32", 1, Nx, Ny, 32) == 4 * Nx * Ni + 8 * H * Ni
+    assert b.kernel_bytes("k_ifft_thom32", 1, Nx, Ny, 32) == 8 * H * Ni + 4 * N + 24 * Nx
     assert b.kernel_bytes("k_thomas_cluster", 1, Nx, Ny) == 16 * H * Ni + 8 * H * Ni + 16 * H * Ny
+    assert b.kernel_bytes("k_thomas_cluster", 1, Nx, Ny, 32) == 8 * H * Ni + 8 * H * Ni + 8 * H * Ny
     assert b.kernel_bytes("k_ifft_thom", 1, Nx, Ny) == 16 * H * Ni + 8 * N + 48 * Nx
     assert b.kernel_bytes("k_maxuv_dt", 0, Nx, Ny) == 8 * N
     assert b.kernel_bytes("k_maxuv32", 0, Nx, Ny) == 4 * N

@@ -1,12 +1,18 @@
-"""The FP32-bulk variant (precision 32) against the FP64 path, on a B200.
+"""The FP32-bulk variant (precision 32) against the FP64 path and the oracle, on a B200.
 
 The variant steps FP32 fluctuations about fixed FP64 base profiles (the x-means of the initial
-state) with the spectral buffer and the tridiagonal solve in FP64. Its error is FP32 rounding of
-the fluctuations, so the bars here are FP32-level:
+state) with an FP32 spectral buffer and the tridiagonal solve's arithmetic and table in FP64. Its
+error is FP32 rounding of the fluctuations, so the bars here are FP32-level:
   - split and export of the initial state: 1e-6 of max |omega| / max |psi|;
   - one step: 2e-5 of max |omega| and 1e-5 of max |psi|;
   - 200 steps of a forced turbulent-ish channel: 1e-3 of max |omega|, and the diagnostics K,
-    Omega, u_tau, Re_tau, C_f and the wall enstrophy flux BOmega_wall within 1e-3 relative.
+    Omega, u_tau, Re_tau, C_f and the wall enstrophy flux BOmega_wall within 1e-3 relative;
+  - against the oracle (the CPU restatement of the reference's FP64 algorithm) at a fixed dt, at
+    256x129 (200 steps) and 4096x2049 (20 steps): omega within 1e-4 of its max away from the walls
+    (the two rows next to each wall within 1e-3: they carry the Thom gain), psi within 1e-6,
+    K and Omega within 1e-6 relative, u_tau, Re_tau and C_f within 1e-5, BOmega_wall within 1e-3;
+    the FP64 path within 1e-9, and 1e-7 for the quantities taken at the walls (the wall vorticity
+    and shear carry the Thom gain on the round-off of psi next to the walls).
 """
 import numpy as np
 import pytest
@@ -85,3 +91,52 @@ def test_run_loop_and_ensemble(nse, cuda):
     e.step(25)
     assert np.array_equal(c.fields()[0], b.fields()[0])
     e.close()
+
+
+SIX = ("K", "Omega", "utau_avg", "Re_tau", "Cf", "BOmega_wall")
+
+
+@pytest.mark.parametrize("Nx,Ny,steps", [(256, 129, 200), (4096, 2049, 20)])
+def test_against_oracle(nse, oracle, cuda, Nx, Ny, steps):
+    import os
+    oracle.lib().or_set_threads(os.cpu_count() or 1)
+    cfg = dict(CFG, Nx=Nx, Ny=Ny, adapt=0)
+    o = oracle.OracleSolver(**cfg)
+    y = o.metric(0)
+    w0 = omega0(Nx, Ny, y)
+    o.set_omega(w0)
+    dt = 0.9 * o.adapt_dt()[0]                     # a fixed step below the CFL and viscous limits
+    cfg["dt_init"] = dt
+    t = 0.0
+    for _ in range(steps):
+        o.step(t, dt)
+        t += dt
+    wo, po = o.fields()
+    do = dict(zip(nse.DIAG_COLUMNS, o.diag_row(t, t0_row=True)))
+    o.close()
+    # the wall enstrophy flux takes the wall vorticity, which carries the Thom closure's gain on the
+    # round-off of psi next to the walls (1e-7 in FP64)
+    # (as do u_tau, Re_tau and C_f, through the wall shear)
+    bars = {64: dict(omega=1e-9, psi=1e-9, bulk=1e-9, wall=1e-7, bw=1e-7),
+            32: dict(omega=1e-4, psi=1e-6, bulk=1e-6, wall=1e-5, bw=1e-3)}
+    for P in (64, 32):
+        g = nse.Solver(precision=P, **cfg)
+        g.set_omega(w0)
+        g.step(steps, use_graph=True)
+        assert g.time()[1] == dt
+        wg, pg = g.fields()
+        dg = g.diagnostics(t0_row=True)
+        g.close()
+        b = bars[P]
+        # omega away from the walls; the wall rows and their neighbours carry the Thom gain
+        # (2/dy_1^2 = 1e8 on the 4096x2049 grid) on the round-off of psi next to the walls
+        scale = np.max(np.abs(wo))
+        e_int = np.max(np.abs(wg[2:-2] - wo[2:-2])) / scale
+        e_wall = np.max(np.abs(wg[[0, 1, -2, -1]] - wo[[0, 1, -2, -1]])) / scale
+        assert e_int < b["omega"], (P, e_int)
+        assert e_wall < max(b["omega"], b["bw"]), (P, e_wall)
+        assert rel(pg, po) < b["psi"], (P, rel(pg, po))
+        for k in SIX:
+            e = abs(dg[k] - do[k]) / abs(do[k])
+            bar = b["bw"] if k == "BOmega_wall" else (b["bulk"] if k in ("K", "Omega") else b["wall"])
+            assert e < bar, (P, k, e, dg[k], do[k])
