@@ -655,7 +655,8 @@ def run_ensemble(args):
     return {"metric": f"ensemble grid-point updates/s (64 channels, configuration 3, {prec})",
             "value": round(pts * K / (ens_ms * 1e-3), 1), "unit": "points/s", "n_gpus": 1, "steps": K,
             "warmup": args.warmup, "ms_per_step": round(ens_ms / K, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == 64 else "f32 bulk (FP64 base profiles and spectra)",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == 64 else "f32 bulk (FP64 base profiles, FP64 tridiagonal arithmetic and table)",
             "data": "synthetic (seeded laminar + random modes per member)", "plans": plans,
             "config": {"workload": "64 channels, (Nx,Ny) on {256,512,1024}x{129,257,513}, Re_b log-uniform "
                                    "[2e3,2e4], nforce {4,8,12}, tanh beta=2, adaptive dt", "members": len(spec),
