@@ -90,8 +90,9 @@ typedef struct nse2d_config {
     int    mms_kx;
     int    closure_diag;      /* accumulate the wall-update enstrophy (Jwall columns) */
     int    precision;         /* 64 (FP64 throughout) or 32 (FP32 bulk with FP64 islands: the
-                                 x-mean base profiles, the spectral buffer and the tridiagonal
-                                 solve; no MMS forcing, no closure diagnostics). With 32, the
+                                 x-mean base profiles and the tridiagonal solve's arithmetic and
+                                 table, over an FP32 spectral buffer; no MMS forcing, no closure
+                                 diagnostics). With 32, the
                                  FP64 fields behind nse2d_field_ptr are refreshed only by the
                                  calls that read them (fields, diagnostics, uv, statistics). */
     const double* y_table;    /* stretch 2: the Ny node coordinates y_0 < ... < y_{Ny-1} (host
