@@ -169,7 +169,8 @@ struct Context {
     CUtensorMap tm32_psi{}, tm32_w[3]{}, tm32_wn{};
     // row transforms at Nx = 4096: the forms whose rows are prefetched by bulk copies
     bool rowfft_pf = false, rowfft_pf_ok = false;
-    bool max_fused = true;           // with rowfft_pf, adaptive FP64: max reduction in the stage-3 inverse transform
+    bool max_fused = false;          // with rowfft_pf, adaptive FP64: max reduction in the stage-3 inverse transform
+                                     // (off by default: measured slower than the separate reduction at 4096x2049)
     bool pdl = false;                // FP64 step kernels launched with programmatic dependent launch
     unsigned int* bcount = nullptr;  // [grid + 1] band-boundary counters of the fused max reduction
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)

@@ -433,11 +433,9 @@ class Solver:
         return pl.as_dict()
 
     def set_plan(self, stage_tma=None, tridiag_clusters=None, rowfft_prefetch=None, max_fused=None, pdl=None):
-        """Select kernel forms (None keeps the current one; max_fused None asks for the fused max
-        reduction wherever it applies); forms the grid cannot use fall back."""
+        """Select kernel forms (None keeps the current one, as nse2d_get_plan reports it); forms the
+        grid cannot use fall back."""
         cur = self.plan()
-        if max_fused is None:
-            max_fused = 1
         pl = Plan(**{k: int(v if v is not None else cur[k]) for k, v in
                      (("stage_tma", stage_tma), ("tridiag_clusters", tridiag_clusters),
                       ("rowfft_prefetch", rowfft_prefetch), ("max_fused", max_fused), ("pdl", pdl))})

@@ -121,15 +121,16 @@ def test_switching_row_transform_form_mid_run(nse, cuda):
     y = np.tanh(2.0 * np.linspace(-1, 1, 2049)) / np.tanh(2.0)
     w0 = laminar_perturbed(4096, 2049, y, seed=8, amp=5e-2)
     a = nse.Solver(**cfg)
-    a.set_plan(rowfft_prefetch=1)
+    a.set_plan(rowfft_prefetch=1, max_fused=1)
+    assert a.plan()["max_fused"] == 1
     a.set_omega(w0)
     b = nse.Solver(**cfg)
-    b.set_plan(rowfft_prefetch=1)
+    b.set_plan(rowfft_prefetch=1, max_fused=1)
     b.set_omega(w0)
     seq_a, seq_b = [], []
     for k, pf in enumerate((1, 0, 1, 1, 0)):
         a.step(1, use_graph=True)
-        b.set_plan(rowfft_prefetch=pf)
+        b.set_plan(rowfft_prefetch=pf, max_fused=1)
         b.step(1, use_graph=True)
         seq_a.append(a.time())
         seq_b.append(b.time())
