@@ -108,11 +108,11 @@ __device__ __forceinline__ double point_rhs(const StageParams& p, int j, int i, 
 __device__ __forceinline__ double nn_max(double a, double b) { return b > a ? b : a; }
 
 // Programmatic dependent launch: a step kernel launched with the programmatic-serialisation
-// attribute may become resident while the kernel before it in the stream is still running.
-// Every step kernel begins with pdl_begin: it waits until the grids it depends on have completed
-// and their writes are visible (a no-op for a kernel launched without the attribute), then lets
-// the next kernel be scheduled, whose CTAs take the SM resources this grid's CTAs free and wait
-// in the same way. Nothing is read or written before the wait.
+// attribute may be launched while the kernel before it in the stream is still finishing (its
+// CTAs trigger the next launch as they exit). Every step kernel begins with pdl_begin: it waits
+// until the grids it depends on have completed and their writes are visible (a no-op for a kernel
+// launched without the attribute). Nothing is read or written before the wait. An explicit trigger
+// right after the wait, which lets the next kernel's CTAs become resident early, measured slower.
 __device__ __forceinline__ void pdl_begin() {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
