@@ -757,8 +757,10 @@ def main():
     ap.add_argument("--workload", choices=["channel", "ensemble", "closure"], default="channel",
                     help="ensemble: the 64-channel batched ensemble; closure: the learned-closure workflow "
                          "(each its own JSON line, 1 GPU)")
-    ap.add_argument("--closure-span", type=float, default=50.0, help="closure: convective units of data and of the test runs")
-    ap.add_argument("--closure-val-span", type=float, default=20.0)
+    ap.add_argument("--closure-span", type=float, default=200.0,
+                    help="closure: convective units of data and of the test runs (200: the specified configuration, "
+                         "about 15 minutes on one B200)")
+    ap.add_argument("--closure-val-span", type=float, default=50.0)
     ap.add_argument("--closure-spinup", type=float, default=20.0)
     ap.add_argument("--closure-train-steps", type=int, default=2000)
     args = ap.parse_args()
