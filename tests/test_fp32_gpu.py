@@ -140,3 +140,24 @@ def test_against_oracle(nse, oracle, cuda, Nx, Ny, steps):
             e = abs(dg[k] - do[k]) / abs(do[k])
             bar = b["bw"] if k == "BOmega_wall" else (b["bulk"] if k in ("K", "Omega") else b["wall"])
             assert e < bar, (P, k, e, dg[k], do[k])
+
+
+def test_fp32_plan_forms_agree(nse, cuda):
+    """The FP32-bulk step's kernel forms (TMA stage kernel or a CTA per tile, cluster or two-pass
+    tridiagonal solve over the FP32 spectra) agree to FP32 round-off after 20 steps at 512x257."""
+    cfg = dict(CFG, Nx=512, Ny=257)
+    out = {}
+    for st in (1, 0):
+        for cl in (1, 0):
+            g = nse.Solver(precision=32, **cfg)
+            g.set_plan(stage_tma=st, tridiag_clusters=cl)
+            p = g.plan()
+            assert (p["stage_tma"], p["tridiag_clusters"]) == (st, cl)
+            g.set_omega(omega0(g.Nx, g.Ny, g.metric(0)))
+            g.step(20, use_graph=True)
+            out[(st, cl)] = g.fields()
+            g.close()
+    wr, pr = out[(1, 1)]
+    for key, (w, psi) in out.items():
+        assert rel(w, wr) < 1e-5, (key, rel(w, wr))
+        assert rel(psi, pr) < 1e-6, (key, rel(psi, pr))
