@@ -138,7 +138,7 @@ int  nse2d_set_tridiag_form(nse2d_ctx* ctx, int clusters);
  * precision 64 only) or read by plain loads (0); max_fused, with the prefetching transforms in an
  * adaptive FP64 step, the max reduction of psi inside the stage-3 inverse transform and dt
  * computed by the next step's stage kernel (1) or a separate max reduction at the start of the
- * step (0, the default: the faster at 4096x2049); pdl, the FP64 step kernels launched with
+ * step (0, the default: the faster at 4096x2049); pdl, the step kernels launched with
  * programmatic dependent launch (1: a kernel's launch is processed while the one before it
  * finishes, and its CTAs wait on the device for that one's completion before they read or write
  * anything) or in plain stream order (0, the default). Every form gives

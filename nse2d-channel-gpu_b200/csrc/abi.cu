@@ -310,7 +310,7 @@ int nse2d_autotune_plan(nse2d_ctx* ctx, int trial_steps, nse2d_plan* best, doubl
         for (int cl = c->thomas_cluster_ok ? 1 : 0; rc == 0 && cl >= 0; --cl)
             for (int pf = c->rowfft_pf_ok ? 1 : 0; rc == 0 && pf >= 0; --pf)
                 for (int mf = (pf && mf_ok) ? 1 : 0; rc == 0 && mf >= 0; --mf)
-                for (int pd = c->prec32 ? 0 : 1; rc == 0 && pd >= 0; --pd) {
+                for (int pd = 1; rc == 0 && pd >= 0; --pd) {
                     if ((rc = set_plan(c, PlanForms{st != 0, cl != 0, pf != 0, mf != 0, pd != 0}))) break;
                     if ((rc = run_steps(c, 1, true, s, false))) break;           // capture and warm
                     cudaEventRecord(a, s);

@@ -173,6 +173,7 @@ __device__ __forceinline__ float stage32_rhs_interior(float rhs, float wc, float
 }
 
 static __global__ void __launch_bounds__(256) k_stage32(Stage32Params p) {
+    pdl_begin();
     __shared__ float sp[ST_H][ST_W + 1];
     __shared__ float so[ST_H][ST_W + 1];
     const int Nx = p.Nx, Ny = p.Ny;
@@ -349,6 +350,7 @@ __device__ __forceinline__ void stage32_tile4(const Stage32Params& p, float dt, 
 
 static __global__ void __launch_bounds__(256, 2) k_stage32_tma(const __grid_constant__ Stage32Maps maps, Stage32Params p) {
     extern __shared__ __align__(16) unsigned char smem_dyn[];
+    pdl_begin();
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ float srow[2][RC32_N][S32_TY];          // per buffer: the row constants of its tile
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -431,6 +433,7 @@ __host__ __device__ constexpr size_t fft32_smem_bytes(int M) { return (size_t)ip
 template <int M>
 static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     cpx<float>* buf = reinterpret_cast<cpx<float>*>(smem_raw);
     constexpr int R0 = p16_plan<M>::R(0), NB0 = M / R0;
     const int je = p.Ny - 1;                            // interior rows 1 .. Ny-2, strided over one wave of CTAs
@@ -489,6 +492,7 @@ static __global__ void __launch_bounds__(IP_NT) k_fft_fwd32(Fft32Params p) {
 template <int M>
 static __global__ void __launch_bounds__(IP_NT, 5) k_ifft_thom32(Fft32Params p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_begin();
     cpx<float>* buf = reinterpret_cast<cpx<float>*>(smem_raw);
     const int Nx = p.Nx, Ny = p.Ny;
     int j0, j1;
@@ -634,6 +638,7 @@ struct Max32Params {
 constexpr int MX32_WCOLS = 120, MX32_COLS = 8 * MX32_WCOLS;
 
 static __global__ void __launch_bounds__(256, 3) k_maxuv32(Max32Params q) {
+    pdl_begin();
     const MaxParams& p = q.base;
     const int Nx = p.Nx, Ny = p.Ny;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

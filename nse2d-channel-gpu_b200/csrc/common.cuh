@@ -171,7 +171,7 @@ struct Context {
     bool rowfft_pf = false, rowfft_pf_ok = false;
     bool max_fused = false;          // with rowfft_pf, adaptive FP64: max reduction in the stage-3 inverse transform
                                      // (off by default: measured slower than the separate reduction at 4096x2049)
-    bool pdl = false;                // FP64 step kernels launched with programmatic dependent launch
+    bool pdl = false;                // step kernels launched with programmatic dependent launch
     unsigned int* bcount = nullptr;  // [grid + 1] band-boundary counters of the fused max reduction
     // stage kernel: TMA tensor maps of psi and of the three omega buffers (Nx >= 128)
     bool stage_tma = false, stage_tma_ok = false;

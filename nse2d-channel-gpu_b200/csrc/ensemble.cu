@@ -200,7 +200,7 @@ int nse2d_ensemble_autotune_plans(nse2d_ensemble* en, int trial_steps, int* grou
     for (size_t k = 0; rc == 0 && k < cls.size(); ++k) {
         Context* c0 = cls[k].m[0];
         const bool ok[5] = {c0->prec32 ? c0->stage32_tma_ok : c0->stage_tma_ok, c0->thomas_cluster_ok, c0->rowfft_pf_ok,
-                            c0->rowfft_pf_ok && c0->cfg.adapt && !c0->prec32, !c0->prec32};
+                            c0->rowfft_pf_ok && c0->cfg.adapt && !c0->prec32, true};
         for (int f = 0; rc == 0 && f < 5; ++f) {
             if (!ok[f]) continue;
             bool v[5];

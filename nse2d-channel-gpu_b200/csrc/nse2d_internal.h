@@ -1,8 +1,30 @@
 // Internal interface between the C-ABI layer and the solver implementation.
 #pragma once
+#include <utility>
+
 #include "common.cuh"
 
 namespace nse2d {
+// A step kernel (each begins with pdl_begin), with the programmatic-serialisation attribute when
+// the plan asks for it; extra: another launch attribute (the cluster shape), or nullptr.
+template <typename... KArgs, typename... Args>
+inline int launch_step_kernel(const Context* c, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, const cudaLaunchAttribute* extra, Args&&... args) {
+    cudaLaunchConfig_t lc{};
+    cudaLaunchAttribute at[2];
+    unsigned na = 0;
+    if (extra) at[na++] = *extra;
+    if (c->pdl) {
+        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    lc.gridDim = grid; lc.blockDim = block; lc.dynamicSmemBytes = smem; lc.stream = s;
+    lc.attrs = at; lc.numAttrs = na;
+    NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, std::forward<Args>(args)...));
+    return 0;
+}
+
 int build_y_metrics(const Config& c, std::vector<double>& y, std::vector<double>& a_node,
                     std::vector<double>& a_edge, std::vector<double>& dy_edge, std::vector<double>& w_node);
 int context_create(const Config& cfg, Context** out);

@@ -525,26 +525,6 @@ void context_destroy(Context* c) {
 static bool fused_max(const Context* c) { return c->cfg.adapt && !c->prec32 && c->rowfft_pf && c->max_fused; }
 
 // ---- launchers ----
-// A step kernel (each begins with pdl_begin), with the programmatic-serialisation attribute when
-// the plan asks for it; extra: another launch attribute (the cluster shape), or nullptr.
-template <typename... KArgs, typename... Args>
-static int launch_step_kernel(const Context* c, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
-                              cudaStream_t s, const cudaLaunchAttribute* extra, Args&&... args) {
-    cudaLaunchConfig_t lc{};
-    cudaLaunchAttribute at[2];
-    unsigned na = 0;
-    if (extra) at[na++] = *extra;
-    if (c->pdl) {
-        at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[na].val.programmaticStreamSerializationAllowed = 1;
-        ++na;
-    }
-    lc.gridDim = grid; lc.blockDim = block; lc.dynamicSmemBytes = smem; lc.stream = s;
-    lc.attrs = at; lc.numAttrs = na;
-    NSE_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, std::forward<Args>(args)...));
-    return 0;
-}
-
 static StageParams stage_params(Context* c) {
     StageParams p{};
     p.psi = c->psi; p.rt = c->rt; p.ctl = c->ctl;
@@ -731,7 +711,7 @@ int set_plan(Context* c, const PlanForms& f) {
     const bool cur = c->prec32 ? c->stage32_tma : c->stage_tma;
     const bool fused_before = fused_max(c);
     const bool fused_after = c->cfg.adapt && !c->prec32 && pf && f.max_fused;
-    const bool pdl = f.pdl && !c->prec32;
+    const bool pdl = f.pdl;
     if (st != cur || pf != c->rowfft_pf || fused_before != fused_after || pdl != c->pdl) {
         NSE_CUDA_TRY(cudaDeviceSynchronize());
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

@@ -128,17 +128,13 @@ template <int M> static int fft32_fwd_t(Context* c, Fft32Params& p, cudaStream_t
     int per_sm = 0;                                      // one wave of CTAs over the interior rows
     NSE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_fwd32<M>, IP_NT, sm));
     const int grid = std::max(1, std::min(c->Ni, std::max(per_sm, 1) * c->num_sms));
-    k_fft_fwd32<M><<<grid, IP_NT, sm, s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_fft_fwd32<M>, dim3(grid), dim3(IP_NT), sm, s, nullptr, p);
 }
 template <int M> static int fft32_inv_t(Context* c, Fft32Params& p, cudaStream_t s) {
     const size_t sm = fft32_smem_bytes(M);
     NSE_CUDA_TRY(cudaFuncSetAttribute(k_ifft_thom32<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     p.rows_per_cta = 3;
-    k_ifft_thom32<M><<<std::max(1, c->Ny / 3), IP_NT, sm, s>>>(p);
-    NSE_CUDA_TRY(cudaGetLastError());
-    return 0;
+    return launch_step_kernel(c, k_ifft_thom32<M>, dim3(std::max(1, c->Ny / 3)), dim3(IP_NT), sm, s, nullptr, p);
 }
 
 #define NSE_FFT32_DISPATCH(FN)                                                     \
@@ -187,9 +183,7 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
         q.dpsibar = c->rc32 + (size_t)RC_DPB * c->Ny;
         int grid = 1;
         maxuv_plan(p, c->maxuv32_ctas, c->maxuv32_ctas, grid, MX32_COLS);
-        k_maxuv32<<<grid, 256, 0, s>>>(q);
-        NSE_CUDA_TRY(cudaGetLastError());
-        if (mark()) return -1;
+        if (launch_step_kernel(c, k_maxuv32, dim3(grid), dim3(256), 0, s, nullptr, q) || mark()) return -1;
     }
     float* wst[3] = {c->w1f, c->w2f, c->wf};
     const float* win[3] = {c->wf, c->w1f, c->w2f};
@@ -205,11 +199,12 @@ int step32_impl(Context* c, cudaStream_t s, bool store_rhs, cudaEvent_t* ev) {
             maps.psi = c->tm32_psi;
             maps.w = c->tm32_w[st - 1];          // w'^(s): wf, w1f, w2f in stages 1, 2, 3
             maps.wn = c->tm32_wn;
-            k_stage32_tma<<<c->stage32_tma_grid, 256, stage32_tma_smem_bytes(), s>>>(maps, sp);
+            if (launch_step_kernel(c, k_stage32_tma, dim3(c->stage32_tma_grid), dim3(256), stage32_tma_smem_bytes(), s,
+                                   nullptr, maps, sp))
+                return -1;
         } else {
-            k_stage32<<<grid, 256, 0, s>>>(sp);
+            if (launch_step_kernel(c, k_stage32, grid, dim3(256), 0, s, nullptr, sp)) return -1;
         }
-        NSE_CUDA_TRY(cudaGetLastError());
         if (mark()) return -1;
         if (fft32_fwd(c, wst[st - 1], s) || mark()) return -1;
         for (int i = 0; i < thomas_launches(c); ++i)

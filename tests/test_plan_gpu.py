@@ -158,8 +158,8 @@ def test_fused_max_same_bits_at_4096(nse, cuda):
     assert np.array_equal(wa, wb) and np.array_equal(pa, pb)
 
 
-@pytest.mark.parametrize("Nx,Ny", [(256, 129), (4096, 2049)])
-def test_programmatic_launch_same_bits(nse, cuda, Nx, Ny):
+@pytest.mark.parametrize("Nx,Ny,precision", [(256, 129, 64), (4096, 2049, 64), (256, 129, 32), (4096, 2049, 32)])
+def test_programmatic_launch_same_bits(nse, cuda, Nx, Ny, precision):
     """With programmatic dependent launch every step kernel waits on the device for the kernel
     before it to complete before it reads or writes anything: the same steps to the bit, through
     plain launches, the one-step graph and the run graph (a WHILE node)."""
@@ -168,7 +168,7 @@ def test_programmatic_launch_same_bits(nse, cuda, Nx, Ny):
     w0 = laminar_perturbed(Nx, Ny, y, seed=9, amp=5e-2)
     out = {}
     for pdl in (1, 0):
-        g = nse.Solver(**cfg)
+        g = nse.Solver(precision=precision, **cfg)
         g.set_plan(pdl=pdl)
         assert g.plan()["pdl"] == pdl
         g.set_omega(w0)
