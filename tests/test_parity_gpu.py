@@ -13,7 +13,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GRIDS = [(8, 5, 0, 0.0), (16, 9, 1, 2.0), (64, 33, 0, 0.0), (64, 65, 1, 2.0), (128, 129, 1, 2.0),
-         (256, 257, 1, 2.0), (512, 257, 1, 2.0)]
+         (256, 257, 1, 2.0), (512, 257, 1, 2.0),
+         # the longest rows the row transforms take (M = 4096 and 8192), with few rows
+         (8192, 65, 1, 2.0), (16384, 33, 0, 0.0)]
 
 
 def laminar_perturbed(Nx, Ny, y, seed=0, amp=1e-3, Ub=1.0, h=1.0):
@@ -248,3 +250,27 @@ def test_diagnostics_rows(nse, oracle, cuda, case):
     for n in range(10):
         o.step(n * dt, dt)
     check(g.diagnostics(t0_row=False), o.diag_row(10 * dt, t0_row=False))
+
+
+@pytest.mark.parametrize("Nx,Ny", [(8192, 65), (16384, 33)])
+def test_steps_long_rows(nse, oracle, cuda, Nx, Ny):
+    """Three adaptive steps on the longest rows the row transforms take, against the oracle:
+    dt and the maxima of every step to 1e-12, the fields to 1e-10."""
+    cfg = dict(Nx=Nx, Ny=Ny, Lx=4 * np.pi, stretch=1, beta=2.0, Ub=1.0, Reb=2000.0, F0=0.05, nforce=8,
+               lin_drag=1e-3, adapt=1, cfl=0.5)
+    g, o = _pair(nse, oracle, **cfg)
+    w0 = laminar_perturbed(Nx, Ny, o.metric(0), seed=7, amp=1e-2)
+    g.set_omega(w0)
+    o.set_omega(w0)
+    t = 0.0
+    for _ in range(3):
+        dto, mo = o.adapt_dt()
+        o.step(t, dto)
+        t += dto
+        g.step(1)
+        tg, dtg, st, mg = g.time()
+        assert abs(dtg - dto) <= 1e-12 * dto, (dtg, dto)
+        assert np.allclose(mg, mo, rtol=1e-12, atol=0)
+    wg, pg = g.fields()
+    wo, po = o.fields()
+    assert_fields_close(wg, pg, wo, po, o.metric(3), 1e-10)
