@@ -15,7 +15,9 @@ pytestmark = pytest.mark.gpu
 GRIDS = [(8, 5, 0, 0.0), (16, 9, 1, 2.0), (64, 33, 0, 0.0), (64, 65, 1, 2.0), (128, 129, 1, 2.0),
          (256, 257, 1, 2.0), (512, 257, 1, 2.0),
          # the longest rows the row transforms take (M = 4096 and 8192), with few rows
-         (8192, 65, 1, 2.0), (16384, 33, 0, 0.0)]
+         (8192, 65, 1, 2.0), (16384, 33, 0, 0.0),
+         # row counts that are not 2^k + 1 (partial stage tiles, uneven Thomas segments and bands)
+         (128, 50, 1, 2.0), (256, 301, 1, 1.5), (1024, 777, 0, 0.0)]
 
 
 def laminar_perturbed(Nx, Ny, y, seed=0, amp=1e-3, Ub=1.0, h=1.0):
@@ -274,3 +276,31 @@ def test_steps_long_rows(nse, oracle, cuda, Nx, Ny):
     wg, pg = g.fields()
     wo, po = o.fields()
     assert_fields_close(wg, pg, wo, po, o.metric(3), 1e-10)
+
+
+@pytest.mark.parametrize("Nx,Ny,precision", [(128, 50, 64), (256, 301, 64), (1024, 777, 64), (256, 301, 32)])
+def test_steps_uneven_rows(nse, oracle, cuda, Nx, Ny, precision):
+    """Five adaptive steps on row counts that are not 2^k + 1, against the oracle: dt to 1e-12 and
+    the fields to 1e-10 in FP64 (FP32 bulk: dt to 1e-6, omega to 1e-5 of its max, psi to 1e-6)."""
+    cfg = dict(Nx=Nx, Ny=Ny, Lx=2 * np.pi, stretch=1, beta=2.0, Ub=1.0, Reb=2000.0, F0=0.05, nforce=4,
+               lin_drag=1e-3, adapt=1, cfl=0.5)
+    g = nse.Solver(precision=precision, **cfg)
+    o = oracle.OracleSolver(**cfg)
+    w0 = laminar_perturbed(Nx, Ny, o.metric(0), seed=11, amp=1e-2)
+    g.set_omega(w0)
+    o.set_omega(w0)
+    t = 0.0
+    for _ in range(5):
+        dto, mo = o.adapt_dt()
+        o.step(t, dto)
+        t += dto
+        g.step(1)
+        dtg = g.time()[1]
+        assert abs(dtg - dto) <= (1e-12 if precision == 64 else 1e-6) * dto, (dtg, dto)
+    wg, pg = g.fields()
+    wo, po = o.fields()
+    if precision == 64:
+        assert_fields_close(wg, pg, wo, po, o.metric(3), 1e-10)
+    else:
+        assert relerr(pg, po) < 1e-6, relerr(pg, po)
+        assert np.max(np.abs(wg - wo)) / np.max(np.abs(wo)) < 1e-5
